@@ -1,0 +1,384 @@
+#!/usr/bin/env python
+"""Benchmark of the per-turn longitudinal tracking path.
+
+Workload (one "step" = one turn over the whole beam): protons at 26 GeV/c,
+C = 6911.5 m, gamma_t = 18, h = 4620, V = 4.5 MV, phi = 0; bi-Gaussian bunch
+(sigma_dt 0.4 ns, sigma_dE matched, seed 0) of 1e7 macro-particles,
+intensity 1e10; 2^14 slices over 2.5 ns around the bunch centre; induced
+voltage of a broadband resonator (R_s 5 MOhm, f_r 1 GHz, Q 1) through
+InducedVoltageFreq (n_fft = 16384), applied with linear_interp_kick; then
+the RF kick, the drift and the slicing.  Synthetic data only.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Our arm times K fused turns (CUDA graph) on the device with CUDA events and
+prints one JSON line; --impl reference times the reference's CPU C++ path
+(oracle/_ref) on the host cores with the same workload and metric.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-turns/s on 1 B200, FP32-batched vs plain FP64 at <=1e-5 rel err"
+UNIT = "particle-turns/s"
+WORKLOAD = ("1e7 protons 26 GeV/c, h=4620 4.5 MV, 2^14 slices, broadband "
+            "resonator 5 MOhm/1 GHz/Q=1 via FFT (n_fft 16384), lik + kick + "
+            "drift + slice per turn")
+BYTES_PER_PARTICLE = {"f64": 32, "f32p64": 24}  # read + write of dt and dE
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--particles", type=float, default=1e7)
+    ap.add_argument("--slices", type=int, default=16384)
+    ap.add_argument("--precision", default="f64", choices=["f64", "f32p64"])
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true")
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------- machine
+def machine(n_turns: int):
+    from blond_b200.beam.beam import Proton
+    from blond_b200.input_parameters.rf_parameters import RFStation
+    from blond_b200.input_parameters.ring import Ring
+    ring = Ring(6911.5, 1 / 18**2, 26e9, Proton(), n_turns)
+    rf = RFStation(ring, [4620], [4.5e6], [0.0])
+    return ring, rf
+
+
+def host_bunch(ring, rf, n: int):
+    from blond_b200.beam.distributions import _get_dE_from_dt, bigaussian_arrays
+    sdE = _get_dE_from_dt(ring, rf, 0.4e-9)
+    centre = (rf.phi_s[0] - rf.phi_rf[0, 0]) / rf.omega_rf[0, 0]
+    dt, dE = bigaussian_arrays(n, 0.4e-9, sdE, centre, 0)
+    return dt, dE, centre
+
+
+def window(centre, S):
+    cl, cr = centre - 1.25e-9, centre + 1.25e-9
+    edges = np.linspace(cl, cr, S + 1)
+    return cl, cr, (edges[:-1] + edges[1:]) / 2
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples (200 ms) during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.rows = []
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(device_index)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = [r for r in self.rows if len(r) >= 7]
+        if not rows:
+            return None
+        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4)
+                          if r[3 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": float(rows[0][1]) if rows[0][1].replace(".", "").isdigit() else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ----------------------------------------------------------------- CPU path
+def cpu_reference(n: int, S: int, turns: int | None, seconds: float | None,
+                  warmup: int = 0):
+    """Reference C++ (oracle/_ref) on the host cores; returns
+    (particle-turns/s, turns timed, kind, cores)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_cpu
+    path = ref_cpu.CpuPath()
+    total = (turns or 1000) + warmup + 2
+    ring, rf = machine(total)
+    dt, dE, centre = host_bunch(ring, rf, n)
+    cl, cr, bc = window(centre, S)
+    bin_size = (cr - cl) / S
+    freq = np.fft.rfftfreq(S, bin_size)
+    Z = _resonator_host(path, freq) / bin_size
+    prog = ref_cpu.programme(rf)
+    kw = dict(impedance=(S, Z), cuts=(cl, cr), bin_centers=bc, n_slices=S,
+              charge=1.0, ratio=1e10 / n)
+    if warmup:
+        path.run(dt, dE, prog, warmup, 0, **kw)
+    if turns is None:
+        # bounded sample: turns until about `seconds` of CPU work
+        one = path.run(dt, dE, prog, 1, warmup, **kw)
+        turns = max(1, min(total - warmup - 2, int(seconds / max(one, 1e-6))))
+        sec = path.run(dt, dE, prog, turns, warmup + 1, **kw)
+    else:
+        sec = path.run(dt, dE, prog, turns, warmup, **kw)
+    return n * turns / sec, turns, path.kind, path.cores, sec
+
+
+def _resonator_host(path, freq):
+    """Impedance on the host with the reference's own fast_resonator (or the
+    restatement when the reference library is absent)."""
+    import ctypes as ct
+    f = np.ascontiguousarray(freq, dtype=np.float64)
+    re, im = np.zeros(len(f)), np.zeros(len(f))
+    R, Q, fr = np.array([5e6]), np.array([1.0]), np.array([1e9])
+    P = lambda a: a.ctypes.data_as(ct.c_void_p)  # noqa: E731
+    fn = getattr(path.lib, "fast_resonator_real_imag", None) or \
+        getattr(path.lib, "oracle_fast_resonator_f64")
+    fn(P(re), P(im), P(f), P(R), P(Q), P(fr), ct.c_int(1), ct.c_int(len(f)))
+    return re + 1j * im
+
+
+# ----------------------------------------------------------------- dist
+def dist_init(args):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        if args.impl == "ours":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def dist_max(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ----------------------------------------------------------------- our arm
+def build_fused(n, S, n_turns, precision):
+    import torch
+    from blond_b200.beam.beam import Beam
+    from blond_b200.beam.profile import CutOptions, Profile
+    from blond_b200.engine import FusedTracker
+    from blond_b200.impedances.impedance import InducedVoltageFreq, TotalInducedVoltage
+    from blond_b200.impedances.impedance_sources import Resonators
+    from blond_b200.trackers.tracker import RingAndRFTracker
+    ring, rf = machine(n_turns)
+    dt, dE, centre = host_bunch(ring, rf, n)
+    beam = Beam(ring, n, 1e10, dt=dt, dE=dE, dtype=torch.float64)
+    cl, cr, _ = window(centre, S)
+    prof = Profile(beam, CutOptions(cut_left=cl, cut_right=cr, n_slices=S))
+    iv = InducedVoltageFreq(beam, prof, [Resonators(5e6, 1e9, 1.0)])
+    tiv = TotalInducedVoltage(beam, prof, [iv])
+    tracker = RingAndRFTracker(rf, beam)
+    fused = FusedTracker(tracker, prof, tiv, precision=precision, turns_per_graph=50)
+    return fused, beam, iv.n_fft
+
+
+def time_turns(fused, turns):
+    import torch
+    s = torch.cuda.current_stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record(s)
+    fused.track(turns)
+    b.record(s)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b)
+
+
+def run_ours(args, world, rank, local):
+    import torch
+    n = int(args.particles)
+    S = args.slices
+    W, K = max(3, args.warmup), args.steps
+    kt = min(K, 20)
+    E = args.e2e_steps
+    total = W + K + kt + E + 4
+    fused, beam, n_fft = build_fused(n, S, total, args.precision)
+    fused.track(W)
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = ClockSampler(local) if rank == 0 else None
+    ms = time_turns(fused, K)
+    clk = clocks.stop() if clocks else None
+    ms_max = dist_max(ms, world)
+    value = world * n * K / (ms_max * 1e-3)
+    # kernel durations (non-graph launches bracketed by events)
+    head_ms, part_ms = fused.time_kernels(kt)
+    part_avg = part_ms / kt
+    head_avg = head_ms / kt
+    alg_bytes = BYTES_PER_PARTICLE[args.precision] * n
+    achieved = alg_bytes / (part_avg * 1e-3) / 1e9
+    peaks = _peaks()
+    peak = peaks.get("hbm_gbs") or 6650.0
+    # end to end through the public API with pinned host buffers
+    hdt = beam.dt.cpu().pin_memory()
+    hdE = fused.dE.cpu().pin_memory()
+    s = torch.cuda.current_stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record(s)
+    for _ in range(E):
+        fused.dt.copy_(hdt, non_blocking=True)
+        fused.dE.copy_(hdE, non_blocking=True)
+        fused.track(1)
+        hdt.copy_(fused.dt, non_blocking=True)
+        hdE.copy_(fused.dE, non_blocking=True)
+    b.record(s)
+    torch.cuda.synchronize()
+    e2e_ms = a.elapsed_time(b)
+    e2e_value = world * n * E / (dist_max(e2e_ms, world) * 1e-3)
+    bytes_io = int(hdt.numel() * hdt.element_size() + hdE.numel() * hdE.element_size())
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": K, "warmup": W, "ms_per_step": ms_max / K,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": args.precision, "data": "synthetic",
+        "config": {"workload": WORKLOAD, "particles": n, "slices": S, "n_fft": n_fft,
+                   "intensity": 1e10, "turns_per_graph": 50,
+                   "l2": f"inputs larger than L2: {alg_bytes // 2 / 1e6:.0f} MB of dt/dE read per turn",
+                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": _traffic(args.precision, n),
+                     "kernel": "particle_kernel (lik+kick+drift+deposit)",
+                     "kernel_ms": part_avg, "head_kernel_ms": head_avg,
+                     "bytes_per_particle": BYTES_PER_PARTICLE[args.precision],
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst copy)"
+                     if peaks.get("hbm_gbs") else "fallback 6650 GB/s"},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": bytes_io,
+                "d2h_bytes_per_step": bytes_io,
+                "note": "per turn: pinned H2D of dt+dE, one fused turn, D2H of dt+dE"},
+        "gpu_launches": 2 * K,
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_mixed and args.precision == "f64":
+        del fused, beam
+        torch.cuda.empty_cache()
+        fm, bm_, _ = build_fused(n, S, W + K + kt + 4, "f32p64")
+        fm.track(W)
+        ms32 = time_turns(fm, K)
+        h32, p32 = fm.time_kernels(kt)
+        ach32 = BYTES_PER_PARTICLE["f32p64"] * n / (p32 / kt * 1e-3) / 1e9
+        out["mixed_precision"] = {"dtype": "f32p64", "value": n * K / (ms32 * 1e-3),
+                                  "ms_per_step": ms32 / K, "kernel_ms": p32 / kt,
+                                  "achieved_gbs": ach32, "frac": ach32 / peak}
+        del fm, bm_
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, turns, kind, cores, sec = cpu_reference(n, S, None, args.cpu_seconds)
+        out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cores, "kind": kind,
+                               "sample": f"{turns} turns of the full {n:.0e}-particle "
+                                         f"workload ({sec:.1f} s)"}
+    return out
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def _traffic(precision, n):
+    """DRAM bytes per launch of the particle kernel from the committed ncu
+    summary (scaled to n particles), or None."""
+    path = os.path.join(ROOT, "profiles", "particle_kernel_c2.txt")
+    try:
+        for line in open(path):
+            if line.startswith(f"traffic_bytes_per_particle_{precision}:"):
+                return float(line.split(":")[1]) * n
+    except OSError:
+        pass
+    return None
+
+
+# ----------------------------------------------------------------- ref arm
+def run_reference(args, world, rank):
+    n = int(args.particles)
+    W, K = max(3, args.warmup), args.steps
+    v, turns, kind, cores, sec = cpu_reference(n, args.slices, K, None, warmup=W)
+    return {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
+        "steps": K, "warmup": W, "ms_per_step": sec / K * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "particles": n, "slices": args.slices,
+                   "n_fft": args.slices, "intensity": 1e10,
+                   "parallelism": f"{cores} host threads"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind,
+                         "sample": f"{K} turns of the full workload after {W} warm-up"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        rank = int(os.environ.get("RANK", "0"))
+        if rank != 0:
+            return
+        print(json.dumps(run_reference(args, world, rank)), flush=True)
+        return
+    world, rank, local = dist_init(args)
+    try:
+        out = run_ours(args, world, rank, local)
+        if rank == 0:
+            print(json.dumps(out), flush=True)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

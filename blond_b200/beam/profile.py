@@ -1,0 +1,145 @@
+"""Profile slicing (blond/beam/profile.py:44-991), hot path on the B200.
+
+``Profile.track()`` runs ``slice_beam`` (or ``slice_smooth``) over the
+device coordinates into ``n_macroparticles``, a device tensor in the beam's
+precision.  Edges and bin centres are computed on the host exactly as the
+reference does (np.linspace, then midpoints) and kept both as numpy arrays
+and as device tensors (``bin_centers_dev``).
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from .. import bmath as bm
+
+
+class CutOptions:
+    """Slicing frame (profile.py:44-259)."""
+
+    def __init__(self, cut_left=None, cut_right=None, n_slices: int = 100,
+                 n_sigma=None, cuts_unit: str = "s", rf_station=None):
+        self.cut_left = float(cut_left) if cut_left is not None else None
+        self.cut_right = float(cut_right) if cut_right is not None else None
+        self.n_slices = int(n_slices)
+        self.n_sigma = float(n_sigma) if n_sigma is not None else None
+        self.cuts_unit = cuts_unit
+        self.rf_station = rf_station
+        if cuts_unit == "rad" and rf_station is None:
+            raise RuntimeError('Argument "rf_station" required to convert from '
+                               "radians to seconds")
+        if cuts_unit not in ("rad", "s"):
+            raise NameError(f'cuts_unit should be "s" or "rad", not {cuts_unit=} !')
+        self.edges = np.zeros(self.n_slices + 1)
+        self.bin_centers = np.zeros(self.n_slices)
+        self.bin_size = 0.0
+
+    def set_cuts(self, beam=None):
+        """profile.py:175-211."""
+        if self.cut_left is None and self.cut_right is None:
+            dt = beam.dt.double()
+            if self.n_sigma is None:
+                dt_min, dt_max = float(dt.min()), float(dt.max())
+                self.cut_left = dt_min - 0.05 * (dt_max - dt_min)
+                self.cut_right = dt_max + 0.05 * (dt_max - dt_min)
+            else:
+                mean, sigma = float(dt.mean()), float(dt.std(unbiased=False))
+                self.cut_left = mean - self.n_sigma * sigma / 2
+                self.cut_right = mean + self.n_sigma * sigma / 2
+        else:
+            self.cut_left = float(self.convert_coordinates(self.cut_left, self.cuts_unit))
+            self.cut_right = float(self.convert_coordinates(self.cut_right, self.cuts_unit))
+        self.edges = np.linspace(self.cut_left, self.cut_right,
+                                 self.n_slices + 1).astype(bm.precision.real_t)
+        self.bin_centers = (self.edges[:-1] + self.edges[1:]) / 2
+        self.bin_size = (self.cut_right - self.cut_left) / self.n_slices
+
+    def convert_coordinates(self, value: float, input_unit_type: str) -> float:
+        if input_unit_type == "s":
+            return value
+        if input_unit_type == "rad":
+            return value / float(self.rf_station.omega_rf[0, self.rf_station.counter[0]])
+        raise NameError(input_unit_type)
+
+    def get_slices_parameters(self):
+        return (self.n_slices, self.cut_left, self.cut_right, self.n_sigma,
+                self.edges, self.bin_centers, self.bin_size)
+
+
+class FitOptions:
+    def __init__(self, fit_option=None, fit_extra_options=None):
+        self.fit_option = fit_option
+        self.fit_extra_options = fit_extra_options
+
+
+class FilterOptions:
+    def __init__(self, filter_method=None, filter_extra_options=None):
+        self.filter_method = filter_method
+        self.filter_extra_options = filter_extra_options
+
+
+class OtherSlicesOptions:
+    def __init__(self, smooth: bool = False, direct_slicing: bool = True):
+        self.smooth = smooth
+        self.direct_slicing = direct_slicing
+
+
+class Profile:
+    """Beam profile on the device (profile.py:561-719)."""
+
+    def __init__(self, beam, cut_options: CutOptions | None = None,
+                 fit_options: FitOptions | None = None,
+                 filter_options: FilterOptions | None = None,
+                 other_slices_options: OtherSlicesOptions | None = None):
+        cut_options = cut_options or CutOptions()
+        fit_options = fit_options or FitOptions()
+        filter_options = filter_options or FilterOptions()
+        other_slices_options = other_slices_options or OtherSlicesOptions()
+        if fit_options.fit_option is not None or filter_options.filter_method is not None:
+            raise NotImplementedError(
+                "profile fits and filters are host-side diagnostics outside the "
+                "tracking hot path; use the reference toolbox on a host copy")
+        self.cut_options = cut_options
+        cut_options.set_cuts(beam)
+        self.beam = beam
+        (self.n_slices, self.cut_left, self.cut_right, self.n_sigma, self.edges,
+         self.bin_centers, self.bin_size) = cut_options.get_slices_parameters()
+        dtype = beam.dt.dtype if beam is not None else bm.precision.torch_t
+        self.bin_centers_dev = torch.as_tensor(self.bin_centers, device="cuda").to(dtype)
+        self.n_macroparticles = torch.zeros(self.n_slices, dtype=dtype, device="cuda")
+        self.beam_spectrum = None
+        self.beam_spectrum_freq = np.array([])
+        self.smooth = bool(other_slices_options.smooth)
+        self.operations = [self._slice_smooth if self.smooth else self._slice]
+        if other_slices_options.direct_slicing and beam is not None:
+            self.track()
+
+    def track(self):
+        for op in self.operations:
+            op()
+
+    def _slice(self):
+        bm.slice_beam(self.beam.dt, self.n_macroparticles, self.cut_left,
+                      self.cut_right)
+
+    def _slice_smooth(self):
+        bm.slice_smooth(self.beam.dt, self.n_macroparticles, self.cut_left,
+                        self.cut_right)
+
+    def beam_spectrum_freq_generation(self, n_sampling_fft: int):
+        self.beam_spectrum_freq = bm.rfftfreq(n_sampling_fft, self.bin_size)
+
+    def beam_spectrum_generation(self, n_sampling_fft: int):
+        self.beam_spectrum = bm.rfft(self.n_macroparticles, n_sampling_fft)
+
+    def beam_profile_derivative(self, mode: str = "gradient"):
+        """profile.py:905-937 ('gradient' only): np.gradient on the device."""
+        if mode != "gradient":
+            raise NotImplementedError(f"derivative mode {mode!r}")
+        dist = float(self.bin_centers[1] - self.bin_centers[0])
+        p = self.n_macroparticles.double()
+        d = torch.empty_like(p)
+        d[1:-1] = (p[2:] - p[:-2]) / (2.0 * dist)
+        d[0] = (p[1] - p[0]) / dist
+        d[-1] = (p[-1] - p[-2]) / dist
+        return self.bin_centers, d

@@ -1,0 +1,258 @@
+"""bmath-level hot-path functions on CUDA tensors.
+
+Same names, argument order and in-place semantics as the reference backend
+functions that ``blond.utils.bmath`` dispatches to
+(blond/utils/butils_wrap_cpp.py:835-989, declared in
+blond/utils/bmath_backends.py:155-181).  Particle arrays are torch CUDA
+tensors (float64 for the 'double' precision, float32 for 'single') and are
+modified in place; small parameter arrays may be numpy arrays, lists or
+tensors.  Every call is asynchronous on torch's current CUDA stream.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+
+import numpy as np
+import torch
+
+from . import _lib
+
+__all__ = [
+    "kick", "drift", "slice_beam", "slice_smooth", "linear_interp_kick",
+    "rf_volt_comp", "fast_resonator", "rfft", "irfft", "rfftfreq",
+    "induced_voltage_1turn", "precision", "use_precision", "B200Backend",
+]
+
+_SOLVERS = {"simple": 0, "legacy": 1, "exact": 2}
+
+
+class _Precision:
+    """Mirror of blond.utils.PrecisionClass (utils/__init__.py:18-55)."""
+
+    def __init__(self):
+        self.set("double")
+
+    def set(self, p: str = "double"):
+        if p in ("single", "s", "32", "float32", "float", "f"):
+            self.str, self.real_t, self.torch_t = "single", np.float32, torch.float32
+            self.complex_t, self.num = np.complex64, 1
+        elif p in ("double", "d", "64", "float64"):
+            self.str, self.real_t, self.torch_t = "double", np.float64, torch.float64
+            self.complex_t, self.num = np.complex128, 2
+        else:
+            raise ValueError(f"{p=} is not recognized, use 'single' or 'double'")
+
+
+precision = _Precision()
+
+
+def use_precision(p: str = "double") -> None:
+    precision.set(p)
+
+
+def _stream() -> ct.c_void_p:
+    return ct.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _ptr(t: torch.Tensor) -> ct.c_void_p:
+    return ct.c_void_p(t.data_ptr())
+
+
+def _suffix(t: torch.Tensor) -> str:
+    if t.dtype == torch.float64:
+        return "f64"
+    if t.dtype == torch.float32:
+        return "f32"
+    raise TypeError(f"particle arrays must be float64 or float32, got {t.dtype}")
+
+
+def _check_particles(*arrays: torch.Tensor) -> None:
+    dtype = None
+    for a in arrays:
+        if not isinstance(a, torch.Tensor) or not a.is_cuda:
+            raise TypeError("particle arrays must be CUDA tensors (in-place update)")
+        if not a.is_contiguous():
+            raise ValueError("particle arrays must be contiguous")
+        if dtype is not None and a.dtype != dtype:
+            raise TypeError(f"dtype mismatch: {a.dtype} vs {dtype}")
+        dtype = a.dtype
+    _suffix(arrays[0])
+
+
+def as_device(x, dtype: torch.dtype, device=None) -> torch.Tensor:
+    """Small parameter array -> contiguous CUDA tensor of ``dtype``."""
+    if device is None:
+        device = torch.device("cuda", torch.cuda.current_device())
+    if isinstance(x, torch.Tensor):
+        return x.to(device=device, dtype=dtype).contiguous()
+    return torch.as_tensor(np.ascontiguousarray(np.asarray(x, dtype=np.float64)),
+                           device=device).to(dtype).contiguous()
+
+
+def _real(t: torch.Tensor):
+    return _lib.c_dbl if t.dtype == torch.float64 else _lib.c_flt
+
+
+# --------------------------------------------------------------------- kick
+def kick(dt, dE, voltage, omega_rf, phi_rf, charge, n_rf, acceleration_kick):
+    """butils_wrap_cpp.kick (:863-898) -> cpp_routines/kick.cpp:16-35."""
+    _check_particles(dt, dE)
+    r = _real(dt)
+    V = as_device(voltage, dt.dtype, dt.device)
+    om = as_device(omega_rf, dt.dtype, dt.device)
+    ph = as_device(phi_rf, dt.dtype, dt.device)
+    _lib.call(f"blond_kick_{_suffix(dt)}", _ptr(dt), _ptr(dE), int(n_rf),
+              r(float(charge)), _ptr(V), _ptr(om), _ptr(ph), dt.numel(),
+              r(float(acceleration_kick)), _stream())
+
+
+def rf_volt_comp(voltages, omega_rf, phi_rf, bin_centers):
+    """butils_wrap_cpp.rf_volt_comp (:835-860): returns a new array."""
+    bc = bin_centers if isinstance(bin_centers, torch.Tensor) else as_device(
+        bin_centers, precision.torch_t)
+    bc = bc.contiguous()
+    out = torch.zeros_like(bc)
+    V = as_device(voltages, bc.dtype, bc.device)
+    om = as_device(omega_rf, bc.dtype, bc.device)
+    ph = as_device(phi_rf, bc.dtype, bc.device)
+    _lib.call(f"blond_rf_volt_comp_{_suffix(bc)}", _ptr(V), _ptr(om), _ptr(ph),
+              _ptr(bc), int(V.numel()), bc.numel(), _ptr(out), _stream())
+    return out
+
+
+# -------------------------------------------------------------------- drift
+def drift(dt, dE, solver, t_rev, length_ratio, alpha_order, eta_0, eta_1,
+          eta_2, alpha_0, alpha_1, alpha_2, beta, energy):
+    """butils_wrap_cpp.drift (:901-943) -> cpp_routines/drift.cpp:19-78."""
+    _check_particles(dt, dE)
+    if solver not in _SOLVERS:
+        raise KeyError(solver)
+    r = _real(dt)
+    vals = [t_rev, length_ratio, alpha_order, eta_0, eta_1, eta_2, alpha_0,
+            alpha_1, alpha_2, beta, energy]
+    _lib.call(f"blond_drift_{_suffix(dt)}", _ptr(dt), _ptr(dE),
+              _SOLVERS[solver], *[r(float(v)) for v in vals], dt.numel(),
+              _stream())
+
+
+# ------------------------------------------------------------------ slicing
+def slice_beam(dt, profile, cut_left, cut_right):
+    """butils_wrap_cpp.slice_beam (:971-984) -> histogram.cpp:22-73."""
+    _check_particles(dt, profile)
+    r = _real(dt)
+    _lib.call(f"blond_histogram_{_suffix(dt)}", _ptr(dt), _ptr(profile),
+              r(float(cut_left)), r(float(cut_right)), profile.numel(),
+              dt.numel(), _stream())
+
+
+def slice_smooth(dt, profile, cut_left, cut_right):
+    """butils_wrap_cpp.slice_smooth (:987-999) -> histogram.cpp:75-132."""
+    _check_particles(dt, profile)
+    r = _real(dt)
+    _lib.call(f"blond_smooth_histogram_{_suffix(dt)}", _ptr(dt), _ptr(profile),
+              r(float(cut_left)), r(float(cut_right)), profile.numel(),
+              dt.numel(), _stream())
+
+
+# ------------------------------------------------------ interpolated kick
+def linear_interp_kick(dt, dE, voltage, bin_centers, charge,
+                       acceleration_kick):
+    """butils_wrap_cpp.linear_interp_kick (:946-968)."""
+    _check_particles(dt, dE)
+    r = _real(dt)
+    V = as_device(voltage, dt.dtype, dt.device)
+    bc = as_device(bin_centers, dt.dtype, dt.device)
+    _lib.call(f"blond_linear_interp_kick_{_suffix(dt)}", _ptr(dt), _ptr(dE),
+              _ptr(V), _ptr(bc), r(float(charge)), bc.numel(), dt.numel(),
+              r(float(acceleration_kick)), _stream())
+
+
+# ------------------------------------------------------- impedance / FFT
+def fast_resonator(R_S, Q, frequency_array, frequency_R, impedance=None):
+    """butils_wrap_cpp.fast_resonator (:1133-1171): complex128 tensor."""
+    f = as_device(frequency_array, torch.float64)
+    R = as_device(R_S, torch.float64)
+    q = as_device(Q, torch.float64)
+    fr = as_device(frequency_R, torch.float64)
+    re = torch.zeros_like(f)
+    im = torch.zeros_like(f)
+    _lib.call("blond_fast_resonator_f64", _ptr(re), _ptr(im), _ptr(f), _ptr(R),
+              _ptr(q), _ptr(fr), int(R.numel()), f.numel(), _stream())
+    out = torch.complex(re, im)
+    if impedance is not None and isinstance(impedance, torch.Tensor) and \
+            impedance.dtype == torch.complex128 and impedance.numel() == out.numel():
+        impedance.copy_(out)
+        return impedance
+    return out
+
+
+def rfft(a, n=None):
+    """numpy.fft.rfft(a, n) semantics (bmath_backends.py:447) in float64."""
+    x = as_device(a, torch.float64).reshape(-1)
+    n = int(x.numel() if n is None else n)
+    out = torch.empty(n // 2 + 1, dtype=torch.complex128, device=x.device)
+    _lib.call("blond_rfft_f64", _ptr(x), x.numel(), n, _ptr(out), _stream())
+    return out
+
+
+def irfft(a, n=None):
+    """numpy.fft.irfft(a, n) semantics (bmath_backends.py:448) in float64."""
+    if isinstance(a, torch.Tensor):
+        spec = a.to(torch.complex128)
+    else:
+        spec = torch.as_tensor(np.asarray(a, dtype=np.complex128),
+                               device=torch.device("cuda", torch.cuda.current_device()))
+    spec = spec.reshape(-1).contiguous()
+    m = spec.numel()
+    n = int(2 * (m - 1) if n is None else n)
+    need = n // 2 + 1
+    if m < need:
+        spec = torch.cat([spec, spec.new_zeros(need - m)])
+    elif m > need:
+        spec = spec[:need].contiguous()
+    out = torch.empty(n, dtype=torch.float64, device=spec.device)
+    _lib.call("blond_irfft_f64", _ptr(spec), n, _ptr(out), n, _stream())
+    return out
+
+
+def rfftfreq(n, d=1.0):
+    """numpy.fft.rfftfreq (host arithmetic, setup only)."""
+    return np.fft.rfftfreq(int(n), d)
+
+
+def induced_voltage_1turn(profile, total_impedance, n_fft, scale, n_out):
+    """-scale * irfft(total_impedance * rfft(profile, n_fft))[:n_out]
+    (impedance.py:475-489) in one launch; float64 tensor of n_out values."""
+    p = as_device(profile, torch.float64)
+    Z = total_impedance if isinstance(total_impedance, torch.Tensor) else \
+        torch.as_tensor(np.asarray(total_impedance, np.complex128),
+                        device=p.device)
+    Z = Z.to(torch.complex128).contiguous()
+    out = torch.empty(int(n_out), dtype=torch.float64, device=p.device)
+    _lib.call("blond_induced_voltage_f64", _ptr(p), p.numel(), _ptr(Z),
+              int(n_fft), float(scale), _ptr(out), int(n_out), _stream())
+    return out
+
+
+class B200Backend:
+    """The hot-path subset of blond's MasterBackend attribute contract
+    (bmath_backends.py:61-201), backed by libblond_b200.  See
+    INTEGRATION.md for installing it into a reference ``bm`` object."""
+
+    device = "GPU_B200"
+
+    def __init__(self):
+        self.precision = precision
+        self.kick = kick
+        self.drift = drift
+        self.slice_beam = slice_beam
+        self.slice_smooth = slice_smooth
+        self.linear_interp_kick = linear_interp_kick
+        self.rf_volt_comp = rf_volt_comp
+        self.fast_resonator = fast_resonator
+        self.rfft = rfft
+        self.irfft = irfft
+        self.rfftfreq = rfftfreq
+
+    def use_precision(self, p: str = "double"):
+        use_precision(p)

@@ -1,0 +1,104 @@
+// Shared helpers for the blond_b200 CUDA library: status codes, the
+// thread-local error message, launch geometry and small device utilities.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdarg.h>
+#include <math.h>
+
+#include "../../include/blond_b200.h"
+
+namespace bb {
+
+// ---------------------------------------------------------------- errors
+void set_error(const char* fmt, ...);
+void clear_error();
+
+#define BB_CHECK_ARG(cond, ...)                                              \
+    do {                                                                     \
+        if (!(cond)) {                                                       \
+            ::bb::set_error(__VA_ARGS__);                                    \
+            return BLOND_ERR_INVALID_ARGUMENT;                               \
+        }                                                                    \
+    } while (0)
+
+#define BB_CHECK_SIZE(cond, ...)                                             \
+    do {                                                                     \
+        if (!(cond)) {                                                       \
+            ::bb::set_error(__VA_ARGS__);                                    \
+            return BLOND_ERR_SIZE;                                           \
+        }                                                                    \
+    } while (0)
+
+#define BB_CUDA(call)                                                        \
+    do {                                                                     \
+        cudaError_t e_ = (call);                                             \
+        if (e_ != cudaSuccess) {                                             \
+            ::bb::set_error("%s failed: %s (%s:%d)", #call,                  \
+                            cudaGetErrorString(e_), __FILE__, __LINE__);     \
+            return BLOND_ERR_CUDA;                                           \
+        }                                                                    \
+    } while (0)
+
+// After a kernel launch: report configuration errors (not asynchronous
+// execution errors, which surface at the caller's next synchronisation).
+#define BB_LAUNCH_CHECK()                                                    \
+    do {                                                                     \
+        cudaError_t e_ = cudaGetLastError();                                 \
+        if (e_ != cudaSuccess) {                                             \
+            ::bb::set_error("kernel launch failed: %s (%s:%d)",              \
+                            cudaGetErrorString(e_), __FILE__, __LINE__);     \
+            return BLOND_ERR_CUDA;                                           \
+        }                                                                    \
+    } while (0)
+
+inline bool aligned(const void* p, size_t a) {
+    return (reinterpret_cast<uintptr_t>(p) & (a - 1)) == 0;
+}
+
+// ------------------------------------------------------- launch geometry
+struct DeviceInfo {
+    int device;
+    int sm_count;
+    int max_smem_optin;  // bytes per block with opt-in
+};
+// Cached per current device.
+const DeviceInfo& device_info();
+
+// Grid for a grid-stride particle loop: a whole number of waves over the
+// SMs, never more blocks than there are chunks of work.
+inline int particle_grid(int64_t n, int threads, int blocks_per_sm,
+                         int items_per_thread = 1) {
+    const DeviceInfo& d = device_info();
+    int64_t need = (n + (int64_t)threads * items_per_thread - 1) /
+                   ((int64_t)threads * items_per_thread);
+    int64_t cap = (int64_t)d.sm_count * blocks_per_sm;
+    if (need < 1) need = 1;
+    return (int)(need < cap ? need : cap);
+}
+
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// ------------------------------------------------------ device utilities
+template <typename T> struct Vec2;
+template <> struct Vec2<double> { using type = double2; };
+template <> struct Vec2<float> { using type = float2; };
+
+__device__ __forceinline__ double dev_sin(double x) { return sin(x); }
+__device__ __forceinline__ float dev_sin(float x) { return sinf(x); }
+__device__ __forceinline__ double dev_floor(double x) { return floor(x); }
+__device__ __forceinline__ float dev_floor(float x) { return floorf(x); }
+__device__ __forceinline__ double dev_sqrt(double x) { return sqrt(x); }
+__device__ __forceinline__ float dev_sqrt(float x) { return sqrtf(x); }
+
+// Plain IEEE multiply / subtract that the compiler may not fuse into an FMA.
+// The histogram bin expression floor((dt - cut_left) * inv_w) must round
+// exactly like the reference's C++ for bit-exact counts.
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+
+}  // namespace bb

@@ -1,0 +1,779 @@
+// Fused per-turn tracking engine.
+//
+// One turn of the reference main loop [TotalInducedVoltage, RingAndRFTracker,
+// Profile] (EX_05_Wake_impedance.py:318-339) touches every particle four
+// times in the reference (lik, kick, drift, histogram: 80 B per particle in
+// FP64).  Here it is two launches:
+//
+//   head      one cluster (spectral_kernel) or one CTA: profile <- histogram
+//             (and clears it), induced voltage + interpolation table for this
+//             turn, turn counter += 1;
+//   particles one pass over SoA dt/dE: interpolated induced kick, RF kick of
+//             turn t, drift with turn t+1 parameters, deposit into a
+//             shared-memory histogram flushed with integer atomics --
+//             32 B per particle in FP64 (24 B in F32P64).
+//
+// The turn index lives in device memory, so a CUDA graph of K turns is
+// captured once and replayed.
+#include "spectral.cuh"
+
+#include <algorithm>
+#include <vector>
+
+namespace bb {
+
+constexpr int kMaxRfEngine = 16;
+
+struct DriftTurn {
+    double Tr;      // t_rev * length_ratio
+    double simple;  // Tr * eta_0 / (beta^2 E)
+    double e0, e1, e2;
+    double ib2, ie2, energy;
+    double a0, a1, a2;
+    double pad;
+};
+
+struct ParticleArgs {
+    void* dt;
+    void* dE;
+    int64_t n;
+    int n_rf;
+    double charge;
+    const double* V;    // [(turns+1) * n_rf]
+    const double* om;
+    const double* ph;
+    const double* acc;  // [turns]
+    const DriftTurn* drift;  // [turns+1]
+    int order;          // legacy alpha order
+    int64_t n_turns;
+    const long long* turn;
+    // slicing
+    int S;
+    double cut_left, inv_w;
+    int* hist;
+    // interpolation table (induced voltage)
+    const void* table;
+    double bc0, lik_inv_w, bw;
+};
+
+enum { PREC_F64 = 0, PREC_F32P64 = 1 };
+
+template <int PREC>
+struct Coord;
+template <> struct Coord<PREC_F64> { using E = double; };
+template <> struct Coord<PREC_F32P64> { using E = float; };
+
+struct TurnConsts {
+    double V[kMaxRfEngine], om[kMaxRfEngine], ph[kMaxRfEngine];
+    float Vf[kMaxRfEngine];
+    double acc;
+    DriftTurn d;
+};
+
+// 2 pi split for the FP64 range reduction of the RF phase.
+__device__ __forceinline__ double reduce_2pi(double x) {
+    const double inv2pi = 0.15915494309189533577;
+    const double twopi = 6.28318530717958647692;
+    return fma(-rint(x * inv2pi), twopi, x);
+}
+
+template <int PREC, int SOLVER, bool LIK, bool KICK, bool HIST, bool WARP_AGG>
+__device__ __forceinline__ void track_one(double& t,
+                                          typename Coord<PREC>::E& e,
+                                          const TurnConsts& c,
+                                          const ParticleArgs& a, int* sh, int order) {
+    using E = typename Coord<PREC>::E;
+    if (KICK) {
+        if (LIK) {
+            const double f = floor((t - a.bc0) * a.lik_inv_w);
+            if (f >= 0.0 && f < (double)(a.S - 1)) {
+                const int k = (int)f;
+                if (PREC == PREC_F64) {
+                    const double2 tb = __ldg(reinterpret_cast<const double2*>(a.table) + k);
+                    e += t * tb.x + tb.y;
+                } else {
+                    const float2 tb = __ldg(reinterpret_cast<const float2*>(a.table) + k);
+                    const float x = (float)(t - (a.bc0 + (double)k * a.bw));
+                    e += tb.x + tb.y * x;
+                }
+            }
+        }
+        if (PREC == PREC_F64) {
+            double s = 0.0;
+            for (int j = 0; j < a.n_rf; ++j) s += c.V[j] * sin(c.om[j] * t + c.ph[j]);
+            e += a.charge * s + c.acc;
+        } else {
+            float s = 0.0f;
+            for (int j = 0; j < a.n_rf; ++j)
+                s += c.Vf[j] * sinf((float)reduce_2pi(fma(c.om[j], t, c.ph[j])));
+            e += (float)a.charge * s + (float)c.acc;
+        }
+        if (SOLVER == BLOND_SOLVER_SIMPLE) {
+            t += c.d.simple * (double)e;
+        } else if (SOLVER == BLOND_SOLVER_LEGACY) {
+            const double d = (double)e;
+            double den;
+            if (order == 0) den = 1.0 - c.d.e0 * d;
+            else if (order == 1) den = 1.0 - c.d.e0 * d - c.d.e1 * d * d;
+            else den = 1.0 - c.d.e0 * d - c.d.e1 * d * d - c.d.e2 * d * d * d;
+            t += c.d.Tr * (1.0 / den - 1.0);
+        } else {
+            const double d = (double)e, en = c.d.energy;
+            const double delta = sqrt(1.0 + c.d.ib2 * (d * d * c.d.ie2 + 2.0 * d / en)) - 1.0;
+            t += c.d.Tr * ((1.0 + c.d.a0 * delta + c.d.a1 * (delta * delta) +
+                            c.d.a2 * (delta * delta * delta)) *
+                               (1.0 + d / en) / (1.0 + delta) -
+                           1.0);
+        }
+    }
+    (void)sh;
+}
+
+__device__ __forceinline__ int engine_bin(double t, double cut_left, double inv_w, int S) {
+    const double f = floor(__dmul_rn(__dsub_rn(t, cut_left), inv_w));
+    return (f >= 0.0 && f < (double)S) ? (int)f : -1;
+}
+
+__device__ __forceinline__ void deposit(int* sh, int b, bool warp_agg, unsigned mask) {
+    if (warp_agg) {
+        const unsigned peers = __match_any_sync(mask, b);
+        if (b >= 0 && (threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&sh[b], __popc(peers));
+    } else if (b >= 0) {
+        atomicAdd(&sh[b], 1);
+    }
+}
+
+constexpr int kEngineThreads = 512;
+
+// Pairs of particles per thread and iteration; pairs are read with one
+// 16-byte (dt) and one 16- or 8-byte (dE) load.
+template <int PREC, int SOLVER, bool LIK, bool KICK, bool WARP_AGG>
+__global__ void __launch_bounds__(kEngineThreads, 2)
+particle_kernel(const ParticleArgs a) {
+    using E = typename Coord<PREC>::E;
+    using E2 = typename Vec2<E>::type;
+    extern __shared__ int sh[];
+    __shared__ TurnConsts c;
+    long long t_idx = a.turn ? (*a.turn - 1) : 0;
+    if (t_idx < 0) t_idx = 0;
+    if (t_idx >= a.n_turns) t_idx = a.n_turns - 1;
+    if (KICK) {
+        for (int j = threadIdx.x; j < a.n_rf; j += blockDim.x) {
+            c.V[j] = a.V[t_idx * a.n_rf + j];
+            c.Vf[j] = (float)c.V[j];
+            c.om[j] = a.om[t_idx * a.n_rf + j];
+            c.ph[j] = a.ph[t_idx * a.n_rf + j];
+        }
+        if (threadIdx.x == 0) {
+            c.acc = a.acc[t_idx];
+            c.d = a.drift[t_idx + 1];
+        }
+    }
+    for (int k = threadIdx.x; k < a.S; k += blockDim.x) sh[k] = 0;
+    __syncthreads();
+
+    double* dt = reinterpret_cast<double*>(a.dt);
+    E* dE = reinterpret_cast<E*>(a.dE);
+    const int64_t npairs = a.n / 2;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int order = a.order;
+    // whole warps iterate together (needed by __match_any_sync)
+    const int lane = threadIdx.x & 31;
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31);
+         base < npairs; base += stride) {
+        const int64_t p = base + lane;
+        int b0 = -1, b1 = -1;
+        if (p < npairs) {
+            double2 tt = reinterpret_cast<const double2*>(dt)[p];
+            E2 ee = reinterpret_cast<const E2*>(dE)[p];
+            track_one<PREC, SOLVER, LIK, KICK, true, WARP_AGG>(tt.x, ee.x, c, a, sh, order);
+            track_one<PREC, SOLVER, LIK, KICK, true, WARP_AGG>(tt.y, ee.y, c, a, sh, order);
+            if (KICK) {
+                reinterpret_cast<double2*>(dt)[p] = tt;
+                reinterpret_cast<E2*>(dE)[p] = ee;
+            }
+            b0 = engine_bin(tt.x, a.cut_left, a.inv_w, a.S);
+            b1 = engine_bin(tt.y, a.cut_left, a.inv_w, a.S);
+        }
+        deposit(sh, b0, WARP_AGG, 0xffffffffu);
+        deposit(sh, b1, WARP_AGG, 0xffffffffu);
+    }
+    // odd tail particle
+    if ((a.n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+        double t = dt[a.n - 1];
+        E e = dE[a.n - 1];
+        track_one<PREC, SOLVER, LIK, KICK, true, false>(t, e, c, a, sh, order);
+        if (KICK) {
+            dt[a.n - 1] = t;
+            dE[a.n - 1] = e;
+        }
+        const int b = engine_bin(t, a.cut_left, a.inv_w, a.S);
+        if (b >= 0) atomicAdd(&sh[b], 1);
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < a.S; k += blockDim.x) {
+        const int v = sh[k];
+        if (v) atomicAdd(&a.hist[k], v);
+    }
+}
+
+// Profile <- histogram.  With clear, the histogram is zeroed and the turn
+// counter advanced (the head of a turn without induced voltage).
+__global__ void profile_kernel(int* hist, double* profile, int S, int clear,
+                               long long* turn) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < S;
+         k += gridDim.x * blockDim.x) {
+        profile[k] = (double)hist[k];
+        if (clear) hist[k] = 0;
+    }
+    if (clear && turn && blockIdx.x == 0 && threadIdx.x == 0) *turn += 1;
+}
+
+}  // namespace bb
+
+using namespace bb;
+
+struct blond_engine {
+    int precision = 0, n_rf = 0, solver = 0, S = 0;
+    int device = 0;
+    // programme
+    int64_t n_turns = 0;
+    double charge = 1.0;
+    double* d_V = nullptr;
+    double* d_om = nullptr;
+    double* d_ph = nullptr;
+    double* d_acc = nullptr;
+    DriftTurn* d_drift = nullptr;
+    int order = 0;
+    bool rf_set = false, drift_set = false;
+    std::vector<double> h_t_rev;
+    // slicing
+    bool slicing_set = false;
+    double cut_left = 0, cut_right = 0, inv_w = 0;
+    double* d_bc = nullptr;
+    double bc0 = 0, lik_inv_w = 0, bw = 0, dbc = 0;
+    // impedance
+    bool has_fft = false;
+    SpecPlan plan = {};
+    double2* d_H = nullptr;
+    double iv_scale = 0.0;
+    bool has_ind = false;
+    double* d_ind = nullptr;
+    // state
+    long long* d_turn = nullptr;
+    long long host_turn = 0;
+    int* d_hist = nullptr;
+    double* d_profile = nullptr;
+    double* d_vind = nullptr;
+    void* d_table = nullptr;
+    // beam
+    void* dt = nullptr;
+    void* dE = nullptr;
+    int64_t n = 0;
+    // tuning
+    int threads = kEngineThreads;
+    int blocks_per_sm = 2;
+    int turns_per_graph = 50;
+    // graph cache
+    cudaStream_t cap_stream = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    int graph_turns = 0;
+    bool graph_dirty = true;
+};
+
+namespace bb {
+
+static void free_ptr(void* p) {
+    if (p) cudaFree(p);
+}
+
+static int engine_smem(const blond_engine* e) { return (int)sizeof(int) * e->S; }
+
+// Raise a kernel's dynamic shared memory limit to the device's opt-in
+// maximum, once per device.  Done outside stream capture (engine_run calls
+// the launchers with launch=false before it captures).
+template <typename K>
+static int allow_max_smem(K kernel, bool* done) {
+    const DeviceInfo& d = device_info();
+    if (!done[d.device & 63]) {
+        BB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     d.max_smem_optin));
+        done[d.device & 63] = true;
+    }
+    return BLOND_OK;
+}
+
+template <int PREC, int SOLVER, bool LIK, bool KICK>
+static int launch_particles_t(blond_engine* e, const ParticleArgs& a, cudaStream_t s,
+                              bool launch) {
+    static bool done_agg[64] = {false}, done_plain[64] = {false};
+    const int smem = engine_smem(e);
+    const bool agg = e->S <= 2048;
+    const int grid = particle_grid(e->n / 2 + 1, e->threads, e->blocks_per_sm);
+    int rc;
+    if (agg) {
+        auto k = particle_kernel<PREC, SOLVER, LIK, KICK, true>;
+        if ((rc = allow_max_smem(k, done_agg))) return rc;
+        if (launch) k<<<grid, e->threads, smem, s>>>(a);
+    } else {
+        auto k = particle_kernel<PREC, SOLVER, LIK, KICK, false>;
+        if ((rc = allow_max_smem(k, done_plain))) return rc;
+        if (launch) k<<<grid, e->threads, smem, s>>>(a);
+    }
+    BB_LAUNCH_CHECK();
+    return BLOND_OK;
+}
+
+template <int PREC>
+static int launch_particles_p(blond_engine* e, const ParticleArgs& a, bool kick,
+                              cudaStream_t s, bool launch) {
+    if (!kick) return launch_particles_t<PREC, 0, false, false>(e, a, s, launch);
+    const bool lik = e->has_fft || e->has_ind;
+    switch (e->solver) {
+        case 0:
+            return lik ? launch_particles_t<PREC, 0, true, true>(e, a, s, launch)
+                       : launch_particles_t<PREC, 0, false, true>(e, a, s, launch);
+        case 1:
+            return lik ? launch_particles_t<PREC, 1, true, true>(e, a, s, launch)
+                       : launch_particles_t<PREC, 1, false, true>(e, a, s, launch);
+        default:
+            return lik ? launch_particles_t<PREC, 2, true, true>(e, a, s, launch)
+                       : launch_particles_t<PREC, 2, false, true>(e, a, s, launch);
+    }
+}
+
+static ParticleArgs particle_args(blond_engine* e) {
+    ParticleArgs a = {};
+    a.dt = e->dt;
+    a.dE = e->dE;
+    a.n = e->n;
+    a.n_rf = e->n_rf;
+    a.charge = e->charge;
+    a.V = e->d_V;
+    a.om = e->d_om;
+    a.ph = e->d_ph;
+    a.acc = e->d_acc;
+    a.drift = e->d_drift;
+    a.order = e->order;
+    a.n_turns = e->n_turns;
+    a.turn = e->d_turn;
+    a.S = e->S;
+    a.cut_left = e->cut_left;
+    a.inv_w = e->inv_w;
+    a.hist = e->d_hist;
+    a.table = e->d_table;
+    a.bc0 = e->bc0;
+    a.lik_inv_w = e->lik_inv_w;
+    a.bw = e->bw;
+    return a;
+}
+
+static int launch_particles(blond_engine* e, bool kick, cudaStream_t s,
+                            bool launch = true) {
+    const ParticleArgs a = particle_args(e);
+    if (e->precision == BLOND_PREC_F64)
+        return launch_particles_p<PREC_F64>(e, a, kick, s, launch);
+    return launch_particles_p<PREC_F32P64>(e, a, kick, s, launch);
+}
+
+static int launch_profile(blond_engine* e, bool clear, cudaStream_t s) {
+    const int threads = 256;
+    const int grid = std::min(64, (e->S + threads - 1) / threads);
+    profile_kernel<<<grid, threads, 0, s>>>(e->d_hist, e->d_profile, e->S, clear ? 1 : 0,
+                                            clear ? e->d_turn : nullptr);
+    BB_LAUNCH_CHECK();
+    return BLOND_OK;
+}
+
+static int launch_head(blond_engine* e, cudaStream_t s) {
+    if (!(e->has_fft || e->has_ind)) return launch_profile(e, true, s);
+    if (!e->has_fft) {
+        set_error("engine: an inductive impedance needs an FFT impedance in this build");
+        return BLOND_ERR_UNSUPPORTED;
+    }
+    SpecParams P = {};
+    P.p = e->plan;
+    P.mode = SPEC_FORWARD | SPEC_MULTIPLY | SPEC_INVERSE;
+    P.in_i32 = e->d_hist;
+    P.n_in = e->S;
+    P.profile_out = e->d_profile;
+    P.H = e->d_H;
+    P.out = e->d_vind;
+    P.n_out = std::min<int64_t>(e->S, e->plan.N);
+    P.out_scale = -e->iv_scale / (double)e->plan.M;
+    P.ind_coeff = e->has_ind ? e->d_ind : nullptr;
+    P.ind_dbc = e->dbc;
+    P.table = e->d_table;
+    P.table_f32 = e->precision == BLOND_PREC_F32P64;
+    P.charge = e->charge;
+    P.inv_w = e->lik_inv_w;
+    P.bc = e->d_bc;
+    P.turn = e->d_turn;
+    P.bump_turn = 1;
+    return launch_spectral(P, s);
+}
+
+static int launch_turn(blond_engine* e, cudaStream_t s) {
+    int rc = launch_head(e, s);
+    if (rc) return rc;
+    return launch_particles(e, true, s);
+}
+
+static int check_ready(blond_engine* e) {
+    if (!e->rf_set || !e->drift_set || !e->slicing_set || !e->dt) {
+        set_error("engine: set_rf, set_drift, set_slicing and bind_beam must all be "
+                  "called before tracking");
+        return BLOND_ERR_STATE;
+    }
+    return BLOND_OK;
+}
+
+static int upload(void** dst, const void* src, size_t bytes) {
+    free_ptr(*dst);
+    *dst = nullptr;
+    BB_CUDA(cudaMalloc(dst, bytes));
+    BB_CUDA(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice));
+    return BLOND_OK;
+}
+
+}  // namespace bb
+
+extern "C" {
+
+int blond_engine_create(blond_engine** out, int precision, int n_rf, int solver,
+                        int n_slices) {
+    BB_CHECK_ARG(out, "engine_create: null output");
+    BB_CHECK_ARG(precision == BLOND_PREC_F64 || precision == BLOND_PREC_F32P64,
+                 "engine_create: unknown precision %d", precision);
+    BB_CHECK_SIZE(n_rf >= 1 && n_rf <= kMaxRfEngine, "engine_create: n_rf=%d not in [1, %d]",
+                  n_rf, kMaxRfEngine);
+    BB_CHECK_ARG(solver >= 0 && solver <= 2, "engine_create: solver %d", solver);
+    const int max_s = (device_info().max_smem_optin - (int)sizeof(TurnConsts) - 1024) / 4;
+    BB_CHECK_SIZE(n_slices >= 2 && n_slices <= max_s,
+                  "engine_create: n_slices=%d not in [2, %d]", n_slices, max_s);
+    blond_engine* e = new blond_engine();
+    e->precision = precision;
+    e->n_rf = n_rf;
+    e->solver = solver;
+    e->S = n_slices;
+    cudaGetDevice(&e->device);
+    int rc = BLOND_OK;
+    do {
+        if (cudaMalloc(&e->d_turn, sizeof(long long)) != cudaSuccess ||
+            cudaMalloc(&e->d_hist, sizeof(int) * n_slices) != cudaSuccess ||
+            cudaMalloc(&e->d_profile, sizeof(double) * n_slices) != cudaSuccess ||
+            cudaMalloc(&e->d_vind, sizeof(double) * n_slices) != cudaSuccess ||
+            cudaMalloc(&e->d_table, sizeof(double2) * n_slices) != cudaSuccess) {
+            set_error("engine_create: cudaMalloc failed");
+            rc = BLOND_ERR_CUDA;
+            break;
+        }
+        cudaMemset(e->d_turn, 0, sizeof(long long));
+        cudaMemset(e->d_hist, 0, sizeof(int) * n_slices);
+        cudaMemset(e->d_profile, 0, sizeof(double) * n_slices);
+        cudaMemset(e->d_vind, 0, sizeof(double) * n_slices);
+        cudaMemset(e->d_table, 0, sizeof(double2) * n_slices);
+        if (cudaStreamCreateWithFlags(&e->cap_stream, cudaStreamNonBlocking) != cudaSuccess) {
+            set_error("engine_create: stream creation failed");
+            rc = BLOND_ERR_CUDA;
+            break;
+        }
+        if (cudaDeviceSynchronize() != cudaSuccess) {
+            set_error("engine_create: device error");
+            rc = BLOND_ERR_CUDA;
+        }
+    } while (0);
+    if (rc) {
+        blond_engine_destroy(e);
+        return rc;
+    }
+    *out = e;
+    return BLOND_OK;
+}
+
+int blond_engine_destroy(blond_engine* e) {
+    if (!e) return BLOND_OK;
+    if (e->graph) cudaGraphExecDestroy(e->graph);
+    if (e->cap_stream) cudaStreamDestroy(e->cap_stream);
+    for (void* p : {(void*)e->d_V, (void*)e->d_om, (void*)e->d_ph, (void*)e->d_acc,
+                    (void*)e->d_drift, (void*)e->d_bc, (void*)e->d_H, (void*)e->d_ind,
+                    (void*)e->d_turn, (void*)e->d_hist, (void*)e->d_profile,
+                    (void*)e->d_vind, e->d_table})
+        free_ptr(p);
+    delete e;
+    return BLOND_OK;
+}
+
+int blond_engine_set_rf(blond_engine* e, int64_t n_turns, const double* V,
+                        const double* om, const double* ph, const double* acc,
+                        double charge) {
+    BB_CHECK_ARG(e && V && om && ph && acc, "engine_set_rf: null pointer");
+    BB_CHECK_ARG(n_turns >= 1, "engine_set_rf: n_turns must be >= 1");
+    const size_t cols = (size_t)(n_turns + 1) * e->n_rf;
+    int rc;
+    if ((rc = upload((void**)&e->d_V, V, sizeof(double) * cols))) return rc;
+    if ((rc = upload((void**)&e->d_om, om, sizeof(double) * cols))) return rc;
+    if ((rc = upload((void**)&e->d_ph, ph, sizeof(double) * cols))) return rc;
+    if ((rc = upload((void**)&e->d_acc, acc, sizeof(double) * n_turns))) return rc;
+    e->n_turns = n_turns;
+    e->charge = charge;
+    e->rf_set = true;
+    e->graph_dirty = true;
+    return BLOND_OK;
+}
+
+int blond_engine_set_drift(blond_engine* e, double length_ratio, double alpha_order,
+                           const double* t_rev, const double* eta_0,
+                           const double* eta_1, const double* eta_2,
+                           const double* alpha_0, const double* alpha_1,
+                           const double* alpha_2, const double* beta,
+                           const double* energy) {
+    BB_CHECK_ARG(e && t_rev && eta_0 && eta_1 && eta_2 && alpha_0 && alpha_1 &&
+                     alpha_2 && beta && energy,
+                 "engine_set_drift: null pointer");
+    BB_CHECK_ARG(e->rf_set, "engine_set_drift: call set_rf first (it fixes n_turns)");
+    const int64_t nt = e->n_turns + 1;
+    std::vector<DriftTurn> h((size_t)nt);
+    e->h_t_rev.assign(t_rev, t_rev + nt);
+    for (int64_t i = 0; i < nt; ++i) {
+        // drift.cpp:31-56, evaluated once per turn on the host
+        DriftTurn d = {};
+        d.Tr = t_rev[i] * length_ratio;
+        d.simple = d.Tr * eta_0[i] / (beta[i] * beta[i] * energy[i]);
+        const double coeff = 1. / (beta[i] * beta[i] * energy[i]);
+        d.e0 = eta_0[i] * coeff;
+        d.e1 = eta_1[i] * coeff * coeff;
+        d.e2 = eta_2[i] * coeff * coeff * coeff;
+        d.ib2 = 1 / (beta[i] * beta[i]);
+        d.ie2 = 1 / (energy[i] * energy[i]);
+        d.energy = energy[i];
+        d.a0 = alpha_0[i];
+        d.a1 = alpha_1[i];
+        d.a2 = alpha_2[i];
+        h[(size_t)i] = d;
+    }
+    e->order = alpha_order == 0 ? 0 : (alpha_order == 1 ? 1 : 2);
+    int rc = upload((void**)&e->d_drift, h.data(), sizeof(DriftTurn) * (size_t)nt);
+    if (rc) return rc;
+    e->drift_set = true;
+    e->graph_dirty = true;
+    return BLOND_OK;
+}
+
+int blond_engine_set_slicing(blond_engine* e, double cut_left, double cut_right,
+                             const double* bc) {
+    BB_CHECK_ARG(e && bc, "engine_set_slicing: null pointer");
+    BB_CHECK_ARG(cut_right > cut_left, "engine_set_slicing: cut_right <= cut_left");
+    const int S = e->S;
+    e->cut_left = cut_left;
+    e->cut_right = cut_right;
+    e->inv_w = S / (cut_right - cut_left);  // histogram.cpp:30
+    e->bc0 = bc[0];
+    e->lik_inv_w = (S - 1) / (bc[S - 1] - bc[0]);  // linear_interp_kick.cpp:31-33
+    e->bw = 1.0 / e->lik_inv_w;
+    e->dbc = bc[1] - bc[0];
+    int rc = upload((void**)&e->d_bc, bc, sizeof(double) * S);
+    if (rc) return rc;
+    e->slicing_set = true;
+    e->graph_dirty = true;
+    return BLOND_OK;
+}
+
+int blond_engine_set_impedance(blond_engine* e, int64_t n_fft, const double* Z,
+                               double scale) {
+    BB_CHECK_ARG(e && Z, "engine_set_impedance: null pointer");
+    SpecPlan plan;
+    if (!make_spec_plan(n_fft, plan)) {
+        set_error("engine_set_impedance: n_fft=%lld must be even, 5-smooth and <= %lld",
+                  (long long)n_fft, (long long)kMaxClusterFFT);
+        return BLOND_ERR_UNSUPPORTED;
+    }
+    BB_CHECK_SIZE(plan.smem <= device_info().max_smem_optin,
+                  "engine_set_impedance: n_fft=%lld needs too much shared memory",
+                  (long long)n_fft);
+    int rc = upload((void**)&e->d_H, Z, sizeof(double2) * (size_t)(n_fft / 2 + 1));
+    if (rc) return rc;
+    e->plan = plan;
+    e->iv_scale = scale;
+    e->has_fft = true;
+    e->graph_dirty = true;
+    return BLOND_OK;
+}
+
+int blond_engine_set_inductive(blond_engine* e, const double* z_over_n, double scale) {
+    BB_CHECK_ARG(e && z_over_n, "engine_set_inductive: null pointer");
+    BB_CHECK_ARG(e->drift_set && e->slicing_set,
+                 "engine_set_inductive: call set_drift and set_slicing first");
+    // impedance.py:996-1005: -(q e / 2pi) ratio Z/n[t] t_rev[t] / bin_size * grad
+    const double bin_size = (e->cut_right - e->cut_left) / e->S;
+    std::vector<double> coeff((size_t)e->n_turns + 1);
+    for (size_t i = 0; i < coeff.size(); ++i)
+        coeff[i] = -(scale * z_over_n[i] * e->h_t_rev[i] / bin_size);
+    int rc = upload((void**)&e->d_ind, coeff.data(), sizeof(double) * coeff.size());
+    if (rc) return rc;
+    e->has_ind = true;
+    e->graph_dirty = true;
+    return BLOND_OK;
+}
+
+int blond_engine_bind_beam(blond_engine* e, void* dt, void* dE, int64_t n) {
+    BB_CHECK_ARG(e && dt && dE, "engine_bind_beam: null pointer");
+    BB_CHECK_ARG(n >= 1, "engine_bind_beam: n must be >= 1");
+    BB_CHECK_ARG(aligned(dt, 16), "engine_bind_beam: dt must be 16-byte aligned");
+    BB_CHECK_ARG(aligned(dE, e->precision == BLOND_PREC_F64 ? 16 : 8),
+                 "engine_bind_beam: dE must be %d-byte aligned",
+                 e->precision == BLOND_PREC_F64 ? 16 : 8);
+    e->dt = dt;
+    e->dE = dE;
+    e->n = n;
+    e->graph_dirty = true;
+    return BLOND_OK;
+}
+
+int blond_engine_set_turn(blond_engine* e, int64_t turn, void* stream) {
+    BB_CHECK_ARG(e && turn >= 0, "engine_set_turn: bad argument");
+    const long long t = turn;
+    BB_CUDA(cudaMemcpyAsync(e->d_turn, &t, sizeof(t), cudaMemcpyHostToDevice,
+                            as_stream(stream)));
+    BB_CUDA(cudaStreamSynchronize(as_stream(stream)));
+    e->host_turn = turn;
+    return BLOND_OK;
+}
+
+int blond_engine_slice(blond_engine* e, void* stream) {
+    BB_CHECK_ARG(e, "engine_slice: null engine");
+    if (!e->dt || !e->slicing_set) {
+        set_error("engine_slice: bind_beam and set_slicing first");
+        return BLOND_ERR_STATE;
+    }
+    cudaStream_t s = as_stream(stream);
+    BB_CUDA(cudaMemsetAsync(e->d_hist, 0, sizeof(int) * e->S, s));
+    int rc = launch_particles(e, false, s);
+    if (rc) return rc;
+    return launch_profile(e, false, s);
+}
+
+int blond_engine_tune(blond_engine* e, int threads, int blocks_per_sm, int turns_per_graph) {
+    BB_CHECK_ARG(e, "engine_tune: null engine");
+    if (threads) {
+        BB_CHECK_ARG(threads % 64 == 0 && threads <= kEngineThreads,
+                     "engine_tune: threads must be a multiple of 64 <= %d", kEngineThreads);
+        e->threads = threads;
+    }
+    if (blocks_per_sm) e->blocks_per_sm = blocks_per_sm;
+    if (turns_per_graph) e->turns_per_graph = turns_per_graph;
+    e->graph_dirty = true;
+    return BLOND_OK;
+}
+
+int blond_engine_run(blond_engine* e, int64_t n_turns, void* stream) {
+    BB_CHECK_ARG(e && n_turns >= 0, "engine_run: bad argument");
+    int rc = check_ready(e);
+    if (rc) return rc;
+    BB_CHECK_SIZE(e->host_turn + n_turns <= e->n_turns,
+                  "engine_run: turns %lld..%lld exceed the programme (%lld turns)",
+                  (long long)e->host_turn, (long long)(e->host_turn + n_turns),
+                  (long long)e->n_turns);
+    if (n_turns == 0) return BLOND_OK;
+    cudaStream_t s = as_stream(stream);
+    const int K = e->turns_per_graph;
+    int64_t done = 0;
+    if (n_turns >= K && K > 1) {
+        if (e->graph_dirty || e->graph_turns != K) {
+            // kernel attributes are set here, never inside the capture
+            if ((rc = launch_particles(e, true, s, false))) return rc;
+            if (e->has_fft && (rc = prepare_spectral())) return rc;
+            if (e->graph) cudaGraphExecDestroy(e->graph);
+            e->graph = nullptr;
+            cudaGraph_t g;
+            BB_CUDA(cudaStreamBeginCapture(e->cap_stream, cudaStreamCaptureModeThreadLocal));
+            int lrc = BLOND_OK;
+            for (int i = 0; i < K && lrc == BLOND_OK; ++i) lrc = launch_turn(e, e->cap_stream);
+            cudaError_t ce = cudaStreamEndCapture(e->cap_stream, &g);
+            if (lrc) return lrc;
+            if (ce != cudaSuccess) {
+                set_error("engine_run: graph capture failed: %s", cudaGetErrorString(ce));
+                return BLOND_ERR_CUDA;
+            }
+            ce = cudaGraphInstantiate(&e->graph, g, 0);
+            cudaGraphDestroy(g);
+            if (ce != cudaSuccess) {
+                set_error("engine_run: graph instantiation failed: %s", cudaGetErrorString(ce));
+                return BLOND_ERR_CUDA;
+            }
+            e->graph_turns = K;
+            e->graph_dirty = false;
+        }
+        for (; done + K <= n_turns; done += K) BB_CUDA(cudaGraphLaunch(e->graph, s));
+    }
+    for (; done < n_turns; ++done) {
+        rc = launch_turn(e, s);
+        if (rc) return rc;
+    }
+    e->host_turn += n_turns;
+    // the profile of the final coordinates (the histogram stays for the
+    // next turn's head)
+    return launch_profile(e, false, s);
+}
+
+int blond_engine_time_kernels(blond_engine* e, int64_t n_turns, double* head_ms,
+                              double* particles_ms, void* stream) {
+    BB_CHECK_ARG(e && head_ms && particles_ms && n_turns >= 1,
+                 "engine_time_kernels: bad argument");
+    int rc = check_ready(e);
+    if (rc) return rc;
+    BB_CHECK_SIZE(e->host_turn + n_turns <= e->n_turns,
+                  "engine_time_kernels: turns exceed the programme");
+    cudaStream_t s = as_stream(stream);
+    std::vector<cudaEvent_t> ev((size_t)(2 * n_turns + 1));
+    for (auto& x : ev) BB_CUDA(cudaEventCreate(&x));
+    rc = BLOND_OK;
+    cudaEventRecord(ev[0], s);
+    for (int64_t i = 0; i < n_turns && rc == BLOND_OK; ++i) {
+        rc = launch_head(e, s);
+        cudaEventRecord(ev[(size_t)(2 * i + 1)], s);
+        if (rc == BLOND_OK) rc = launch_particles(e, true, s);
+        cudaEventRecord(ev[(size_t)(2 * i + 2)], s);
+    }
+    cudaError_t ce = cudaEventSynchronize(ev.back());
+    double h = 0, p = 0;
+    for (int64_t i = 0; i < n_turns && ce == cudaSuccess; ++i) {
+        float a = 0, b = 0;
+        cudaEventElapsedTime(&a, ev[(size_t)(2 * i)], ev[(size_t)(2 * i + 1)]);
+        cudaEventElapsedTime(&b, ev[(size_t)(2 * i + 1)], ev[(size_t)(2 * i + 2)]);
+        h += a;
+        p += b;
+    }
+    for (auto& x : ev) cudaEventDestroy(x);
+    if (rc) return rc;
+    if (ce != cudaSuccess) {
+        set_error("engine_time_kernels: %s", cudaGetErrorString(ce));
+        return BLOND_ERR_CUDA;
+    }
+    e->host_turn += n_turns;
+    *head_ms = h;
+    *particles_ms = p;
+    return launch_profile(e, false, s);
+}
+
+int blond_engine_get_profile(blond_engine* e, double* out, void* stream) {
+    BB_CHECK_ARG(e && out, "engine_get_profile: null pointer");
+    BB_CUDA(cudaMemcpyAsync(out, e->d_profile, sizeof(double) * e->S,
+                            cudaMemcpyDeviceToDevice, as_stream(stream)));
+    return BLOND_OK;
+}
+
+int blond_engine_get_induced_voltage(blond_engine* e, double* out, void* stream) {
+    BB_CHECK_ARG(e && out, "engine_get_induced_voltage: null pointer");
+    BB_CUDA(cudaMemcpyAsync(out, e->d_vind, sizeof(double) * e->S,
+                            cudaMemcpyDeviceToDevice, as_stream(stream)));
+    return BLOND_OK;
+}
+
+int blond_engine_get_turn(blond_engine* e, int64_t* turn) {
+    BB_CHECK_ARG(e && turn, "engine_get_turn: null pointer");
+    *turn = e->host_turn;
+    return BLOND_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,262 @@
+// Host side of the cluster FFT (plan, launch) and the C ABI for rfft,
+// irfft and the one-turn induced voltage; plus a direct-DFT path for the
+// lengths the cluster transform does not take (odd, or prime factors > 5).
+#define BB_SPECTRAL_KERNELS
+#include "spectral.cuh"
+
+#include <vector>
+
+namespace bb {
+
+static void radix_schedule(int L, int* r, int& n) {
+    n = 0;
+    while (L % 4 == 0) { r[n++] = 4; L /= 4; }
+    while (L % 2 == 0) { r[n++] = 2; L /= 2; }
+    while (L % 3 == 0) { r[n++] = 3; L /= 3; }
+    while (L % 5 == 0) { r[n++] = 5; L /= 5; }
+}
+
+static bool smooth5(int64_t x) {
+    if (x < 1) return false;
+    for (int f : {2, 3, 5})
+        while (x % f == 0) x /= f;
+    return x == 1;
+}
+
+bool make_spec_plan(int64_t N, SpecPlan& plan) {
+    if (N < 2 || (N & 1) || N > kMaxClusterFFT) return false;
+    const int M = (int)(N / 2);
+    if (!smooth5(M)) return false;
+    // Pick M1 | M (M1 <= M2) maximising the cluster size C (a power of two
+    // dividing both factors, with at least 64 points per CTA), then the
+    // most square split.
+    int best_m1 = 1, best_c = 1;
+    double best_score = -1.0;
+    for (int m1 = 1; (int64_t)m1 * m1 <= M; ++m1) {
+        if (M % m1) continue;
+        const int m2 = M / m1;
+        int cc = 1;
+        while (cc * 2 <= kMaxCluster && m1 % (cc * 2) == 0 && m2 % (cc * 2) == 0 &&
+               M / (cc * 2) >= 64)
+            cc *= 2;
+        const double score = cc * 1e6 + (double)m1 / (double)m2;
+        if (score > best_score) {
+            best_score = score;
+            best_m1 = m1;
+            best_c = cc;
+        }
+    }
+    plan.N = (int)N;
+    plan.M = M;
+    plan.M1 = best_m1;
+    plan.M2 = M / best_m1;
+    plan.C = best_c;
+    plan.Bc = plan.M2 / plan.C;
+    plan.Br = plan.M1 / plan.C;
+    radix_schedule(plan.M1, plan.r1, plan.n1);
+    radix_schedule(plan.M2, plan.r2, plan.n2);
+    plan.smem = (int)sizeof(double2) * (2 * (M / plan.C) + plan.M1 + plan.M2);
+    return true;
+}
+
+int prepare_spectral() {
+    static bool attr_done[64] = {false};
+    const DeviceInfo& d = device_info();
+    if (!attr_done[d.device & 63]) {
+        BB_CUDA(cudaFuncSetAttribute(spectral_kernel,
+                                     cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        BB_CUDA(cudaFuncSetAttribute(spectral_kernel,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     d.max_smem_optin));
+        attr_done[d.device & 63] = true;
+    }
+    return BLOND_OK;
+}
+
+int launch_spectral(const SpecParams& P, cudaStream_t stream) {
+    const DeviceInfo& d = device_info();
+    if (P.p.smem > d.max_smem_optin) {
+        set_error("spectral: %d B of shared memory per CTA exceeds %d", P.p.smem,
+                  d.max_smem_optin);
+        return BLOND_ERR_SIZE;
+    }
+    int rc = prepare_spectral();
+    if (rc) return rc;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(P.p.C, 1, 1);
+    cfg.blockDim = dim3(kSpecThreads, 1, 1);
+    cfg.dynamicSmemBytes = P.p.smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = P.p.C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    BB_CUDA(cudaLaunchKernelEx(&cfg, spectral_kernel, P));
+    return BLOND_OK;
+}
+
+// ---------------------------------------------------------------- direct DFT
+// Single-CTA O(N^2) transforms for short lengths the cluster plan rejects.
+// Twiddles are indexed (k n mod N) from a shared table.
+constexpr int kDirectThreads = 512;
+
+__global__ void __launch_bounds__(kDirectThreads)
+direct_rfft_kernel(const double* __restrict__ x, int64_t n_x, int N,
+                   double2* __restrict__ out, const double2* __restrict__ H,
+                   double2* __restrict__ keep_spectrum) {
+    extern __shared__ double2 tw[];
+    for (int q = threadIdx.x; q < N; q += blockDim.x) tw[q] = twiddle<false>(q, N);
+    __syncthreads();
+    const int nk = N / 2 + 1;
+    const int nx = (int)(n_x < N ? n_x : N);
+    for (int k = threadIdx.x; k < nk; k += blockDim.x) {
+        double re = 0.0, im = 0.0;
+        int e = 0;
+        for (int n = 0; n < nx; ++n) {
+            const double2 w = tw[e];
+            re += x[n] * w.x;
+            im += x[n] * w.y;
+            e += k;
+            if (e >= N) e -= N;
+        }
+        double2 X = make_double2(re, im);
+        if (keep_spectrum) keep_spectrum[k] = X;
+        if (H) X = cmul(X, H[k]);
+        out[k] = X;
+    }
+}
+
+// irfft of length N from spectrum Y[0..n_y-1] (missing entries are zero,
+// imaginary parts of Y[0] and Y[N/2] ignored), y[n] = scale * (...).
+__global__ void __launch_bounds__(kDirectThreads)
+direct_irfft_kernel(const double2* __restrict__ Y, int64_t n_y, int N,
+                    double* __restrict__ y, int64_t n_out, double scale) {
+    extern __shared__ double2 tw[];
+    for (int q = threadIdx.x; q < N; q += blockDim.x) tw[q] = twiddle<true>(q, N);
+    __syncthreads();
+    const int half = N / 2;
+    const int kmax = (int)((int64_t)(N - 1) / 2 < n_y - 1 ? (N - 1) / 2 : n_y - 1);
+    for (int n = threadIdx.x; n < n_out && n < N; n += blockDim.x) {
+        double acc = n_y > 0 ? Y[0].x : 0.0;
+        int e = n;
+        for (int k = 1; k <= kmax; ++k) {
+            const double2 w = tw[e];
+            acc += 2.0 * (Y[k].x * w.x - Y[k].y * w.y);
+            e += n;
+            if (e >= N) e -= N;
+        }
+        if ((N & 1) == 0 && half < n_y) acc += Y[half].x * ((n & 1) ? -1.0 : 1.0);
+        y[n] = acc * scale;
+    }
+}
+
+static int direct_smem(int N) { return (int)sizeof(double2) * N; }
+
+static int set_direct_attrs() {
+    static bool done[64] = {false};
+    const DeviceInfo& d = device_info();
+    if (!done[d.device & 63]) {
+        BB_CUDA(cudaFuncSetAttribute(direct_rfft_kernel,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     direct_smem((int)kMaxDirectDFT)));
+        BB_CUDA(cudaFuncSetAttribute(direct_irfft_kernel,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     direct_smem((int)kMaxDirectDFT)));
+        done[d.device & 63] = true;
+    }
+    return BLOND_OK;
+}
+
+}  // namespace bb
+
+using namespace bb;
+
+extern "C" {
+
+int blond_rfft_f64(const double* x, int64_t n_x, int64_t n_fft, double* spectrum,
+                   void* stream) {
+    BB_CHECK_ARG(n_x >= 0 && n_fft >= 1, "rfft: bad length (n_x=%lld, n_fft=%lld)",
+                 (long long)n_x, (long long)n_fft);
+    BB_CHECK_ARG(spectrum && (n_x == 0 || x), "rfft: null pointer");
+    cudaStream_t s = as_stream(stream);
+    SpecParams P = {};
+    if (make_spec_plan(n_fft, P.p)) {
+        P.mode = SPEC_FORWARD | SPEC_OUT_SPECTRUM;
+        P.in_f64 = x;
+        P.n_in = n_x;
+        P.spec_out = reinterpret_cast<double2*>(spectrum);
+        return launch_spectral(P, s);
+    }
+    if (n_fft > kMaxDirectDFT) {
+        set_error("rfft: n_fft=%lld is neither an even 5-smooth length <= %lld nor "
+                  "<= %lld", (long long)n_fft, (long long)kMaxClusterFFT,
+                  (long long)kMaxDirectDFT);
+        return BLOND_ERR_UNSUPPORTED;
+    }
+    int rc = set_direct_attrs();
+    if (rc) return rc;
+    direct_rfft_kernel<<<1, kDirectThreads, direct_smem((int)n_fft), s>>>(
+        x, n_x, (int)n_fft, reinterpret_cast<double2*>(spectrum), nullptr, nullptr);
+    BB_LAUNCH_CHECK();
+    return BLOND_OK;
+}
+
+int blond_irfft_f64(const double* spectrum, int64_t n_fft, double* y,
+                    int64_t n_out, void* stream) {
+    BB_CHECK_ARG(n_fft >= 1 && n_out >= 0, "irfft: bad length");
+    BB_CHECK_ARG(spectrum && (n_out == 0 || y), "irfft: null pointer");
+    if (n_out > n_fft) n_out = n_fft;
+    cudaStream_t s = as_stream(stream);
+    SpecParams P = {};
+    if (make_spec_plan(n_fft, P.p)) {
+        P.mode = SPEC_IN_SPECTRUM | SPEC_INVERSE;
+        P.spec_in = reinterpret_cast<const double2*>(spectrum);
+        P.n_spec_in = n_fft / 2 + 1;
+        P.out = y;
+        P.n_out = n_out;
+        P.out_scale = 1.0 / (double)P.p.M;
+        return launch_spectral(P, s);
+    }
+    if (n_fft > kMaxDirectDFT) {
+        set_error("irfft: n_fft=%lld unsupported", (long long)n_fft);
+        return BLOND_ERR_UNSUPPORTED;
+    }
+    int rc = set_direct_attrs();
+    if (rc) return rc;
+    direct_irfft_kernel<<<1, kDirectThreads, direct_smem((int)n_fft), s>>>(
+        reinterpret_cast<const double2*>(spectrum), n_fft / 2 + 1, (int)n_fft, y, n_out,
+        1.0 / (double)n_fft);
+    BB_LAUNCH_CHECK();
+    return BLOND_OK;
+}
+
+int blond_induced_voltage_f64(const double* profile, int n_slices,
+                              const double* impedance, int64_t n_fft,
+                              double scale, double* v_out, int64_t n_out,
+                              void* stream) {
+    BB_CHECK_ARG(n_slices >= 1 && n_fft >= 1 && n_out >= 0,
+                 "induced_voltage: bad length");
+    BB_CHECK_ARG(profile && impedance && (n_out == 0 || v_out),
+                 "induced_voltage: null pointer");
+    cudaStream_t s = as_stream(stream);
+    SpecParams P = {};
+    if (make_spec_plan(n_fft, P.p)) {
+        P.mode = SPEC_FORWARD | SPEC_MULTIPLY | SPEC_INVERSE;
+        P.in_f64 = profile;
+        P.n_in = n_slices;
+        P.H = reinterpret_cast<const double2*>(impedance);
+        P.out = v_out;
+        P.n_out = n_out < n_fft ? n_out : n_fft;
+        P.out_scale = -scale / (double)P.p.M;
+        return launch_spectral(P, s);
+    }
+    set_error("induced_voltage: n_fft=%lld is not an even 5-smooth length <= %lld; "
+              "use blond_rfft_f64/blond_irfft_f64", (long long)n_fft,
+              (long long)kMaxClusterFFT);
+    return BLOND_ERR_UNSUPPORTED;
+}
+
+}  // extern "C"

@@ -1,0 +1,197 @@
+"""Fused turn loop: the reference main loop in two launches per turn.
+
+``FusedTracker`` takes the drop-in objects of one beam -- a
+``RingAndRFTracker``, its ``Profile`` and optionally a
+``TotalInducedVoltage`` -- and replaces
+
+    for turn in range(n):                 # EX_05_Wake_impedance.py:336-339
+        total_induced_voltage.track()     # impedance.py:133-146
+        tracker.track()                   # tracker.py:521-615
+        profile.track()                   # profile.py:700-719
+
+by ``FusedTracker(...).track(n)``: per turn one cluster launch (profile ->
+induced voltage -> interpolation table) and one pass over the particles
+(induced kick, RF kick, drift, deposit), replayed from a CUDA graph.
+
+Precision modes
+---------------
+'f64'    : dt, dE float64, everything float64 (the reference's arithmetic).
+'f32p64' : dt float64, dE float32; the RF phase argument omega*dt+phi and
+           the drift accumulate in float64, the kick in float32.  The
+           engine keeps its own float32 energy array (``dE``).
+"""
+from __future__ import annotations
+
+import ctypes as ct
+
+import numpy as np
+import torch
+from scipy.constants import e
+
+from . import _lib
+from .impedances.impedance import (InducedVoltageFreq, InducedVoltageTime,
+                                   InductiveImpedance)
+
+PREC = {"f64": 0, "f32p64": 1}
+SOLVER = {"simple": 0, "legacy": 1, "exact": 2}
+
+
+def _host(a) -> np.ndarray:
+    if isinstance(a, torch.Tensor):
+        return a.detach().cpu().numpy()
+    return np.asarray(a)
+
+
+def _p(a: np.ndarray) -> ct.c_void_p:
+    return a.ctypes.data_as(ct.c_void_p)
+
+
+class TurnEngine:
+    """Thin owner of a blond_engine handle (include/blond_b200.h)."""
+
+    def __init__(self, precision: str, n_rf: int, solver: str, n_slices: int):
+        _lib.load()
+        self.h = ct.c_void_p()
+        _lib.call("blond_engine_create", ct.byref(self.h), PREC[precision],
+                  int(n_rf), SOLVER[solver], int(n_slices))
+        self.n_slices = int(n_slices)
+        self._keep = []
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h is not None and h.value:
+            try:
+                _lib.load().blond_engine_destroy(h)
+            except Exception:
+                pass
+            self.h = None
+
+    def call(self, name, *args):
+        _lib.call(f"blond_engine_{name}", self.h, *args)
+
+
+def _stream():
+    return ct.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+class FusedTracker:
+    def __init__(self, tracker, profile, total_induced_voltage=None,
+                 precision: str = "f64", turns_per_graph: int = 50,
+                 threads: int = 0, blocks_per_sm: int = 0):
+        if precision not in PREC:
+            raise ValueError(f"precision must be one of {list(PREC)}")
+        if tracker.interpolation:
+            raise NotImplementedError("the fused engine tracks the "
+                                      "non-interpolated kick")
+        if getattr(profile, "smooth", False):
+            raise NotImplementedError("the fused engine deposits with slice_beam")
+        rf = tracker.rf_params
+        beam = tracker.beam
+        self.tracker, self.profile, self.tiv = tracker, profile, total_induced_voltage
+        self.rf, self.beam = rf, beam
+        self.precision = precision
+        S = int(profile.n_slices)
+        self.eng = TurnEngine(precision, rf.n_rf, tracker.solver, S)
+        nt = int(rf.n_turns)
+        # programmes, turn-major (column t of the F-ordered [n_rf, n_turns+1])
+        V = np.ascontiguousarray(np.asarray(rf.voltage, float).T)
+        om = np.ascontiguousarray(np.asarray(rf.omega_rf, float).T)
+        ph = np.ascontiguousarray(np.asarray(rf.phi_rf, float).T)
+        acc = np.ascontiguousarray(np.asarray(tracker.acceleration_kick, float))
+        self.eng.call("set_rf", nt, _p(V), _p(om), _p(ph), _p(acc),
+                      float(rf.particle.charge))
+        arr = [np.ascontiguousarray(np.asarray(getattr(rf, k), float))
+               for k in ("t_rev", "eta_0", "eta_1", "eta_2", "alpha_0",
+                         "alpha_1", "alpha_2", "beta", "energy")]
+        self.eng.call("set_drift", float(rf.length_ratio), float(rf.alpha_order),
+                      *[_p(a) for a in arr])
+        bc = np.ascontiguousarray(np.asarray(profile.bin_centers, float))
+        self.eng.call("set_slicing", float(profile.cut_left),
+                      float(profile.cut_right), _p(bc))
+        if total_induced_voltage is not None:
+            self._set_impedance(total_induced_voltage, beam, rf)
+        # coordinates
+        if beam.dt.dtype != torch.float64:
+            raise TypeError("the fused engine needs float64 dt")
+        self.dt = beam.dt
+        if precision == "f64":
+            if beam.dE.dtype != torch.float64:
+                raise TypeError("precision 'f64' needs float64 dE")
+            self.dE = beam.dE
+        else:
+            self.dE = beam.dE.to(torch.float32).contiguous()
+        self.eng.call("bind_beam", ct.c_void_p(self.dt.data_ptr()),
+                      ct.c_void_p(self.dE.data_ptr()), int(beam.n_macroparticles))
+        self.eng.call("tune", int(threads), int(blocks_per_sm), int(turns_per_graph))
+        self.eng.call("set_turn", int(rf.counter[0]), _stream())
+        self.eng.call("slice", _stream())
+
+    def _set_impedance(self, tiv, beam, rf):
+        Z = None
+        n_fft = None
+        for obj in tiv.induced_voltage_list:
+            if isinstance(obj, InductiveImpedance):
+                zn = np.ascontiguousarray(np.asarray(obj.Z_over_n, float))
+                scale = beam.particle.charge * e / (2 * np.pi) * beam.ratio
+                self._zn = zn
+                self._ind_scale = scale
+                continue
+            if not isinstance(obj, (InducedVoltageFreq, InducedVoltageTime)):
+                raise NotImplementedError(type(obj).__name__)
+            if n_fft is not None and obj.n_fft != n_fft:
+                raise NotImplementedError("contributions with different n_fft")
+            n_fft = obj.n_fft
+            zi = _host(obj.total_impedance).astype(np.complex128)
+            Z = zi if Z is None else Z + zi
+        if Z is None:
+            raise NotImplementedError("an inductive impedance alone needs an FFT "
+                                      "impedance in the fused engine")
+        if n_fft < self.profile.n_slices:
+            raise NotImplementedError("n_fft shorter than the profile")
+        self._Z = np.ascontiguousarray(Z)
+        self.eng.call("set_impedance", int(n_fft), _p(self._Z.view(np.float64)),
+                      float(beam.particle.charge * e * beam.ratio))
+        if hasattr(self, "_zn"):
+            self.eng.call("set_inductive", _p(self._zn), float(self._ind_scale))
+
+    def track(self, n_turns: int = 1):
+        """Advance n_turns; updates the RF counter and beam energy fields."""
+        self.eng.call("run", int(n_turns), _stream())
+        rf = self.rf
+        rf.counter[0] += int(n_turns)
+        t = rf.counter[0]
+        self.beam.beta = float(rf.beta[t])
+        self.beam.gamma = float(rf.gamma[t])
+        self.beam.energy = float(rf.energy[t])
+        self.beam.momentum = float(rf.momentum[t])
+
+    def time_kernels(self, n_turns: int):
+        """Track n_turns with CUDA events around each launch; returns the
+        summed (head_ms, particles_ms).  Synchronises the current stream."""
+        h, p = ct.c_double(), ct.c_double()
+        self.eng.call("time_kernels", int(n_turns), ct.byref(h), ct.byref(p), _stream())
+        self.rf.counter[0] += int(n_turns)
+        return h.value, p.value
+
+    def sync(self):
+        """Copy the engine's profile (and induced voltage) into the drop-in
+        objects, and the float32 energies back into beam.dE ('f32p64')."""
+        prof = torch.empty(self.profile.n_slices, dtype=torch.float64, device="cuda")
+        self.eng.call("get_profile", ct.c_void_p(prof.data_ptr()), _stream())
+        self.profile.n_macroparticles.copy_(prof)
+        if self.tiv is not None:
+            v = torch.empty_like(prof)
+            self.eng.call("get_induced_voltage", ct.c_void_p(v.data_ptr()), _stream())
+            self.tiv.induced_voltage = v.to(self.profile.n_macroparticles.dtype)
+        if self.precision == "f32p64":
+            self.beam.dE.copy_(self.dE)
+
+    def profile_tensor(self) -> torch.Tensor:
+        prof = torch.empty(self.profile.n_slices, dtype=torch.float64, device="cuda")
+        self.eng.call("get_profile", ct.c_void_p(prof.data_ptr()), _stream())
+        return prof
+
+    def induced_voltage_tensor(self) -> torch.Tensor:
+        v = torch.empty(self.profile.n_slices, dtype=torch.float64, device="cuda")
+        self.eng.call("get_induced_voltage", ct.c_void_p(v.data_ptr()), _stream())
+        return v

@@ -1,0 +1,1 @@
+"""Drop-in counterparts of the reference package of the same name."""

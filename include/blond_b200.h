@@ -1,0 +1,221 @@
+/*
+ * blond_b200 -- C ABI of the B200 longitudinal tracking engine.
+ *
+ * All array arguments are DEVICE pointers (CUDA global memory on the current
+ * device) unless a comment says "host".  Every call is asynchronous on the
+ * given stream (a cudaStream_t passed as void*, NULL = legacy default
+ * stream) and returns a status code; blond_b200_last_error() gives the
+ * message of the last failure on the calling thread.  Lengths are int64_t.
+ * Nothing here allocates memory visible to the caller; callers own every
+ * array they pass.
+ *
+ * The bmath-level entry points mirror the reference's libblond exports
+ * (blond/cpp_routines/*.cpp, bound by blond/utils/butils_wrap_cpp.py) with
+ * the same argument order and meaning; _f64 corresponds to
+ * libblond_double.so and _f32 to libblond_single.so (blond_common.h:22-36).
+ */
+#ifndef BLOND_B200_H
+#define BLOND_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------ status codes */
+#define BLOND_OK 0
+#define BLOND_ERR_INVALID_ARGUMENT 1 /* null pointer, negative length, bad enum */
+#define BLOND_ERR_SIZE 2             /* n_slices / n_fft / n_rf outside the supported range */
+#define BLOND_ERR_ALIGNMENT 3        /* pointer not aligned to its element size */
+#define BLOND_ERR_CUDA 4             /* CUDA runtime error (launch, allocation, graph) */
+#define BLOND_ERR_UNSUPPORTED 5      /* e.g. an FFT length with a prime factor > 5 */
+#define BLOND_ERR_TIMEOUT 6          /* a bounded device-side wait gave up */
+#define BLOND_ERR_STATE 7            /* engine used before it was configured */
+
+/* drift solvers, as butils_wrap_cpp.drift maps them (butils_wrap_cpp.py:920-925) */
+#define BLOND_SOLVER_SIMPLE 0
+#define BLOND_SOLVER_LEGACY 1
+#define BLOND_SOLVER_EXACT 2
+
+/* fused-engine precision modes */
+#define BLOND_PREC_F64 0    /* dt, dE float64; all arithmetic float64 (plain) */
+#define BLOND_PREC_F32P64 1 /* dt float64, dE float32; RF phase argument and
+                               drift in float64, kick arithmetic in float32 */
+
+const char* blond_b200_last_error(void);
+int blond_b200_version(void);
+/* Largest n_slices the shared-memory histogram privatises (bins beyond it
+ * fall back to global atomics); informational. */
+int blond_b200_max_smem_slices(void);
+
+/* ------------------------------------------------------------ RF kick
+ * replaces kick()          cpp_routines/kick.cpp:16-35
+ *   dE[i] += charge * sum_j voltage[j] sin(omega_rf[j] dt[i] + phi_rf[j]) + acc_kick
+ * voltage/omega_rf/phi_rf: n_rf device values (one turn column). */
+int blond_kick_f64(const double* dt, double* dE, int n_rf, double charge,
+                   const double* voltage, const double* omega_rf,
+                   const double* phi_rf, int64_t n, double acc_kick,
+                   void* stream);
+int blond_kick_f32(const float* dt, float* dE, int n_rf, float charge,
+                   const float* voltage, const float* omega_rf,
+                   const float* phi_rf, int64_t n, float acc_kick,
+                   void* stream);
+
+/* replaces rf_volt_comp()  cpp_routines/kick.cpp:37-51  (accumulates: +=) */
+int blond_rf_volt_comp_f64(const double* voltage, const double* omega_rf,
+                           const double* phi_rf, const double* bin_centers,
+                           int n_rf, int64_t n_bins, double* rf_voltage,
+                           void* stream);
+int blond_rf_volt_comp_f32(const float* voltage, const float* omega_rf,
+                           const float* phi_rf, const float* bin_centers,
+                           int n_rf, int64_t n_bins, float* rf_voltage,
+                           void* stream);
+
+/* ------------------------------------------------------------ drift
+ * replaces drift()         cpp_routines/drift.cpp:19-78 (solver 0/1/2) */
+int blond_drift_f64(double* dt, const double* dE, int solver, double t_rev,
+                    double length_ratio, double alpha_order, double eta_0,
+                    double eta_1, double eta_2, double alpha_0,
+                    double alpha_1, double alpha_2, double beta,
+                    double energy, int64_t n, void* stream);
+int blond_drift_f32(float* dt, const float* dE, int solver, float t_rev,
+                    float length_ratio, float alpha_order, float eta_0,
+                    float eta_1, float eta_2, float alpha_0, float alpha_1,
+                    float alpha_2, float beta, float energy, int64_t n,
+                    void* stream);
+
+/* ------------------------------------------------------------ slicing
+ * replaces histogram()        cpp_routines/histogram.cpp:22-73
+ * profile[n_slices] is OVERWRITTEN with the counts (exact integers). */
+int blond_histogram_f64(const double* dt, double* profile, double cut_left,
+                        double cut_right, int n_slices, int64_t n,
+                        void* stream);
+int blond_histogram_f32(const float* dt, float* profile, float cut_left,
+                        float cut_right, int n_slices, int64_t n,
+                        void* stream);
+/* replaces smooth_histogram() cpp_routines/histogram.cpp:75-132 (overwrites) */
+int blond_smooth_histogram_f64(const double* dt, double* profile,
+                               double cut_left, double cut_right,
+                               int n_slices, int64_t n, void* stream);
+int blond_smooth_histogram_f32(const float* dt, float* profile,
+                               float cut_left, float cut_right, int n_slices,
+                               int64_t n, void* stream);
+
+/* ------------------------------------------------------------ interpolated kick
+ * replaces linear_interp_kick() cpp_routines/linear_interp_kick.cpp:21-71 */
+int blond_linear_interp_kick_f64(const double* dt, double* dE,
+                                 const double* voltage,
+                                 const double* bin_centers, double charge,
+                                 int n_slices, int64_t n, double acc_kick,
+                                 void* stream);
+int blond_linear_interp_kick_f32(const float* dt, float* dE,
+                                 const float* voltage,
+                                 const float* bin_centers, float charge,
+                                 int n_slices, int64_t n, float acc_kick,
+                                 void* stream);
+
+/* ------------------------------------------------------------ impedance setup
+ * replaces fast_resonator_real_imag() cpp_routines/fast_resonator.cpp:19-74
+ * re/im accumulate (+= / -=); index 0 (DC) is untouched. */
+int blond_fast_resonator_f64(double* re, double* im, const double* freq,
+                             const double* R_S, const double* Q,
+                             const double* freq_R, int n_resonators,
+                             int64_t n_freq, void* stream);
+
+/* ------------------------------------------------------------ FFT
+ * numpy.fft.rfft(x, n_fft) / numpy.fft.irfft(X, n_fft) as used by
+ * bmath_backends.py:447-449 (Profile.beam_spectrum_generation,
+ * profile.py:899-903; _InducedVoltage.induced_voltage_1turn,
+ * impedance.py:475-485).  Complex arrays are interleaved (re, im) doubles.
+ * n_fft must be even, 2..131072, with no prime factor above 5 (every
+ * next_regular() result qualifies), or any length <= 4096 (direct DFT). */
+int blond_rfft_f64(const double* x, int64_t n_x, int64_t n_fft,
+                   double* spectrum, void* stream);
+int blond_irfft_f64(const double* spectrum, int64_t n_fft, double* y,
+                    int64_t n_out, void* stream);
+
+/* One-turn induced voltage from the FFT path (impedance.py:457-489 with the
+ * truncation of TotalInducedVoltage.induced_voltage_sum, impedance.py:113-131):
+ *   v_out[k] = -scale * irfft(impedance * rfft(profile, n_fft), n_fft)[k]
+ * for k < n_out, scale = charge * e * ratio; impedance holds n_fft/2+1
+ * complex values (already divided by bin_size, impedance.py:889). */
+int blond_induced_voltage_f64(const double* profile, int n_slices,
+                              const double* impedance, int64_t n_fft,
+                              double scale, double* v_out, int64_t n_out,
+                              void* stream);
+
+/* ------------------------------------------------------------ fused turn engine
+ * One object per beam.  A turn is, in the order of the reference main loop
+ * [TotalInducedVoltage, RingAndRFTracker, Profile]
+ * (__EXAMPLES/main_files/EX_05_Wake_impedance.py:318-339):
+ *   induced voltage from the current profile -> linear_interp_kick (acc 0)
+ *   -> RF kick (turn t) -> drift (turn t+1 parameters) -> slice_beam.
+ * It replaces RingAndRFTracker.track() (trackers/tracker.py:521-615),
+ * Profile.track() (beam/profile.py:700-719) and TotalInducedVoltage.track()
+ * (impedances/impedance.py:133-146) for one beam, as two kernels per turn
+ * replayed from a CUDA graph.  The turn counter lives on the device. */
+typedef struct blond_engine blond_engine;
+
+int blond_engine_create(blond_engine** engine, int precision, int n_rf,
+                        int solver, int n_slices);
+int blond_engine_destroy(blond_engine* engine);
+/* host arrays over turns; column t of the reference's F-ordered
+ * [n_rf, n_turns+1] programmes is voltage[t*n_rf .. t*n_rf+n_rf-1]
+ * (rf_parameters.py:317-328).  acc_kick has n_turns entries
+ * (= -RFStation.delta_E). */
+int blond_engine_set_rf(blond_engine* engine, int64_t n_turns,
+                        const double* voltage, const double* omega_rf,
+                        const double* phi_rf, const double* acc_kick,
+                        double charge);
+/* host arrays of n_turns+1 entries (Ring/RFStation per-turn values). */
+int blond_engine_set_drift(blond_engine* engine, double length_ratio,
+                           double alpha_order, const double* t_rev,
+                           const double* eta_0, const double* eta_1,
+                           const double* eta_2, const double* alpha_0,
+                           const double* alpha_1, const double* alpha_2,
+                           const double* beta, const double* energy);
+/* bin_centers: host, n_slices values exactly as Profile.bin_centers. */
+int blond_engine_set_slicing(blond_engine* engine, double cut_left,
+                             double cut_right, const double* bin_centers);
+/* FFT impedance (host, interleaved complex, n_fft/2+1 values, the sum of
+ * every InducedVoltageFreq/Time total_impedance with this n_fft);
+ * scale = charge * e * ratio. */
+int blond_engine_set_impedance(blond_engine* engine, int64_t n_fft,
+                               const double* impedance, double scale);
+/* InductiveImpedance (impedance.py:986-1009): host z_over_n[n_turns+1];
+ * scale = charge * e / (2 pi) * ratio; uses t_rev from set_drift. */
+int blond_engine_set_inductive(blond_engine* engine, const double* z_over_n,
+                               double scale);
+/* dt/dE: device arrays of n macro-particles in the engine's precision
+ * (F64: both double; F32P64: dt double, dE float). */
+int blond_engine_bind_beam(blond_engine* engine, void* dt, void* dE,
+                           int64_t n);
+int blond_engine_set_turn(blond_engine* engine, int64_t turn, void* stream);
+/* Re-slice the bound beam into the profile (Profile.track()). */
+int blond_engine_slice(blond_engine* engine, void* stream);
+/* Track n_turns fused turns; afterwards the profile holds the slices of the
+ * final coordinates. */
+int blond_engine_run(blond_engine* engine, int64_t n_turns, void* stream);
+/* Device copies of the current state (n_slices doubles each). */
+int blond_engine_get_profile(blond_engine* engine, double* profile,
+                             void* stream);
+int blond_engine_get_induced_voltage(blond_engine* engine, double* v,
+                                     void* stream);
+int blond_engine_get_turn(blond_engine* engine, int64_t* turn_host);
+/* Track n_turns like blond_engine_run but without a graph, bracketing each
+ * of the two launches of every turn with CUDA events on `stream`; returns
+ * the summed device durations of the head and particle kernels (ms) and
+ * synchronises the stream.  Measurement only. */
+int blond_engine_time_kernels(blond_engine* engine, int64_t n_turns,
+                              double* head_ms, double* particles_ms,
+                              void* stream);
+/* Grid size and block size of the particle kernel (0 = automatic). */
+int blond_engine_tune(blond_engine* engine, int threads, int blocks_per_sm,
+                      int turns_per_graph);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BLOND_B200_H */

@@ -1,0 +1,79 @@
+"""Host-side logic of the drop-in layer against the reference (no GPU)."""
+import numpy as np
+
+from conftest import golden, normwise
+from blond_b200.beam.beam import Proton
+from blond_b200.beam.distributions import _get_dE_from_dt, bigaussian_arrays
+from blond_b200.impedances.impedance import induced_voltage_lengths
+from blond_b200.input_parameters.rf_parameters import RFStation
+from blond_b200.input_parameters.ring import Ring
+from blond_b200.toolbox.next_regular import next_regular
+
+
+def test_next_regular_table():
+    g = golden("nfft_known.npz")
+    got = np.array([next_regular(int(t)) for t in g["next_regular_targets"]])
+    np.testing.assert_array_equal(got, g["next_regular_values"])
+
+
+def test_n_fft_known_answers():
+    """unittests/impedances/test_impedance.py:30-125 (16 slices over 5 ns)."""
+    g = golden("nfft_known.npz")
+    S, cl, cr = 16, 0.0, 5e-9
+    bs = (cr - cl) / S
+    n_iv, _ = induced_voltage_lengths(S, bs, cl, cr)
+    assert [next_regular(n_iv), n_iv] == list(g["freq_default"])
+    n_iv, _ = induced_voltage_lengths(S, bs, cl, cr, frequency_resolution=3e6)
+    assert [next_regular(n_iv), n_iv] == list(g["freq_res3e6"]) == [1080, 1067]
+    n_iv, _ = induced_voltage_lengths(S, bs, cl, cr)
+    assert [next_regular(n_iv + S - 1), n_iv] == list(g["time_default"])
+    n_iv, _ = induced_voltage_lengths(S, bs, cl, cr, wake_length=11e-9)
+    assert [next_regular(n_iv + S - 1), n_iv] == list(g["time_wake11ns"])
+
+
+def test_ring_and_rfstation_match_reference():
+    g = golden("machine_c1.npz")
+    ring = Ring(6911.5, 1 / 18**2, 26e9, Proton(), 1000)
+    rf = RFStation(ring, [4620], [4.5e6], [0.0])
+    for k in ("beta", "gamma", "energy", "momentum", "eta_0", "eta_1", "eta_2"):
+        np.testing.assert_allclose(getattr(ring, k)[0, :3], g[k], rtol=1e-15, atol=0)
+    np.testing.assert_allclose(ring.t_rev[:3], g["t_rev"], rtol=1e-15)
+    np.testing.assert_allclose(rf.omega_rf[:, :3], g["omega_rf"], rtol=1e-15)
+    np.testing.assert_allclose(rf.phi_s[:3], g["phi_s"], rtol=1e-15)
+    np.testing.assert_allclose(rf.Q_s[:3], g["Q_s"], rtol=1e-14)
+    np.testing.assert_allclose(rf.t_rf[:, :3], g["t_rf"], rtol=1e-15)
+    rf2 = RFStation(Ring(6911.5, 1 / 18**2, 26e9, Proton(), 100),
+                    [4620, 4 * 4620], [4.5e6, 0.45e6], [0.0, np.pi], n_rf=2)
+    np.testing.assert_allclose(rf2.omega_rf[:, :3], g["omega_rf_2"], rtol=1e-15)
+
+
+def test_bigaussian_streams_match_reference():
+    g = golden("machine_c1.npz")
+    ring = Ring(6911.5, 1 / 18**2, 26e9, Proton(), 1000)
+    rf = RFStation(ring, [4620], [4.5e6], [0.0])
+    sigma_dE = _get_dE_from_dt(ring, rf, 0.4e-9)
+    assert np.isclose(sigma_dE, g["sigma_dE"][0], rtol=1e-15)
+    centre = (rf.phi_s[0] - rf.phi_rf[0, 0]) / rf.omega_rf[0, 0]
+    dt, dE = bigaussian_arrays(len(g["dt"]), 0.4e-9, sigma_dE, centre, 0)
+    np.testing.assert_array_equal(dt, g["dt"])
+    np.testing.assert_array_equal(dE, g["dE"])
+
+
+def test_spectral_plan_factorisation_covers_next_regular_lengths():
+    """Every even n_fft that next_regular can return up to 2^17 has M = n/2
+    5-smooth, so the cluster transform takes it without the DFT path."""
+    for t in range(7, 131073, 97):
+        n = next_regular(t)
+        if n > 131072:
+            continue
+        assert n % 2 == 0
+        m = n // 2
+        for f in (2, 3, 5):
+            while m % f == 0:
+                m //= f
+        assert m == 1, n
+
+
+def test_normwise_helper():
+    assert normwise([1.0, 2.0], [1.0, 2.0]) == 0.0
+    assert np.isclose(normwise([1.0, 2.2], [1.0, 2.0]), 0.1)
