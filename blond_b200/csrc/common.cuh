@@ -100,5 +100,48 @@ __device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(
 __device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
 __device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double div_rn(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ float div_rn(float a, float b) { return __fdiv_rn(a, b); }
+
+// ------------------------------------------------------------ drift solvers
+// drift.cpp:29-76.  The expressions of the 'legacy' and 'exact' solvers
+// cancel (1/(1-x)-1 with x ~ 1e-6), so they are evaluated operation by
+// operation without FMA contraction, in the reference's order and with its
+// C promotion rules: the constants are double literals (1., 2.), so in the
+// float build the marked sub-expressions run in double and are rounded to
+// the element type only where the reference assigns them.  This makes the
+// result bit-identical to the reference compiled without -ffast-math.
+template <typename T>
+__device__ __forceinline__ T drift_simple(T dt, T d, T coeff) {
+    return add_rn(dt, mul_rn(coeff, d));
+}
+
+template <typename T>
+__device__ __forceinline__ T drift_legacy(T dt, T d, T Tr, T e0, T e1, T e2, int order) {
+    double den = __dsub_rn(1.0, (double)mul_rn(e0, d));
+    if (order >= 1) den = __dsub_rn(den, (double)mul_rn(mul_rn(e1, d), d));
+    if (order >= 2) den = __dsub_rn(den, (double)mul_rn(mul_rn(mul_rn(e2, d), d), d));
+    const double inc = __dmul_rn((double)Tr, __dsub_rn(__ddiv_rn(1.0, den), 1.0));
+    return (T)__dadd_rn((double)dt, inc);
+}
+
+template <typename T>
+__device__ __forceinline__ T drift_exact(T dt, T d, T Tr, T ib2, T ie2, T a0, T a1,
+                                         T a2, T energy) {
+    const double inner = __dadd_rn((double)mul_rn(mul_rn(d, d), ie2),
+                                   __ddiv_rn(__dmul_rn(2.0, (double)d), (double)energy));
+    const T delta = (T)__dsub_rn(__dsqrt_rn(__dadd_rn(1.0, __dmul_rn((double)ib2, inner))),
+                                 1.0);
+    double num = __dadd_rn(1.0, (double)mul_rn(a0, delta));
+    num = __dadd_rn(num, (double)mul_rn(a1, mul_rn(delta, delta)));
+    num = __dadd_rn(num, (double)mul_rn(a2, mul_rn(mul_rn(delta, delta), delta)));
+    const double f = __dsub_rn(
+        __ddiv_rn(__dmul_rn(num, __dadd_rn(1.0, (double)div_rn(d, energy))),
+                  __dadd_rn(1.0, (double)delta)),
+        1.0);
+    return (T)__dadd_rn((double)dt, __dmul_rn((double)Tr, f));
+}
 
 }  // namespace bb

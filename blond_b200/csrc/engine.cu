@@ -108,23 +108,14 @@ __device__ __forceinline__ void track_one(double& t,
                 s += c.Vf[j] * sinf((float)reduce_2pi(fma(c.om[j], t, c.ph[j])));
             e += (float)a.charge * s + (float)c.acc;
         }
-        if (SOLVER == BLOND_SOLVER_SIMPLE) {
-            t += c.d.simple * (double)e;
-        } else if (SOLVER == BLOND_SOLVER_LEGACY) {
-            const double d = (double)e;
-            double den;
-            if (order == 0) den = 1.0 - c.d.e0 * d;
-            else if (order == 1) den = 1.0 - c.d.e0 * d - c.d.e1 * d * d;
-            else den = 1.0 - c.d.e0 * d - c.d.e1 * d * d - c.d.e2 * d * d * d;
-            t += c.d.Tr * (1.0 / den - 1.0);
-        } else {
-            const double d = (double)e, en = c.d.energy;
-            const double delta = sqrt(1.0 + c.d.ib2 * (d * d * c.d.ie2 + 2.0 * d / en)) - 1.0;
-            t += c.d.Tr * ((1.0 + c.d.a0 * delta + c.d.a1 * (delta * delta) +
-                            c.d.a2 * (delta * delta * delta)) *
-                               (1.0 + d / en) / (1.0 + delta) -
-                           1.0);
-        }
+        // dt accumulates in float64 in both precision modes
+        if (SOLVER == BLOND_SOLVER_SIMPLE)
+            t = drift_simple<double>(t, (double)e, c.d.simple);
+        else if (SOLVER == BLOND_SOLVER_LEGACY)
+            t = drift_legacy<double>(t, (double)e, c.d.Tr, c.d.e0, c.d.e1, c.d.e2, order);
+        else
+            t = drift_exact<double>(t, (double)e, c.d.Tr, c.d.ib2, c.d.ie2, c.d.a0, c.d.a1,
+                                    c.d.a2, c.d.energy);
     }
     (void)sh;
 }
@@ -296,8 +287,11 @@ template <typename K>
 static int allow_max_smem(K kernel, bool* done) {
     const DeviceInfo& d = device_info();
     if (!done[d.device & 63]) {
+        // the opt-in limit covers static + dynamic shared memory
+        cudaFuncAttributes fa;
+        BB_CUDA(cudaFuncGetAttributes(&fa, kernel));
         BB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     d.max_smem_optin));
+                                     d.max_smem_optin - (int)fa.sharedSizeBytes));
         done[d.device & 63] = true;
     }
     return BLOND_OK;

@@ -148,21 +148,12 @@ drift_kernel(T* __restrict__ dt, const T* __restrict__ dE, int64_t n,
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += stride) {
         const T d = dE[i];
-        if (SOLVER == BLOND_SOLVER_SIMPLE) {
-            dt[i] += c_simple * d;
-        } else if (SOLVER == BLOND_SOLVER_LEGACY) {
-            T den;
-            if (order == 0) den = T(1) - e0 * d;
-            else if (order == 1) den = T(1) - e0 * d - e1 * d * d;
-            else den = T(1) - e0 * d - e1 * d * d - e2 * d * d * d;
-            dt[i] += Tr * (T(1) / den - T(1));
-        } else {
-            const T delta = dev_sqrt(T(1) + ib2 * (d * d * ie2 + T(2) * d / energy)) - T(1);
-            dt[i] += Tr * ((T(1) + a0 * delta + a1 * (delta * delta) +
-                            a2 * (delta * delta * delta)) *
-                               (T(1) + d / energy) / (T(1) + delta) -
-                           T(1));
-        }
+        if (SOLVER == BLOND_SOLVER_SIMPLE)
+            dt[i] = drift_simple<T>(dt[i], d, c_simple);
+        else if (SOLVER == BLOND_SOLVER_LEGACY)
+            dt[i] = drift_legacy<T>(dt[i], d, Tr, e0, e1, e2, order);
+        else
+            dt[i] = drift_exact<T>(dt[i], d, Tr, ib2, ie2, a0, a1, a2, energy);
     }
 }
 
@@ -180,7 +171,8 @@ static int drift_impl(T* dt, const T* dE, int solver, T t_rev, T length_ratio,
     // order (drift.cpp:33-56).
     const T Tr = t_rev * length_ratio;
     const T c_simple = Tr * eta_0 / (beta * beta * energy);
-    const T coeff = T(1) / (beta * beta * energy);
+    // `1. / (...)` in the reference: a double division rounded to T
+    const T coeff = (T)(1.0 / (double)(beta * beta * energy));
     const T e0 = eta_0 * coeff, e1 = eta_1 * coeff * coeff,
             e2 = eta_2 * coeff * coeff * coeff;
     const T ib2 = T(1) / (beta * beta), ie2 = T(1) / (energy * energy);

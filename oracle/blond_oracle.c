@@ -59,28 +59,31 @@ void oracle_drift_##SUF(real *dt, const real *dE, int solver, real t_rev,     \
         const real coeff = T * eta_0 / (beta * beta * energy);                \
         for (int i = 0; i < n; ++i) dt[i] += coeff * dE[i];                   \
     } else if (solver == 1) {                                                 \
-        const real c = (real)1 / (beta * beta * energy);                      \
+        /* The reference writes the constants as double literals (1., 2.), \
+         * so in its float build these expressions run in double and are   \
+         * rounded to float only on assignment; kept verbatim in form.     */ \
+        const real c = 1. / (beta * beta * energy);                           \
         const real e0 = eta_0 * c, e1 = eta_1 * c * c, e2 = eta_2 * c * c * c;\
         for (int i = 0; i < n; ++i) {                                         \
             const real d = dE[i];                                             \
-            real den;                                                         \
-            if (alpha_order == 0) den = (real)1 - e0 * d;                     \
-            else if (alpha_order == 1) den = (real)1 - e0 * d - e1 * d * d;   \
-            else den = (real)1 - e0 * d - e1 * d * d - e2 * d * d * d;        \
-            dt[i] += T * ((real)1 / den - (real)1);                           \
+            double den;                                                       \
+            if (alpha_order == 0) den = 1. - e0 * d;                          \
+            else if (alpha_order == 1) den = 1. - e0 * d - e1 * d * d;        \
+            else den = 1. - e0 * d - e1 * d * d - e2 * d * d * d;             \
+            dt[i] += T * (1. / den - 1.);                                     \
         }                                                                     \
     } else {                                                                  \
-        const real ib2 = (real)1 / (beta * beta);                             \
-        const real ie2 = (real)1 / (energy * energy);                         \
+        const real ib2 = 1 / (beta * beta);                                   \
+        const real ie2 = 1 / (energy * energy);                               \
         for (int i = 0; i < n; ++i) {                                         \
             const real d = dE[i];                                             \
-            const real delta = SQRT((real)1 + ib2 * (d * d * ie2              \
-                                    + (real)2 * d / energy)) - (real)1;       \
-            dt[i] += T * (((real)1 + alpha_0 * delta                          \
+            const real delta = sqrt(1. + ib2 * (d * d * ie2                   \
+                                    + 2. * d / energy)) - 1.;                 \
+            dt[i] += T * ((1. + alpha_0 * delta                               \
                            + alpha_1 * (delta * delta)                        \
                            + alpha_2 * (delta * delta * delta))               \
-                          * ((real)1 + d / energy) / ((real)1 + delta)        \
-                          - (real)1);                                         \
+                          * (1. + d / energy) / (1. + delta)                  \
+                          - 1.);                                              \
         }                                                                     \
     }                                                                         \
 }                                                                             \
@@ -164,8 +167,8 @@ void oracle_fast_resonator_##SUF(real *re, real *im, const real *freq,       \
         const real q2 = Q[r] * Q[r];                                          \
         for (int k = 1; k < n_f; ++k) {                                       \
             const real x = freq[k] / fr[r] - fr[r] / freq[k];                 \
-            re[k] += R[r] / ((real)1 + q2 * x * x);                           \
-            im[k] -= R[r] * (Q[r] * x) / ((real)1 + q2 * x * x);              \
+            re[k] += R[r] / (1.0 + q2 * x * x);                               \
+            im[k] -= R[r] * (Q[r] * x) / (1.0 + q2 * x * x);                  \
         }                                                                     \
     }                                                                         \
 }
