@@ -52,6 +52,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--kernel", default="auto", choices=["auto", "tma", "plain"])
     return ap.parse_args()
 
 
@@ -203,7 +204,7 @@ def barrier(world):
 
 
 # ----------------------------------------------------------------- our arm
-def build_fused(n, S, n_turns, precision):
+def build_fused(n, S, n_turns, precision, kernel="auto"):
     import torch
     from blond_b200.beam.beam import Beam
     from blond_b200.beam.profile import CutOptions, Profile
@@ -219,7 +220,8 @@ def build_fused(n, S, n_turns, precision):
     iv = InducedVoltageFreq(beam, prof, [Resonators(5e6, 1e9, 1.0)])
     tiv = TotalInducedVoltage(beam, prof, [iv])
     tracker = RingAndRFTracker(rf, beam)
-    fused = FusedTracker(tracker, prof, tiv, precision=precision, turns_per_graph=50)
+    fused = FusedTracker(tracker, prof, tiv, precision=precision, turns_per_graph=50,
+                         kernel=kernel)
     return fused, beam, iv.n_fft
 
 
@@ -243,8 +245,9 @@ def run_ours(args, world, rank, local):
     kt = min(K, 20)
     E = args.e2e_steps
     total = W + K + kt + E + 4
-    fused, beam, n_fft = build_fused(n, S, total, args.precision)
+    fused, beam, n_fft = build_fused(n, S, total, args.precision, args.kernel)
     fused.track(W)
+    fused.prepare()  # graph capture/upload outside the timed region
     torch.cuda.synchronize()
     barrier(world)
     clocks = ClockSampler(local) if rank == 0 else None
@@ -253,6 +256,7 @@ def run_ours(args, world, rank, local):
     ms_max = dist_max(ms, world)
     value = world * n * K / (ms_max * 1e-3)
     # kernel durations (non-graph launches bracketed by events)
+    fused.check()
     head_ms, part_ms = fused.time_kernels(kt)
     part_avg = part_ms / kt
     head_avg = head_ms / kt
@@ -289,7 +293,8 @@ def run_ours(args, world, rank, local):
                    "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": _traffic(args.precision, n),
-                     "kernel": "particle_kernel (lik+kick+drift+deposit)",
+                     "kernel": f"particle_kernel{'_tma' if fused.kernel == 'tma' else ''} "
+                               "(lik+kick+drift+deposit)",
                      "kernel_ms": part_avg, "head_kernel_ms": head_avg,
                      "bytes_per_particle": BYTES_PER_PARTICLE[args.precision],
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst copy)"
@@ -303,8 +308,9 @@ def run_ours(args, world, rank, local):
     if rank == 0 and world == 1 and not args.no_mixed and args.precision == "f64":
         del fused, beam
         torch.cuda.empty_cache()
-        fm, bm_, _ = build_fused(n, S, W + K + kt + 4, "f32p64")
+        fm, bm_, _ = build_fused(n, S, W + K + kt + 4, "f32p64", args.kernel)
         fm.track(W)
+        fm.prepare()
         ms32 = time_turns(fm, K)
         h32, p32 = fm.time_kernels(kt)
         ach32 = BYTES_PER_PARTICLE["f32p64"] * n / (p32 / kt * 1e-3) / 1e9

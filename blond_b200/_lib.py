@@ -67,6 +67,9 @@ _EXTRA = {
     "blond_engine_set_turn": [c_ptr, c_i64, c_ptr],
     "blond_engine_slice": [c_ptr, c_ptr],
     "blond_engine_run": [c_ptr, c_i64, c_ptr],
+    "blond_engine_prepare": [c_ptr, c_ptr],
+    "blond_engine_check": [c_ptr, c_ptr],
+    "blond_engine_set_kernel": [c_ptr, c_int],
     "blond_engine_get_profile": [c_ptr, c_ptr, c_ptr],
     "blond_engine_get_induced_voltage": [c_ptr, c_ptr, c_ptr],
     "blond_engine_get_turn": [c_ptr, ct.POINTER(c_i64)],

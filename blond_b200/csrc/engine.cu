@@ -120,6 +120,78 @@ __device__ __forceinline__ void track_one(double& t,
     (void)sh;
 }
 
+// Two particles at once, with the interpolation-table gathers (L2-resident,
+// the longest-latency loads of the pass) issued before the RF sines so their
+// latency overlaps the sine arithmetic.  Same operations, in the same order
+// per particle, as two calls of track_one.
+template <int PREC, int SOLVER, bool LIK>
+__device__ __forceinline__ void track_pair(double& t0, double& t1,
+                                           typename Coord<PREC>::E& e0,
+                                           typename Coord<PREC>::E& e1,
+                                           const TurnConsts& c, const ParticleArgs& a,
+                                           int order) {
+    using E = typename Coord<PREC>::E;
+    using TB = typename Vec2<E>::type;
+    bool in0 = false, in1 = false;
+    TB tb0, tb1;
+    if (LIK) {
+        const double f0 = floor((t0 - a.bc0) * a.lik_inv_w);
+        const double f1 = floor((t1 - a.bc0) * a.lik_inv_w);
+        in0 = f0 >= 0.0 && f0 < (double)(a.S - 1);
+        in1 = f1 >= 0.0 && f1 < (double)(a.S - 1);
+        const int k0 = in0 ? (int)f0 : 0, k1 = in1 ? (int)f1 : 0;
+        tb0 = __ldg(reinterpret_cast<const TB*>(a.table) + k0);
+        tb1 = __ldg(reinterpret_cast<const TB*>(a.table) + k1);
+        if (PREC == PREC_F32P64) {
+            // offsets from the slice centre, needed before t changes
+            tb0.y = tb0.y * (float)(t0 - (a.bc0 + (double)k0 * a.bw));
+            tb1.y = tb1.y * (float)(t1 - (a.bc0 + (double)k1 * a.bw));
+        }
+    }
+    E s0, s1;
+    if (PREC == PREC_F64) {
+        double x0 = 0.0, x1 = 0.0;
+        for (int j = 0; j < a.n_rf; ++j) {
+            x0 += c.V[j] * sin(c.om[j] * t0 + c.ph[j]);
+            x1 += c.V[j] * sin(c.om[j] * t1 + c.ph[j]);
+        }
+        s0 = (E)x0;
+        s1 = (E)x1;
+    } else {
+        float x0 = 0.0f, x1 = 0.0f;
+        for (int j = 0; j < a.n_rf; ++j) {
+            x0 += c.Vf[j] * sinf((float)reduce_2pi(fma(c.om[j], t0, c.ph[j])));
+            x1 += c.Vf[j] * sinf((float)reduce_2pi(fma(c.om[j], t1, c.ph[j])));
+        }
+        s0 = (E)x0;
+        s1 = (E)x1;
+    }
+    if (LIK) {
+        if (PREC == PREC_F64) {
+            if (in0) e0 += t0 * tb0.x + tb0.y;
+            if (in1) e1 += t1 * tb1.x + tb1.y;
+        } else {
+            if (in0) e0 += tb0.x + tb0.y;
+            if (in1) e1 += tb1.x + tb1.y;
+        }
+    }
+    const E q = (E)a.charge, acc = (E)c.acc;
+    e0 += q * s0 + acc;
+    e1 += q * s1 + acc;
+    if (SOLVER == BLOND_SOLVER_SIMPLE) {
+        t0 = drift_simple<double>(t0, (double)e0, c.d.simple);
+        t1 = drift_simple<double>(t1, (double)e1, c.d.simple);
+    } else if (SOLVER == BLOND_SOLVER_LEGACY) {
+        t0 = drift_legacy<double>(t0, (double)e0, c.d.Tr, c.d.e0, c.d.e1, c.d.e2, order);
+        t1 = drift_legacy<double>(t1, (double)e1, c.d.Tr, c.d.e0, c.d.e1, c.d.e2, order);
+    } else {
+        t0 = drift_exact<double>(t0, (double)e0, c.d.Tr, c.d.ib2, c.d.ie2, c.d.a0, c.d.a1,
+                                 c.d.a2, c.d.energy);
+        t1 = drift_exact<double>(t1, (double)e1, c.d.Tr, c.d.ib2, c.d.ie2, c.d.a0, c.d.a1,
+                                 c.d.a2, c.d.energy);
+    }
+}
+
 __device__ __forceinline__ int engine_bin(double t, double cut_left, double inv_w, int S) {
     const double f = floor(__dmul_rn(__dsub_rn(t, cut_left), inv_w));
     return (f >= 0.0 && f < (double)S) ? (int)f : -1;
@@ -134,7 +206,32 @@ __device__ __forceinline__ void deposit(int* sh, int b, bool warp_agg, unsigned 
     }
 }
 
+// Flush the block-private histograms of one thread-block cluster: CTA r sums
+// bin range r of every CTA's shared histogram through distributed shared
+// memory and adds the sums to the global histogram, so a cluster of C
+// blocks issues S global atomics instead of C * S.  (A launch without a
+// cluster attribute is a cluster of one.)
+__device__ __forceinline__ void cluster_flush(int* sh, int* hist, int S) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    const int C = (int)cl.num_blocks();
+    const int r = (int)cl.block_rank();
+    cl.sync();  // every CTA of the cluster has finished depositing
+    const int per = (S + C - 1) / C;
+    const int hi = min(S, (r + 1) * per);
+    for (int k = r * per + threadIdx.x; k < hi; k += blockDim.x) {
+        int sum = 0;
+        for (int q = 0; q < C; ++q) sum += cl.map_shared_rank(sh, q)[k];
+        if (sum) atomicAdd(&hist[k], sum);
+    }
+    cl.sync();  // remote reads done before any CTA's shared memory goes away
+}
+
 constexpr int kEngineThreads = 512;
+// CTAs whose histograms are merged on chip before the global flush.  1: on
+// the C2 workload (64 KB histograms, 2 blocks/SM) clusters of 8 cost more
+// in lost co-scheduling than they save in atomics (142 vs 87 us measured).
+constexpr int kEngineCluster = 1;
 
 // Pairs of particles per thread and iteration; pairs are read with one
 // 16-byte (dt) and one 16- or 8-byte (dE) load.
@@ -177,8 +274,7 @@ particle_kernel(const ParticleArgs a) {
         if (p < npairs) {
             double2 tt = reinterpret_cast<const double2*>(dt)[p];
             E2 ee = reinterpret_cast<const E2*>(dE)[p];
-            track_one<PREC, SOLVER, LIK, KICK, true, WARP_AGG>(tt.x, ee.x, c, a, sh, order);
-            track_one<PREC, SOLVER, LIK, KICK, true, WARP_AGG>(tt.y, ee.y, c, a, sh, order);
+            if (KICK) track_pair<PREC, SOLVER, LIK>(tt.x, tt.y, ee.x, ee.y, c, a, order);
             if (KICK) {
                 reinterpret_cast<double2*>(dt)[p] = tt;
                 reinterpret_cast<E2*>(dE)[p] = ee;
@@ -200,6 +296,159 @@ particle_kernel(const ParticleArgs a) {
         }
         const int b = engine_bin(t, a.cut_left, a.inv_w, a.S);
         if (b >= 0) atomicAdd(&sh[b], 1);
+    }
+    cluster_flush(sh, a.hist, a.S);
+}
+
+// ------------------------------------------------------ TMA-pipelined pass
+// The plain kernel above is latency-bound (ncu: long-scoreboard stalls at
+// 50% occupancy): each warp has only its own few loads in flight while it
+// computes the FP64 sines.  Here one block per SM streams fixed-size chunks
+// of dt/dE into shared memory with bulk asynchronous copies
+// (cp.async.bulk ... mbarrier::complete_tx) kSt stages ahead, so the copy
+// engine keeps the HBM busy while the warps compute; results go straight
+// back to global memory with coalesced stores.
+constexpr int kTile = 2048;    // particles per chunk
+constexpr int kStages = 4;     // chunks in flight per block
+constexpr int kTmaThreads = 1024;  // 32 warps: enough to hide the FP64 sine chains
+constexpr long long kWaitLimit = 1LL << 26;  // bounded mbarrier spin
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes,
+                                         uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.b32 %0, 1, 0, p;\n}" : "=r"(ok) : "r"(smem_u32(bar)), "r"(parity) : "memory");
+    return ok != 0;
+}
+// Bounded wait, warp-uniform: every lane polls (each needs the acquire of
+// the completed phase) and the warp leaves together.  Returns false (and
+// sets the error word) if the copy never lands.
+__device__ __forceinline__ bool mbar_wait_warp(uint64_t* bar, uint32_t parity, int* err) {
+    for (long long it = 0; it < kWaitLimit; ++it)
+        if (__all_sync(0xffffffffu, mbar_try_wait(bar, parity))) return true;
+    if ((threadIdx.x & 31) == 0) atomicExch(err, 1);
+    return false;
+}
+// Single-thread bounded wait used on the error path.
+__device__ __forceinline__ void mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+    for (long long it = 0; it < kWaitLimit; ++it)
+        if (mbar_try_wait(bar, parity)) return;
+}
+
+template <int PREC, int SOLVER, bool LIK, bool WARP_AGG>
+__global__ void __launch_bounds__(kTmaThreads, 1)
+particle_kernel_tma(const ParticleArgs a, int* err) {
+    using E = typename Coord<PREC>::E;
+    using E2 = typename Vec2<E>::type;
+    extern __shared__ __align__(128) unsigned char dsm[];
+    __shared__ TurnConsts c;
+    __shared__ __align__(8) uint64_t full[kStages];
+    int* sh = reinterpret_cast<int*>(dsm);
+    const size_t hist_bytes = ((size_t)a.S * sizeof(int) + 127) & ~(size_t)127;
+    double* st_dt = reinterpret_cast<double*>(dsm + hist_bytes);
+    E* st_dE = reinterpret_cast<E*>(dsm + hist_bytes + sizeof(double) * kTile * kStages);
+
+    long long t_idx = a.turn ? (*a.turn - 1) : 0;
+    if (t_idx < 0) t_idx = 0;
+    if (t_idx >= a.n_turns) t_idx = a.n_turns - 1;
+    for (int j = threadIdx.x; j < a.n_rf; j += blockDim.x) {
+        c.V[j] = a.V[t_idx * a.n_rf + j];
+        c.Vf[j] = (float)c.V[j];
+        c.om[j] = a.om[t_idx * a.n_rf + j];
+        c.ph[j] = a.ph[t_idx * a.n_rf + j];
+    }
+    if (threadIdx.x == 0) {
+        c.acc = a.acc[t_idx];
+        c.d = a.drift[t_idx + 1];
+        for (int s = 0; s < kStages; ++s) mbar_init(&full[s], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    for (int k = threadIdx.x; k < a.S; k += blockDim.x) sh[k] = 0;
+    __syncthreads();
+
+    double* dt = reinterpret_cast<double*>(a.dt);
+    E* dE = reinterpret_cast<E*>(a.dE);
+    const long long nchunks = a.n / kTile;
+    // this block's chunks: blockIdx.x, blockIdx.x + gridDim.x, ...
+    const long long mine = nchunks > blockIdx.x
+                               ? (nchunks - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+    const uint32_t bytes_dt = sizeof(double) * kTile, bytes_dE = sizeof(E) * kTile;
+    auto issue = [&](long long i) {
+        const int s = (int)(i % kStages);
+        const long long chunk = blockIdx.x + i * gridDim.x;
+        mbar_expect_tx(&full[s], bytes_dt + bytes_dE);
+        bulk_g2s(st_dt + (size_t)s * kTile, dt + chunk * kTile, bytes_dt, &full[s]);
+        bulk_g2s(st_dE + (size_t)s * kTile, dE + chunk * kTile, bytes_dE, &full[s]);
+    };
+    if (threadIdx.x == 0)
+        for (long long i = 0; i < mine && i < kStages; ++i) issue(i);
+
+    const int order = a.order;
+    for (long long i = 0; i < mine; ++i) {
+        const int s = (int)(i % kStages);
+        const bool got = mbar_wait_warp(&full[s], (uint32_t)((i / kStages) & 1), err);
+        if (got) {
+            const long long base = (blockIdx.x + i * gridDim.x) * (long long)kTile;
+            const double2* sdt = reinterpret_cast<const double2*>(st_dt + (size_t)s * kTile);
+            const E2* sdE = reinterpret_cast<const E2*>(st_dE + (size_t)s * kTile);
+#pragma unroll
+            for (int q = 0; q < kTile / 2 / kTmaThreads; ++q) {
+                const int p = threadIdx.x + q * kTmaThreads;  // pair within the chunk
+                double2 tt = sdt[p];
+                E2 ee = sdE[p];
+                track_pair<PREC, SOLVER, LIK>(tt.x, tt.y, ee.x, ee.y, c, a, order);
+                reinterpret_cast<double2*>(dt + base)[p] = tt;
+                reinterpret_cast<E2*>(dE + base)[p] = ee;
+                deposit(sh, engine_bin(tt.x, a.cut_left, a.inv_w, a.S), WARP_AGG, 0xffffffffu);
+                deposit(sh, engine_bin(tt.y, a.cut_left, a.inv_w, a.S), WARP_AGG, 0xffffffffu);
+            }
+        }
+        // stage s fully consumed; the failure decision is block-uniform
+        if (__syncthreads_or(!got)) {
+            // copies i .. min(mine, i + kStages) - 1 are in flight: give
+            // them a bounded chance to land before the block's shared
+            // memory is released, then leave without flushing
+            if (threadIdx.x == 0)
+                for (long long j = i; j < mine && j < i + kStages; ++j)
+                    mbar_wait_bounded(&full[j % kStages], (uint32_t)((j / kStages) & 1));
+            __syncthreads();
+            return;
+        }
+        if (threadIdx.x == 0 && i + kStages < mine) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            issue(i + kStages);
+        }
+    }
+    // remainder particles (fewer than one chunk): plain loads, last block
+    if (blockIdx.x == gridDim.x - 1) {
+        for (long long i = nchunks * kTile + threadIdx.x; i < a.n; i += blockDim.x) {
+            double t = dt[i];
+            E e = dE[i];
+            track_one<PREC, SOLVER, LIK, true, true, false>(t, e, c, a, sh, order);
+            dt[i] = t;
+            dE[i] = e;
+            const int b = engine_bin(t, a.cut_left, a.inv_w, a.S);
+            if (b >= 0) atomicAdd(&sh[b], 1);
+        }
     }
     __syncthreads();
     for (int k = threadIdx.x; k < a.S; k += blockDim.x) {
@@ -247,11 +496,13 @@ struct blond_engine {
     bool has_fft = false;
     SpecPlan plan = {};
     double2* d_H = nullptr;
+    double2* d_tw = nullptr;  // twiddle tables of the spectral plan
     double iv_scale = 0.0;
     bool has_ind = false;
     double* d_ind = nullptr;
     // state
     long long* d_turn = nullptr;
+    int* d_err = nullptr;  // set by a kernel whose bounded wait gave up
     long long host_turn = 0;
     int* d_hist = nullptr;
     double* d_profile = nullptr;
@@ -265,6 +516,7 @@ struct blond_engine {
     int threads = kEngineThreads;
     int blocks_per_sm = 2;
     int turns_per_graph = 50;
+    int variant = 0;  // 0: TMA-pipelined particle pass, 1: plain loads
     // graph cache
     cudaStream_t cap_stream = nullptr;
     cudaGraphExec_t graph = nullptr;
@@ -297,22 +549,62 @@ static int allow_max_smem(K kernel, bool* done) {
     return BLOND_OK;
 }
 
+template <int PREC>
+static size_t tma_smem(int S) {
+    using E = typename Coord<PREC>::E;
+    const size_t hist = ((size_t)S * sizeof(int) + 127) & ~(size_t)127;
+    return hist + (size_t)kStages * kTile * (sizeof(double) + sizeof(E));
+}
+
 template <int PREC, int SOLVER, bool LIK, bool KICK>
 static int launch_particles_t(blond_engine* e, const ParticleArgs& a, cudaStream_t s,
                               bool launch) {
     static bool done_agg[64] = {false}, done_plain[64] = {false};
+    static bool done_tma_agg[64] = {false}, done_tma[64] = {false};
     const int smem = engine_smem(e);
     const bool agg = e->S <= 2048;
-    const int grid = particle_grid(e->n / 2 + 1, e->threads, e->blocks_per_sm);
     int rc;
-    if (agg) {
-        auto k = particle_kernel<PREC, SOLVER, LIK, KICK, true>;
-        if ((rc = allow_max_smem(k, done_agg))) return rc;
-        if (launch) k<<<grid, e->threads, smem, s>>>(a);
-    } else {
-        auto k = particle_kernel<PREC, SOLVER, LIK, KICK, false>;
-        if ((rc = allow_max_smem(k, done_plain))) return rc;
-        if (launch) k<<<grid, e->threads, smem, s>>>(a);
+    if (KICK && e->variant == 0) {
+        const size_t tsm = tma_smem<PREC>(e->S);
+        auto k_agg = particle_kernel_tma<PREC, SOLVER, LIK, true>;
+        auto k_pl = particle_kernel_tma<PREC, SOLVER, LIK, false>;
+        cudaFuncAttributes fa;
+        BB_CUDA(cudaFuncGetAttributes(&fa, agg ? k_agg : k_pl));
+        if (tsm + fa.sharedSizeBytes <= (size_t)device_info().max_smem_optin) {
+            const long long nchunks = e->n / kTile;
+            const int grid = (int)std::max<long long>(
+                1, std::min<long long>(nchunks, device_info().sm_count));
+            if (agg) {
+                if ((rc = allow_max_smem(k_agg, done_tma_agg))) return rc;
+                if (launch) k_agg<<<grid, kTmaThreads, tsm, s>>>(a, e->d_err);
+            } else {
+                if ((rc = allow_max_smem(k_pl, done_tma))) return rc;
+                if (launch) k_pl<<<grid, kTmaThreads, tsm, s>>>(a, e->d_err);
+            }
+            BB_LAUNCH_CHECK();
+            return BLOND_OK;
+        }
+        // profile too long for the staged copy: plain loads below
+    }
+    int grid = particle_grid(e->n / 2 + 1, e->threads, e->blocks_per_sm);
+    grid = (grid + kEngineCluster - 1) / kEngineCluster * kEngineCluster;
+    auto k = agg ? particle_kernel<PREC, SOLVER, LIK, KICK, true>
+                 : particle_kernel<PREC, SOLVER, LIK, KICK, false>;
+    if ((rc = allow_max_smem(k, agg ? done_agg : done_plain))) return rc;
+    if (launch) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(grid, 1, 1);
+        cfg.blockDim = dim3(e->threads, 1, 1);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = s;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = kEngineCluster;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = kEngineCluster > 1 ? 1 : 0;
+        BB_CUDA(cudaLaunchKernelEx(&cfg, k, a));
     }
     BB_LAUNCH_CHECK();
     return BLOND_OK;
@@ -404,6 +696,7 @@ static int launch_head(blond_engine* e, cudaStream_t s) {
     P.bc = e->d_bc;
     P.turn = e->d_turn;
     P.bump_turn = 1;
+    P.twg = e->d_tw;
     return launch_spectral(P, s);
 }
 
@@ -454,6 +747,7 @@ int blond_engine_create(blond_engine** out, int precision, int n_rf, int solver,
     int rc = BLOND_OK;
     do {
         if (cudaMalloc(&e->d_turn, sizeof(long long)) != cudaSuccess ||
+            cudaMalloc(&e->d_err, sizeof(int)) != cudaSuccess ||
             cudaMalloc(&e->d_hist, sizeof(int) * n_slices) != cudaSuccess ||
             cudaMalloc(&e->d_profile, sizeof(double) * n_slices) != cudaSuccess ||
             cudaMalloc(&e->d_vind, sizeof(double) * n_slices) != cudaSuccess ||
@@ -463,6 +757,7 @@ int blond_engine_create(blond_engine** out, int precision, int n_rf, int solver,
             break;
         }
         cudaMemset(e->d_turn, 0, sizeof(long long));
+        cudaMemset(e->d_err, 0, sizeof(int));
         cudaMemset(e->d_hist, 0, sizeof(int) * n_slices);
         cudaMemset(e->d_profile, 0, sizeof(double) * n_slices);
         cudaMemset(e->d_vind, 0, sizeof(double) * n_slices);
@@ -490,8 +785,9 @@ int blond_engine_destroy(blond_engine* e) {
     if (e->graph) cudaGraphExecDestroy(e->graph);
     if (e->cap_stream) cudaStreamDestroy(e->cap_stream);
     for (void* p : {(void*)e->d_V, (void*)e->d_om, (void*)e->d_ph, (void*)e->d_acc,
-                    (void*)e->d_drift, (void*)e->d_bc, (void*)e->d_H, (void*)e->d_ind,
-                    (void*)e->d_turn, (void*)e->d_hist, (void*)e->d_profile,
+                    (void*)e->d_drift, (void*)e->d_bc, (void*)e->d_H, (void*)e->d_tw,
+                    (void*)e->d_ind,
+                    (void*)e->d_turn, (void*)e->d_err, (void*)e->d_hist, (void*)e->d_profile,
                     (void*)e->d_vind, e->d_table})
         free_ptr(p);
     delete e;
@@ -585,8 +881,14 @@ int blond_engine_set_impedance(blond_engine* e, int64_t n_fft, const double* Z,
     BB_CHECK_SIZE(plan.smem <= device_info().max_smem_optin,
                   "engine_set_impedance: n_fft=%lld needs too much shared memory",
                   (long long)n_fft);
+    BB_CHECK_SIZE(n_fft >= e->S, "engine_set_impedance: n_fft=%lld shorter than the "
+                  "profile (%d slices)", (long long)n_fft, e->S);
     int rc = upload((void**)&e->d_H, Z, sizeof(double2) * (size_t)(n_fft / 2 + 1));
     if (rc) return rc;
+    // twiddle tables of this plan, computed once instead of every turn
+    free_ptr(e->d_tw);
+    e->d_tw = nullptr;
+    if ((rc = make_spec_twiddles(plan, &e->d_tw))) return rc;
     e->plan = plan;
     e->iv_scale = scale;
     e->has_fft = true;
@@ -614,9 +916,8 @@ int blond_engine_bind_beam(blond_engine* e, void* dt, void* dE, int64_t n) {
     BB_CHECK_ARG(e && dt && dE, "engine_bind_beam: null pointer");
     BB_CHECK_ARG(n >= 1, "engine_bind_beam: n must be >= 1");
     BB_CHECK_ARG(aligned(dt, 16), "engine_bind_beam: dt must be 16-byte aligned");
-    BB_CHECK_ARG(aligned(dE, e->precision == BLOND_PREC_F64 ? 16 : 8),
-                 "engine_bind_beam: dE must be %d-byte aligned",
-                 e->precision == BLOND_PREC_F64 ? 16 : 8);
+    // 16 bytes: pair loads, and the bulk copies need 16-byte aligned sources
+    BB_CHECK_ARG(aligned(dE, 16), "engine_bind_beam: dE must be 16-byte aligned");
     e->dt = dt;
     e->dE = dE;
     e->n = n;
@@ -647,6 +948,28 @@ int blond_engine_slice(blond_engine* e, void* stream) {
     return launch_profile(e, false, s);
 }
 
+int blond_engine_set_kernel(blond_engine* e, int variant) {
+    BB_CHECK_ARG(e && (variant == 0 || variant == 1), "engine_set_kernel: variant 0 or 1");
+    e->variant = variant;
+    e->graph_dirty = true;
+    return BLOND_OK;
+}
+
+int blond_engine_check(blond_engine* e, void* stream) {
+    BB_CHECK_ARG(e, "engine_check: null engine");
+    int flag = 0;
+    BB_CUDA(cudaMemcpyAsync(&flag, e->d_err, sizeof(int), cudaMemcpyDeviceToHost,
+                            as_stream(stream)));
+    BB_CUDA(cudaStreamSynchronize(as_stream(stream)));
+    if (flag) {
+        BB_CUDA(cudaMemsetAsync(e->d_err, 0, sizeof(int), as_stream(stream)));
+        set_error("engine: a bounded device-side wait gave up (bulk copy never "
+                  "completed); the coordinates of this run are not valid");
+        return BLOND_ERR_TIMEOUT;
+    }
+    return BLOND_OK;
+}
+
 int blond_engine_tune(blond_engine* e, int threads, int blocks_per_sm, int turns_per_graph) {
     BB_CHECK_ARG(e, "engine_tune: null engine");
     if (threads) {
@@ -658,6 +981,47 @@ int blond_engine_tune(blond_engine* e, int threads, int blocks_per_sm, int turns
     if (turns_per_graph) e->turns_per_graph = turns_per_graph;
     e->graph_dirty = true;
     return BLOND_OK;
+}
+
+// Capture (once per configuration) the graph of turns_per_graph turns and
+// upload it to the device, so that the first replay costs no set-up time.
+static int ensure_graph(blond_engine* e, cudaStream_t s) {
+    const int K = e->turns_per_graph;
+    if (!e->graph_dirty && e->graph_turns == K && e->graph) return BLOND_OK;
+    int rc;
+    // kernel attributes are set here, never inside the capture
+    if ((rc = launch_particles(e, true, s, false))) return rc;
+    if (e->has_fft && (rc = prepare_spectral())) return rc;
+    if (e->graph) cudaGraphExecDestroy(e->graph);
+    e->graph = nullptr;
+    cudaGraph_t g;
+    BB_CUDA(cudaStreamBeginCapture(e->cap_stream, cudaStreamCaptureModeThreadLocal));
+    int lrc = BLOND_OK;
+    for (int i = 0; i < K && lrc == BLOND_OK; ++i) lrc = launch_turn(e, e->cap_stream);
+    cudaError_t ce = cudaStreamEndCapture(e->cap_stream, &g);
+    if (lrc) return lrc;
+    if (ce != cudaSuccess) {
+        set_error("engine: graph capture failed: %s", cudaGetErrorString(ce));
+        return BLOND_ERR_CUDA;
+    }
+    ce = cudaGraphInstantiate(&e->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (ce != cudaSuccess) {
+        set_error("engine: graph instantiation failed: %s", cudaGetErrorString(ce));
+        return BLOND_ERR_CUDA;
+    }
+    BB_CUDA(cudaGraphUpload(e->graph, s));
+    e->graph_turns = K;
+    e->graph_dirty = false;
+    return BLOND_OK;
+}
+
+int blond_engine_prepare(blond_engine* e, void* stream) {
+    BB_CHECK_ARG(e, "engine_prepare: null engine");
+    int rc = check_ready(e);
+    if (rc) return rc;
+    if (e->turns_per_graph <= 1) return BLOND_OK;
+    return ensure_graph(e, as_stream(stream));
 }
 
 int blond_engine_run(blond_engine* e, int64_t n_turns, void* stream) {
@@ -673,31 +1037,7 @@ int blond_engine_run(blond_engine* e, int64_t n_turns, void* stream) {
     const int K = e->turns_per_graph;
     int64_t done = 0;
     if (n_turns >= K && K > 1) {
-        if (e->graph_dirty || e->graph_turns != K) {
-            // kernel attributes are set here, never inside the capture
-            if ((rc = launch_particles(e, true, s, false))) return rc;
-            if (e->has_fft && (rc = prepare_spectral())) return rc;
-            if (e->graph) cudaGraphExecDestroy(e->graph);
-            e->graph = nullptr;
-            cudaGraph_t g;
-            BB_CUDA(cudaStreamBeginCapture(e->cap_stream, cudaStreamCaptureModeThreadLocal));
-            int lrc = BLOND_OK;
-            for (int i = 0; i < K && lrc == BLOND_OK; ++i) lrc = launch_turn(e, e->cap_stream);
-            cudaError_t ce = cudaStreamEndCapture(e->cap_stream, &g);
-            if (lrc) return lrc;
-            if (ce != cudaSuccess) {
-                set_error("engine_run: graph capture failed: %s", cudaGetErrorString(ce));
-                return BLOND_ERR_CUDA;
-            }
-            ce = cudaGraphInstantiate(&e->graph, g, 0);
-            cudaGraphDestroy(g);
-            if (ce != cudaSuccess) {
-                set_error("engine_run: graph instantiation failed: %s", cudaGetErrorString(ce));
-                return BLOND_ERR_CUDA;
-            }
-            e->graph_turns = K;
-            e->graph_dirty = false;
-        }
+        if ((rc = ensure_graph(e, s))) return rc;
         for (; done + K <= n_turns; done += K) BB_CUDA(cudaGraphLaunch(e->graph, s));
     }
     for (; done < n_turns; ++done) {

@@ -55,7 +55,18 @@ bool make_spec_plan(int64_t N, SpecPlan& plan) {
     plan.Br = plan.M1 / plan.C;
     radix_schedule(plan.M1, plan.r1, plan.n1);
     radix_schedule(plan.M2, plan.r2, plan.n2);
-    plan.smem = (int)sizeof(double2) * (2 * (M / plan.C) + plan.M1 + plan.M2);
+    plan.L = 1;
+    while ((int64_t)plan.L * plan.L < M) plan.L *= 2;
+    // fewest cluster barriers (three buffers) and staged impedance when the
+    // shared memory allows, else fall back step by step
+    const int budget = device_info().max_smem_optin;
+    const int options[4][2] = {{3, 1}, {3, 0}, {2, 1}, {2, 0}};
+    for (const auto& o : options) {
+        plan.nbuf = o[0];
+        plan.prefetch = o[1];
+        plan.smem = spec_layout(plan).total;
+        if (plan.smem <= budget) break;
+    }
     return true;
 }
 
@@ -95,6 +106,25 @@ int launch_spectral(const SpecParams& P, cudaStream_t stream) {
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     BB_CUDA(cudaLaunchKernelEx(&cfg, spectral_kernel, P));
+    return BLOND_OK;
+}
+
+__global__ void twiddle_table_kernel(const SpecPlan p, double2* out) {
+    const SpecLayout lay = spec_layout(p);
+    double2* base = out;
+    auto at = [&](int off) { return base + (off - lay.tw1) / 16; };
+    fill_twiddles(p, at(lay.tw1), at(lay.tw2), at(lay.tam), at(lay.tbm), at(lay.tan_),
+                  at(lay.tbn), threadIdx.x, blockDim.x);
+}
+
+int make_spec_twiddles(const SpecPlan& plan, double2** out) {
+    const SpecLayout lay = spec_layout(plan);
+    const size_t bytes = (size_t)(lay.hk - lay.tw1);
+    *out = nullptr;
+    BB_CUDA(cudaMalloc(out, bytes));
+    twiddle_table_kernel<<<1, 512>>>(plan, *out);
+    BB_LAUNCH_CHECK();
+    BB_CUDA(cudaDeviceSynchronize());
     return BLOND_OK;
 }
 

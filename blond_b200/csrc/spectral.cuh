@@ -16,7 +16,16 @@
 // (the autosort formulation of Govindaraju et al., "High performance
 // discrete Fourier transforms on graphics processors", SC 2008) over an
 // interleaved batch layout element(b, i) = buf[i * B + b].  Twiddles come
-// from sincospi() in double precision.
+// from shared tables filled with sincospi() in double precision; the
+// four-step and real-to-complex twiddles use a two-level table
+// (W^j = A[j / L] * B[j % L]).
+//
+// Latency is what bounds this kernel, so it is organised around the number
+// of cluster barriers: with three buffers per CTA (when they fit) a
+// transform never writes the buffer that other CTAs read in the same phase,
+// leaving four barriers for the whole rfft -> x Z -> irfft chain; the
+// impedance and bin centres are prefetched with cp.async at launch and the
+// interpolation table is built from shared memory.
 #pragma once
 
 #include <cooperative_groups.h>
@@ -27,7 +36,7 @@ namespace bb {
 
 namespace cg = cooperative_groups;
 
-constexpr int kSpecThreads = 256;
+constexpr int kSpecThreads = 512;
 constexpr int kMaxPasses = 24;
 constexpr int kMaxCluster = 16;
 constexpr int64_t kMaxClusterFFT = 131072;  // real length N
@@ -41,6 +50,9 @@ struct SpecPlan {
     int Bc, Br;   // M2 / C columns and M1 / C rows per CTA
     int n1, n2;   // radix passes for M1 and M2
     int r1[kMaxPasses], r2[kMaxPasses];
+    int L;        // split of the two-level twiddle tables (power of two)
+    int nbuf;     // 3 (fewer cluster barriers) or 2 (largest lengths)
+    int prefetch; // impedance / bin centres staged in shared memory
     int smem;     // dynamic shared memory per CTA, bytes
 };
 
@@ -79,11 +91,19 @@ struct SpecParams {
     const double* bc;
     long long* turn;          // device turn counter (read; incremented if bump)
     int bump_turn;
+    // twiddle tables precomputed for this plan (make_spec_twiddles), or
+    // nullptr to compute them in the kernel
+    const double2* twg;
 };
 
 // Device code below is compiled only in spectral.cu (which defines
 // BB_SPECTRAL_KERNELS); other files see the types and host entry points.
 #ifdef BB_SPECTRAL_KERNELS
+
+// Phase marker for out-of-tree timing builds; expands to nothing here.
+#ifndef BB_PHASE
+#define BB_PHASE(i)
+#endif
 
 // ------------------------------------------------------------ complex ops
 __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
@@ -106,97 +126,104 @@ __device__ __forceinline__ double2 twiddle(long long num, long long den) {
     return make_double2(c, INV ? s : -s);
 }
 
-// ------------------------------------------------------------ radix kernels
-template <bool INV>
-__device__ __forceinline__ void dft2(double2* v) {
-    const double2 a = v[0], b = v[1];
-    v[0] = cadd(a, b);
-    v[1] = csub(a, b);
+// ------------------------------------------------------------ radix passes
+// The kernel runs each phase a handful of times per launch, so its speed is
+// set by instruction fetch (ncu: "no_instruction" was the top stall of a
+// version with one inlined pass per radix and direction).  One compact,
+// non-inlined pass with a runtime radix and direction serves every
+// transform: after its first use it runs from the instruction cache.
+//
+// multiply by -i (forward, s = -1) or +i (inverse, s = +1)
+__device__ __forceinline__ double2 crot_s(double2 a, double s) {
+    return make_double2(-s * a.y, s * a.x);
 }
-template <bool INV>
-__device__ __forceinline__ void dft4(double2* v) {
-    const double2 s02 = cadd(v[0], v[2]), d02 = csub(v[0], v[2]);
-    const double2 s13 = cadd(v[1], v[3]), d13 = crot<INV>(csub(v[1], v[3]));
-    v[0] = cadd(s02, s13);
-    v[2] = csub(s02, s13);
-    v[1] = cadd(d02, d13);
-    v[3] = csub(d02, d13);
-}
-template <bool INV>
-__device__ __forceinline__ void dft3(double2* v) {
-    const double h = 0.86602540378443864676;  // sin(2 pi / 3)
-    const double2 a = v[0], s = cadd(v[1], v[2]), d = csub(v[1], v[2]);
-    const double2 m = make_double2(a.x - 0.5 * s.x, a.y - 0.5 * s.y);
-    const double2 r = crot<INV>(cscale(d, h));
-    v[0] = cadd(a, s);
-    v[1] = cadd(m, r);
-    v[2] = csub(m, r);
-}
-template <bool INV>
-__device__ __forceinline__ void dft5(double2* v) {
-    const double c1 = 0.30901699437494742410, c2 = -0.80901699437494742410;
-    const double s1 = 0.95105651629515357212, s2 = 0.58778525229247312917;
-    const double2 a = v[0];
-    const double2 t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]);
-    const double2 t3 = csub(v[1], v[4]), t4 = csub(v[2], v[3]);
-    const double2 m1 = make_double2(a.x + c1 * t1.x + c2 * t2.x, a.y + c1 * t1.y + c2 * t2.y);
-    const double2 m2 = make_double2(a.x + c2 * t1.x + c1 * t2.x, a.y + c2 * t1.y + c1 * t2.y);
-    const double2 r1 = crot<INV>(make_double2(s1 * t3.x + s2 * t4.x, s1 * t3.y + s2 * t4.y));
-    const double2 r2 = crot<INV>(make_double2(s2 * t3.x - s1 * t4.x, s2 * t3.y - s1 * t4.y));
-    v[0] = cadd(a, cadd(t1, t2));
-    v[1] = cadd(m1, r1);
-    v[4] = csub(m1, r1);
-    v[2] = cadd(m2, r2);
-    v[3] = csub(m2, r2);
+
+// In-place R-point DFT (R = 2, 3, 4, 5) of v, sign s of the exponent.
+__device__ __forceinline__ void small_dft(double2* v, int R, double s) {
+    if (R == 2) {
+        const double2 a = v[0], b = v[1];
+        v[0] = cadd(a, b);
+        v[1] = csub(a, b);
+    } else if (R == 4) {
+        const double2 s02 = cadd(v[0], v[2]), d02 = csub(v[0], v[2]);
+        const double2 s13 = cadd(v[1], v[3]), d13 = crot_s(csub(v[1], v[3]), s);
+        v[0] = cadd(s02, s13);
+        v[2] = csub(s02, s13);
+        v[1] = cadd(d02, d13);
+        v[3] = csub(d02, d13);
+    } else if (R == 3) {
+        const double h = 0.86602540378443864676;  // sin(2 pi / 3)
+        const double2 a = v[0], t = cadd(v[1], v[2]), d = csub(v[1], v[2]);
+        const double2 m = make_double2(a.x - 0.5 * t.x, a.y - 0.5 * t.y);
+        const double2 r = crot_s(cscale(d, h), s);
+        v[0] = cadd(a, t);
+        v[1] = cadd(m, r);
+        v[2] = csub(m, r);
+    } else {
+        // cos / sin of 2 pi / 5 and 4 pi / 5
+        const double c1 = 0.30901699437494742410, c2 = -0.80901699437494742410;
+        const double s1 = 0.95105651629515357212, s2 = 0.58778525229247312917;
+        const double2 a = v[0];
+        const double2 t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]);
+        const double2 t3 = csub(v[1], v[4]), t4 = csub(v[2], v[3]);
+        const double2 m1 = make_double2(a.x + c1 * t1.x + c2 * t2.x, a.y + c1 * t1.y + c2 * t2.y);
+        const double2 m2 = make_double2(a.x + c2 * t1.x + c1 * t2.x, a.y + c2 * t1.y + c1 * t2.y);
+        const double2 r1 = crot_s(make_double2(s1 * t3.x + s2 * t4.x, s1 * t3.y + s2 * t4.y), s);
+        const double2 r2 = crot_s(make_double2(s2 * t3.x - s1 * t4.x, s2 * t3.y - s1 * t4.y), s);
+        v[0] = cadd(a, cadd(t1, t2));
+        v[1] = cadd(m1, r1);
+        v[4] = csub(m1, r1);
+        v[2] = cadd(m2, r2);
+        v[3] = csub(m2, r2);
+    }
 }
 
 // One Stockham pass of radix R over B interleaved transforms of length L.
-template <bool INV, int R>
-__device__ __forceinline__ void stockham_pass(const double2* __restrict__ src,
-                                              double2* __restrict__ dst, int L,
-                                              int B, int Ns,
-                                              const double2* __restrict__ tw) {
-    const int LR = L / R;
+// Index arithmetic avoids integer division when the batch count B and the
+// stride Ns are powers of two (lgB / lgNs >= 0): every power-of-two length,
+// i.e. every next_regular result of the usual 2^k slice counts.
+__device__ __noinline__ void stockham_pass(const double2* __restrict__ src,
+                                           double2* __restrict__ dst, int L, int B,
+                                           int Ns, int R, const double2* __restrict__ tw,
+                                           double s, int lgB, int lgNs, int LR, int step) {
     const int total = B * LR;
-    const int step = L / (Ns * R);
     for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
-        const int b = idx % B;
-        const int j = idx / B;
-        const int k = j % Ns;
-        double2 v[R];
+        const int b = lgB >= 0 ? (idx & (B - 1)) : idx % B;
+        const int j = lgB >= 0 ? (idx >> lgB) : idx / B;
+        const int k = lgNs >= 0 ? (j & (Ns - 1)) : j % Ns;
+        const int jq = lgNs >= 0 ? (j >> lgNs) : j / Ns;
+        double2 v[5];
 #pragma unroll
-        for (int t = 0; t < R; ++t) {
-            double2 x = src[(j + t * LR) * B + b];
-            if (t > 0 && k > 0) {
-                double2 w = tw[t * k * step];
-                if (INV) w.y = -w.y;
-                x = cmul(x, w);
+        for (int t = 0; t < 5; ++t) {
+            if (t < R) {
+                double2 x = src[(j + t * LR) * B + b];
+                if (t > 0 && k > 0) {
+                    double2 w = tw[t * k * step];
+                    w.y = -s * w.y;  // table holds exp(-2 pi i q / L)
+                    x = cmul(x, w);
+                }
+                v[t] = x;
             }
-            v[t] = x;
         }
-        if (R == 2) dft2<INV>(v);
-        if (R == 3) dft3<INV>(v);
-        if (R == 4) dft4<INV>(v);
-        if (R == 5) dft5<INV>(v);
-        const int d = (j / Ns) * Ns * R + k;
+        small_dft(v, R, s);
+        const int d = jq * Ns * R + k;
 #pragma unroll
-        for (int t = 0; t < R; ++t) dst[(d + t * Ns) * B + b] = v[t];
+        for (int t = 0; t < 5; ++t)
+            if (t < R) dst[(d + t * Ns) * B + b] = v[t];
     }
 }
 
 // B transforms of length L, interleaved, starting in a[]; returns the buffer
 // (a or b) that holds the result.  Ends with __syncthreads().
-template <bool INV>
-__device__ double2* batch_fft(double2* a, double2* b, int L, int B,
-                              const int* radices, int npass,
-                              const double2* tw) {
+__device__ double2* batch_fft(double2* a, double2* b, int L, int B, const int* radices,
+                              int npass, const double2* tw, bool inverse) {
+    const double s = inverse ? 1.0 : -1.0;
+    const int lgB = (B & (B - 1)) == 0 ? __ffs(B) - 1 : -1;
     int Ns = 1;
     for (int p = 0; p < npass; ++p) {
         const int R = radices[p];
-        if (R == 4) stockham_pass<INV, 4>(a, b, L, B, Ns, tw);
-        else if (R == 2) stockham_pass<INV, 2>(a, b, L, B, Ns, tw);
-        else if (R == 3) stockham_pass<INV, 3>(a, b, L, B, Ns, tw);
-        else stockham_pass<INV, 5>(a, b, L, B, Ns, tw);
+        const int lgNs = (Ns & (Ns - 1)) == 0 ? __ffs(Ns) - 1 : -1;
+        stockham_pass(a, b, L, B, Ns, R, tw, s, lgB, lgNs, L / R, L / (Ns * R));
         __syncthreads();
         double2* t = a;
         a = b;
@@ -206,32 +233,146 @@ __device__ double2* batch_fft(double2* a, double2* b, int L, int B,
     return a;
 }
 
+// The six twiddle tables of a plan (contiguous in the shared layout, and in
+// the same order in a precomputed global copy): tw1[q] = W_M1^q,
+// tw2[q] = W_M2^q, tam[a] = W_M^(aL), tbm[b] = W_M^b, tan[a] = W_N^(aL),
+// tbn[b] = W_N^b, with W_X = exp(-2 pi i / X) from sincospi.
+__device__ inline void fill_twiddles(const SpecPlan& p, double2* tw1, double2* tw2,
+                                     double2* tam, double2* tbm, double2* tan_,
+                                     double2* tbn, int tid, int nth) {
+    const int M = p.M, L = p.L, nA = (M + L - 1) / L;
+    for (int q = tid; q < p.M1; q += nth) tw1[q] = twiddle<false>(q, p.M1);
+    for (int q = tid; q < p.M2; q += nth) tw2[q] = twiddle<false>(q, p.M2);
+    for (int q = tid; q < nA; q += nth) {
+        tam[q] = twiddle<false>((long long)q * L, M);
+        tan_[q] = twiddle<false>((long long)q * L, 2LL * M);
+    }
+    for (int q = tid; q < L; q += nth) {
+        tbm[q] = twiddle<false>(q, M);
+        tbn[q] = twiddle<false>(q, 2LL * M);
+    }
+}
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                     (uint32_t)__cvta_generic_to_shared(smem)),
+                 "l"(gmem)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(
+                     (uint32_t)__cvta_generic_to_shared(smem)),
+                 "l"(gmem)
+                 : "memory");
+}
+
+// Shared-memory carve-up of one CTA (offsets in bytes), shared with the host.
+struct SpecLayout {
+    int bufs, tw1, tw2, tam, tbm, tan_, tbn, hk, hp, bcs, vloc, nbr, total;
+};
+__host__ __device__ inline SpecLayout spec_layout(const SpecPlan& p) {
+    SpecLayout s;
+    const int per = p.M / p.C, nA = (p.M + p.L - 1) / p.L;
+    int o = 0;
+    s.bufs = o; o += 16 * p.nbuf * per;
+    s.tw1 = o;  o += 16 * p.M1;
+    s.tw2 = o;  o += 16 * p.M2;
+    s.tam = o;  o += 16 * nA;
+    s.tbm = o;  o += 16 * p.L;
+    s.tan_ = o; o += 16 * nA;
+    s.tbn = o;  o += 16 * p.L;
+    s.hk = o;   o += p.prefetch ? 16 * per : 0;
+    s.hp = o;   o += p.prefetch ? 16 * per : 0;
+    s.bcs = o;  o += p.prefetch ? 16 * per : 0;  // two doubles per element
+    s.vloc = o; o += 8 * per;
+    s.nbr = o;  o += 8 * p.M1;
+    s.total = o;
+    return s;
+}
+
 // ------------------------------------------------------------ the kernel
 // One cluster of p.C CTAs.  Column phase: CTA c owns n2 in [c Bc, (c+1) Bc),
 // element (n1, n2) at n1 * Bc + n2 - c Bc.  Row phase: CTA c owns k1 in
 // [c Br, (c+1) Br), element (k1, k2) at k2 * Br + k1 - c Br.
-__global__ void __launch_bounds__(kSpecThreads)
+__global__ void __launch_bounds__(kSpecThreads, 1)
 spectral_kernel(const SpecParams P) {
     cg::cluster_group cluster = cg::this_cluster();
     const SpecPlan& p = P.p;
     const int c = (int)cluster.block_rank();
     const int tid = threadIdx.x, nth = blockDim.x;
-    extern __shared__ double2 smem[];
+    extern __shared__ __align__(16) unsigned char sraw[];
+    const SpecLayout lay = spec_layout(p);
     const int per = p.M / p.C;
-    double2* buf0 = smem;
-    double2* buf1 = smem + per;
-    double2* tw1 = smem + 2 * per;     // M1 entries
-    double2* tw2 = tw1 + p.M1;         // M2 entries
-    const int M = p.M, M1 = p.M1, M2 = p.M2, Bc = p.Bc, Br = p.Br;
+    const int M = p.M, M1 = p.M1, M2 = p.M2, Bc = p.Bc, Br = p.Br, L = p.L;
+    double2* buf[3] = {reinterpret_cast<double2*>(sraw + lay.bufs),
+                       reinterpret_cast<double2*>(sraw + lay.bufs) + per,
+                       reinterpret_cast<double2*>(sraw + lay.bufs) + 2 * per};
+    double2* tw1 = reinterpret_cast<double2*>(sraw + lay.tw1);
+    double2* tw2 = reinterpret_cast<double2*>(sraw + lay.tw2);
+    double2* tam = reinterpret_cast<double2*>(sraw + lay.tam);
+    double2* tbm = reinterpret_cast<double2*>(sraw + lay.tbm);
+    double2* tan_ = reinterpret_cast<double2*>(sraw + lay.tan_);
+    double2* tbn = reinterpret_cast<double2*>(sraw + lay.tbn);
+    double2* hk = reinterpret_cast<double2*>(sraw + lay.hk);
+    double2* hp = reinterpret_cast<double2*>(sraw + lay.hp);
+    double* bcs = reinterpret_cast<double*>(sraw + lay.bcs);
+    double* vloc = reinterpret_cast<double*>(sraw + lay.vloc);
+    double* nbr = reinterpret_cast<double*>(sraw + lay.nbr);
+    const bool three = p.nbuf == 3;
+    const bool inverse = (P.mode & SPEC_INVERSE) != 0;
 
-    for (int q = tid; q < M1; q += nth) tw1[q] = twiddle<false>(q, M1);
-    for (int q = tid; q < M2; q += nth) tw2[q] = twiddle<false>(q, M2);
+    BB_PHASE(0);
+    // ---- twiddle tables precomputed by the engine: copied asynchronously
+    // (one contiguous block tw1 .. tbn of the layout), first group
+    if (P.twg) {
+        double2* dst = reinterpret_cast<double2*>(sraw + lay.tw1);
+        const int cnt = (lay.hk - lay.tw1) / 16;
+        for (int q = tid; q < cnt; q += nth) cp_async16(&dst[q], &P.twg[q]);
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    }
+    // ---- prefetch what later phases read from global memory
+    if (p.prefetch) {
+        if (P.mode & SPEC_MULTIPLY) {
+            for (int e = tid; e < per; e += nth) {
+                const int k = c * Br + e % Br + M1 * (e / Br);
+                cp_async16(&hk[e], &P.H[k]);
+                cp_async16(&hp[e], &P.H[k == 0 ? M : M - k]);
+            }
+        }
+        if (inverse && P.table) {
+            for (int e = tid; e < per; e += nth) {
+                const int64_t m = (int64_t)c * Bc + e % Bc + (int64_t)M2 * (e / Bc);
+                if (2 * m < P.n_out - 1) cp_async8(&bcs[2 * e], &P.bc[2 * m]);
+                if (2 * m + 1 < P.n_out - 1) cp_async8(&bcs[2 * e + 1], &P.bc[2 * m + 1]);
+            }
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    }
     const long long turn = P.turn ? *P.turn : 0;
+    double ind = 0.0;
+    if (P.ind_coeff) ind = P.ind_coeff[turn];
 
-    double2* rows = nullptr;  // row-phase buffer holding Z (forward) / U
-    double2* other = nullptr;
+    BB_PHASE(1);
+    // ---- twiddle tables (computed here unless they were copied)
+    if (!P.twg) fill_twiddles(p, tw1, tw2, tam, tbm, tan_, tbn, tid, nth);
+    // the copied tables must have landed before the first transform;
+    // the prefetch group (if any) may still be in flight
+    auto wait_twiddles = [&]() {
+        if (P.twg) {
+            if (p.prefetch) asm volatile("cp.async.wait_group 1;" ::: "memory");
+            else asm volatile("cp.async.wait_group 0;" ::: "memory");
+        }
+    };
+    // W_M^j and W_N^j (N = 2M) for 0 <= j < M from the two-level tables
+    auto twm = [&](long long j) { return cmul(tam[j / L], tbm[j % L]); };
+    auto twn = [&](long long j) { return cmul(tan_[j / L], tbn[j % L]); };
+
+    double2* rows = nullptr;   // row-phase buffer holding Z
+    double2* spare = nullptr;  // buffers that no other CTA reads right now
+    double2* spare2 = nullptr;
 
     if (P.mode & SPEC_FORWARD) {
+        BB_PHASE(2);
         // ---- load: z[m] = x[2m] + i x[2m+1], m = c Bc + b + M2 n1
         const int64_t nlim = P.n_in < (int64_t)p.N ? P.n_in : (int64_t)p.N;
         for (int e = tid; e < per; e += nth) {
@@ -250,7 +391,7 @@ spectral_kernel(const SpecParams P) {
                 if (i0 < nlim) x0 = P.in_f64[i0];
                 if (i1 < nlim) x1 = P.in_f64[i1];
             }
-            buf0[n1 * Bc + b] = make_double2(x0, x1);
+            buf[0][n1 * Bc + b] = make_double2(x0, x1);
         }
         // histogram bins beyond the transform length (profile longer than
         // n_fft): converted and cleared but not transformed
@@ -261,35 +402,54 @@ spectral_kernel(const SpecParams P) {
                 if (P.profile_out) P.profile_out[i] = x;
             }
         }
+        wait_twiddles();
         __syncthreads();
+        BB_PHASE(3);
         // ---- column transforms (length M1 over n1, Bc of them)
-        double2* colres = batch_fft<false>(buf0, buf1, M1, Bc, p.r1, p.n1, tw1);
-        double2* colfree = colres == buf0 ? buf1 : buf0;
-        cluster.sync();
-        // ---- transpose into rows with the four-step twiddle W_M^(n2 k1)
+        double2* r1 = batch_fft(buf[0], buf[1], M1, Bc, p.r1, p.n1, tw1, false);
+        double2* f1 = r1 == buf[0] ? buf[1] : buf[0];
+        cluster.sync();  // (A) every CTA's columns done
+        BB_PHASE(4);
+        // ---- transpose into rows with the four-step twiddle W_M^(n2 k1),
+        // written to a buffer nobody reads remotely
         for (int e = tid; e < Br * M2; e += nth) {
             const int n2 = e % M2, br = e / M2;
             const int k1 = c * Br + br;
             const int owner = n2 / Bc;
-            const double2* remote = cluster.map_shared_rank(colres, owner);
+            const double2* remote = cluster.map_shared_rank(r1, owner);
             double2 v = remote[k1 * Bc + (n2 - owner * Bc)];
             const long long ex = ((long long)n2 * k1) % M;
-            if (ex) v = cmul(v, twiddle<false>(ex, M));
-            colfree[n2 * Br + br] = v;
+            if (ex) v = cmul(v, twm(ex));
+            f1[n2 * Br + br] = v;
         }
-        cluster.sync();
-        // ---- row transforms (length M2 over n2, Br of them) -> Z[k1 + M1 k2]
-        rows = batch_fft<false>(colfree, colres, M2, Br, p.r2, p.n2, tw2);
-        other = rows == colfree ? colres : colfree;
-        cluster.sync();
+        // with two buffers the row transform would overwrite r1 while other
+        // CTAs may still read it
+        if (three) {
+            __syncthreads();
+            rows = batch_fft(f1, buf[2], M2, Br, p.r2, p.n2, tw2, false);
+            spare = rows == f1 ? buf[2] : f1;
+            spare2 = r1;
+        } else {
+            cluster.sync();
+            rows = batch_fft(f1, r1, M2, Br, p.r2, p.n2, tw2, false);
+            spare = rows == f1 ? r1 : f1;
+        }
+        cluster.sync();  // (C) Z complete everywhere
+        BB_PHASE(5);
+    } else {
+        wait_twiddles();
+        __syncthreads();  // twiddle tables
+        spare = buf[0];
+        spare2 = three ? buf[2] : nullptr;
     }
 
+    if (p.prefetch) asm volatile("cp.async.wait_group 0;" ::: "memory");
+    BB_PHASE(6);
+
+    double2* ubuf = nullptr;
     if (P.mode & (SPEC_OUT_SPECTRUM | SPEC_MULTIPLY | SPEC_IN_SPECTRUM)) {
-        if (!rows) {
-            rows = buf0;
-            other = buf1;
-        }
         // ---- spectral step on own k = k1 + M1 k2 with partner M - k
+        ubuf = spare;
         for (int e = tid; e < per; e += nth) {
             const int br = e % Br, k2 = e / Br;
             const int k1 = c * Br + br;
@@ -311,10 +471,9 @@ spectral_kernel(const SpecParams P) {
                 } else {
                     const double2 E = cscale(cadd(Zk, cconj(Zp)), 0.5);
                     const double2 O = crot<false>(cscale(csub(Zk, cconj(Zp)), 0.5));
-                    const double2 wk = twiddle<false>(k, 2LL * M);  // e^{-2 pi i k/N}
-                    const double2 wO = cmul(wk, O);
-                    Yk = cadd(E, wO);                 // X[k]
-                    Yp = cconj(csub(E, wO));          // X[M-k]
+                    const double2 wO = cmul(twn(k), O);  // e^{-2 pi i k/N} O
+                    Yk = cadd(E, wO);                    // X[k]
+                    Yp = cconj(csub(E, wO));             // X[M-k]
                 }
                 if (P.mode & SPEC_OUT_SPECTRUM) {
                     // every k < M is owned once; X[M] comes from k == 0
@@ -323,10 +482,12 @@ spectral_kernel(const SpecParams P) {
                 }
             }
             if (P.mode & SPEC_MULTIPLY) {
-                Yk = cmul(Yk, P.H[k]);
-                Yp = cmul(Yp, P.H[k == 0 ? M : M - k]);
+                const double2 Hk = p.prefetch ? hk[e] : P.H[k];
+                const double2 Hp = p.prefetch ? hp[e] : P.H[k == 0 ? M : M - k];
+                Yk = cmul(Yk, Hk);
+                Yp = cmul(Yp, Hp);
             }
-            if (P.mode & SPEC_INVERSE) {
+            if (inverse) {
                 double2 U;
                 if (k == 0) {
                     // irfft ignores the imaginary parts of Y[0] and Y[N/2]
@@ -334,26 +495,37 @@ spectral_kernel(const SpecParams P) {
                     U = make_double2(e0, o0);
                 } else {
                     const double2 Ye = cscale(cadd(Yk, cconj(Yp)), 0.5);
-                    const double2 Yo = cmul(twiddle<true>(k, 2LL * M),
-                                            cscale(csub(Yk, cconj(Yp)), 0.5));
+                    const double2 Yo = cmul(cconj(twn(k)), cscale(csub(Yk, cconj(Yp)), 0.5));
                     U = cadd(Ye, crot<true>(Yo));     // Ye + i Yo
                 }
-                other[k2 * Br + br] = U;
+                ubuf[k2 * Br + br] = U;
             }
         }
-        cluster.sync();
-        double2* t = rows;
-        rows = other;
-        other = t;
+    }
+    if (!inverse) {
+        cluster.sync();  // partners' reads of `rows` done before this CTA exits
+        return;
     }
 
-    if (!(P.mode & SPEC_INVERSE)) return;
-
-    // ---- inverse row transforms (length M2 over k2) -> B[k1][m2]
-    double2* rres = batch_fft<true>(rows, other, M2, Br, p.r2, p.n2, tw2);
-    double2* rfree = rres == rows ? other : rows;
-    cluster.sync();
+    // ---- inverse row transforms (length M2 over k2) -> B[k1][m2], never
+    // touching `rows`, which partners may still read (three buffers), or
+    // after a barrier (two)
+    double2* rres;
+    double2* rfree;
+    if (three || !rows) {
+        double2* other = three ? spare2 : buf[1];
+        __syncthreads();
+        rres = batch_fft(ubuf, other, M2, Br, p.r2, p.n2, tw2, true);
+        rfree = rres == ubuf ? other : ubuf;
+    } else {
+        cluster.sync();
+        rres = batch_fft(ubuf, rows, M2, Br, p.r2, p.n2, tw2, true);
+        rfree = rres == ubuf ? rows : ubuf;
+    }
+    cluster.sync();  // (E) every CTA's rows done
+    BB_PHASE(7);
     // ---- transpose into columns with the conjugate four-step twiddle
+    double2* cdst = (three && rows) ? rows : rfree;  // rows is free after (E)
     for (int e = tid; e < Bc * M1; e += nth) {
         const int k1 = e % M1, bcol = e / M1;
         const int m2 = c * Bc + bcol;
@@ -361,64 +533,86 @@ spectral_kernel(const SpecParams P) {
         const double2* remote = cluster.map_shared_rank(rres, owner);
         double2 v = remote[m2 * Br + (k1 - owner * Br)];
         const long long ex = ((long long)k1 * m2) % M;
-        if (ex) v = cmul(v, twiddle<true>(ex, M));
-        rfree[k1 * Bc + bcol] = v;
+        if (ex) v = cmul(v, cconj(twm(ex)));
+        cdst[k1 * Bc + bcol] = v;
     }
-    cluster.sync();
-    double2* cres = batch_fft<true>(rfree, rres, M1, Bc, p.r1, p.n1, tw1);
+    double2* cres;
+    if (three && rows) {
+        __syncthreads();
+        cres = batch_fft(cdst, rfree, M1, Bc, p.r1, p.n1, tw1, true);
+    } else {
+        cluster.sync();
+        cres = batch_fft(cdst, rres, M1, Bc, p.r1, p.n1, tw1, true);
+    }
 
+    BB_PHASE(8);
     // ---- real output y[2m], y[2m+1] with m = c Bc + b + M2 m1
-    double ind = 0.0;
-    if (P.ind_coeff) ind = P.ind_coeff[turn];
     const int64_t S = P.n_in;
+    auto value = [&](int64_t n, double y) {
+        double v = y * P.out_scale;
+        if (P.ind_coeff) {
+            // np.gradient(profile, dbc): central inside, one-sided at ends
+            double g;
+            if (S < 2) g = 0.0;
+            else if (n == 0) g = (P.profile_out[1] - P.profile_out[0]) / P.ind_dbc;
+            else if (n == S - 1) g = (P.profile_out[S - 1] - P.profile_out[S - 2]) / P.ind_dbc;
+            else g = (P.profile_out[n + 1] - P.profile_out[n - 1]) / (2.0 * P.ind_dbc);
+            v = v + ind * g;
+        }
+        return v;
+    };
     for (int e = tid; e < per; e += nth) {
         const int b = e % Bc, m1 = e / Bc;
         const int64_t m = (int64_t)c * Bc + b + (int64_t)M2 * m1;
         const double2 u = cres[m1 * Bc + b];
-        const double y2[2] = {u.x, u.y};
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int64_t n = 2 * m + h;
-            if (n >= P.n_out) continue;
-            double v = y2[h] * P.out_scale;
-            if (P.ind_coeff) {
-                // np.gradient(profile, dbc): central inside, one-sided at ends
-                double g;
-                if (S < 2) g = 0.0;
-                else if (n == 0) g = (P.profile_out[1] - P.profile_out[0]) / P.ind_dbc;
-                else if (n == S - 1) g = (P.profile_out[S - 1] - P.profile_out[S - 2]) / P.ind_dbc;
-                else g = (P.profile_out[n + 1] - P.profile_out[n - 1]) / (2.0 * P.ind_dbc);
-                v = v + ind * g;
+        const double v0 = value(2 * m, u.x), v1 = value(2 * m + 1, u.y);
+        if (2 * m < P.n_out) P.out[2 * m] = v0;
+        if (2 * m + 1 < P.n_out) P.out[2 * m + 1] = v1;
+        if (P.table) {
+            vloc[e] = v0;
+            // v0 is V[2(m-1)+2] for the element before m: hand it to the
+            // CTA that owns that element (first column of a CTA only)
+            if (b == 0 && m > 0) {
+                if (c > 0) cluster.map_shared_rank(nbr, c - 1)[m1] = v0;
+                else cluster.map_shared_rank(nbr, p.C - 1)[m1 - 1] = v0;
             }
-            P.out[n] = v;
         }
     }
+    // (G) the neighbour values have landed, and every CTA has finished
+    // reading the others' `rres` -- no CTA may exit before that
+    cluster.sync();
+    BB_PHASE(9);
     if (!P.table && !P.bump_turn) return;
-    cluster.sync();  // P.out visible cluster-wide
     if (P.table) {
         const int64_t nt = P.n_out - 1;
         for (int e = tid; e < per; e += nth) {
             const int b = e % Bc, m1 = e / Bc;
             const int64_t m = (int64_t)c * Bc + b + (int64_t)M2 * m1;
+            const double2 u = cres[m1 * Bc + b];
+            const double v0 = vloc[e];
+            const double v1 = value(2 * m + 1, u.y);
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 const int64_t n = 2 * m + h;
                 if (n >= nt) continue;
-                const double v0 = P.out[n], v1 = P.out[n + 1];
+                const double a0 = h == 0 ? v0 : v1;
+                const double a1 = h == 0 ? v1 : (b + 1 < Bc ? vloc[e + 1] : nbr[m1]);
+                const double bcn = p.prefetch ? bcs[2 * e + h] : P.bc[n];
                 if (!P.table_f32) {
                     // linear_interp_kick.cpp:44-47 with acc = 0
-                    const double slope = P.charge * (v1 - v0) * P.inv_w;
-                    const double offset = P.charge * v0 - P.bc[n] * slope;
+                    const double slope = P.charge * (a1 - a0) * P.inv_w;
+                    const double offset = P.charge * a0 - bcn * slope;
                     reinterpret_cast<double2*>(P.table)[n] = make_double2(slope, offset);
                 } else {
                     reinterpret_cast<float2*>(P.table)[n] =
-                        make_float2((float)(P.charge * v0),
-                                    (float)(P.charge * (v1 - v0) * P.inv_w));
+                        make_float2((float)(P.charge * a0),
+                                    (float)(P.charge * (a1 - a0) * P.inv_w));
                 }
             }
         }
     }
     if (P.bump_turn && c == 0 && tid == 0) *P.turn = turn + 1;
+    BB_PHASE(10);
 }
 
 #endif  // BB_SPECTRAL_KERNELS
@@ -431,5 +625,8 @@ int launch_spectral(const SpecParams& P, cudaStream_t stream);
 // Set spectral_kernel's launch attributes on the current device (idempotent;
 // call before a stream capture that will contain the kernel).
 int prepare_spectral();
+// Allocate (cudaMalloc) and fill the twiddle tables of a plan for
+// SpecParams::twg; the caller frees *out with cudaFree.  Synchronous.
+int make_spec_twiddles(const SpecPlan& plan, double2** out);
 
 }  // namespace bb

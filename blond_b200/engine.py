@@ -77,7 +77,7 @@ def _stream():
 class FusedTracker:
     def __init__(self, tracker, profile, total_induced_voltage=None,
                  precision: str = "f64", turns_per_graph: int = 50,
-                 threads: int = 0, blocks_per_sm: int = 0):
+                 threads: int = 0, blocks_per_sm: int = 0, kernel: str = "auto"):
         if precision not in PREC:
             raise ValueError(f"precision must be one of {list(PREC)}")
         if tracker.interpolation:
@@ -123,6 +123,14 @@ class FusedTracker:
         self.eng.call("bind_beam", ct.c_void_p(self.dt.data_ptr()),
                       ct.c_void_p(self.dE.data_ptr()), int(beam.n_macroparticles))
         self.eng.call("tune", int(threads), int(blocks_per_sm), int(turns_per_graph))
+        if kernel not in ("auto", "tma", "plain"):
+            raise ValueError("kernel must be 'auto', 'tma' or 'plain'")
+        if kernel == "auto":
+            # measured on the B200 (C2 workload): plain loads win for FP64
+            # (87 vs 107 us), the bulk-copy pipeline ties or wins for F32P64
+            kernel = "plain" if precision == "f64" else "tma"
+        self.kernel = kernel
+        self.eng.call("set_kernel", 0 if kernel == "tma" else 1)
         self.eng.call("set_turn", int(rf.counter[0]), _stream())
         self.eng.call("slice", _stream())
 
@@ -165,6 +173,15 @@ class FusedTracker:
         self.beam.energy = float(rf.energy[t])
         self.beam.momentum = float(rf.momentum[t])
 
+    def prepare(self):
+        """Build and upload the CUDA graph now (otherwise the first track()
+        of at least turns_per_graph turns builds it)."""
+        self.eng.call("prepare", _stream())
+
+    def check(self):
+        """Synchronise and raise if a kernel's bounded wait gave up."""
+        self.eng.call("check", _stream())
+
     def time_kernels(self, n_turns: int):
         """Track n_turns with CUDA events around each launch; returns the
         summed (head_ms, particles_ms).  Synchronises the current stream."""
@@ -176,6 +193,7 @@ class FusedTracker:
     def sync(self):
         """Copy the engine's profile (and induced voltage) into the drop-in
         objects, and the float32 energies back into beam.dE ('f32p64')."""
+        self.check()
         prof = torch.empty(self.profile.n_slices, dtype=torch.float64, device="cuda")
         self.eng.call("get_profile", ct.c_void_p(prof.data_ptr()), _stream())
         self.profile.n_macroparticles.copy_(prof)

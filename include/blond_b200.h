@@ -194,9 +194,20 @@ int blond_engine_bind_beam(blond_engine* engine, void* dt, void* dE,
 int blond_engine_set_turn(blond_engine* engine, int64_t turn, void* stream);
 /* Re-slice the bound beam into the profile (Profile.track()). */
 int blond_engine_slice(blond_engine* engine, void* stream);
+/* Capture and upload the CUDA graph of turns_per_graph turns now (it is
+ * otherwise built by the first blond_engine_run that needs it). */
+int blond_engine_prepare(blond_engine* engine, void* stream);
 /* Track n_turns fused turns; afterwards the profile holds the slices of the
  * final coordinates. */
 int blond_engine_run(blond_engine* engine, int64_t n_turns, void* stream);
+/* Synchronise `stream` and report a device-side failure of the runs so far:
+ * BLOND_ERR_TIMEOUT if a bounded wait in a kernel gave up (the coordinates
+ * are then not valid), else BLOND_OK.  Clears the flag. */
+int blond_engine_check(blond_engine* engine, void* stream);
+/* Particle-pass implementation: 0 = bulk-copy (TMA) pipelined (default;
+ * falls back to 1 when the profile is too long for its shared memory),
+ * 1 = plain loads. */
+int blond_engine_set_kernel(blond_engine* engine, int variant);
 /* Device copies of the current state (n_slices doubles each). */
 int blond_engine_get_profile(blond_engine* engine, double* profile,
                              void* stream);

@@ -109,7 +109,8 @@ FUSED = ["track_rf.npz", "track_exact.npz", "track_legacy.npz", "track_full.npz"
 
 @pytest.mark.parametrize("name", FUSED)
 @pytest.mark.parametrize("turns_per_graph", [1, 3])
-def test_fused_engine_matches_reference(cuda, name, turns_per_graph):
+@pytest.mark.parametrize("kernel", ["tma", "plain"])
+def test_fused_engine_matches_reference(cuda, name, turns_per_graph, kernel):
     g = golden(name)
     ring, rf, beam = build(g)
     prof = make_profile(g, beam)
@@ -117,7 +118,7 @@ def test_fused_engine_matches_reference(cuda, name, turns_per_graph):
     tiv = TotalInducedVoltage(beam, prof, ivs) if ivs else None
     tracker = RingAndRFTracker(rf, beam, solver=str(g["solver"][0]))
     fused = FusedTracker(tracker, prof, tiv, precision="f64",
-                         turns_per_graph=turns_per_graph)
+                         turns_per_graph=turns_per_graph, kernel=kernel)
     nt = int(g["n_turns"][0])
     np.testing.assert_array_equal(fused.profile_tensor().cpu().numpy(), g["profiles"][0])
     fused.track(nt - 1)
@@ -165,3 +166,65 @@ def test_fused_odd_particle_count_and_ragged_tail(cuda):
     assert normwise(beam.dt.cpu().numpy(), odt) < 1e-12
     assert normwise(beam.dE.cpu().numpy(), odE) < 1e-12
     np.testing.assert_array_equal(fused.profile_tensor().cpu().numpy(), oprof[-1])
+
+
+@pytest.mark.parametrize("n", [1, 1000, 2048, 2048 * 149 + 7, 2048 * 300 + 1])
+@pytest.mark.parametrize("kernel", ["tma", "plain"])
+def test_fused_chunk_boundaries(cuda, n, kernel):
+    """Particle counts below one 2048-particle chunk, exactly one chunk, more
+    chunks than SMs, and ragged tails, against the oracle (3 turns)."""
+    import cpu_oracle as o
+    from blond_b200.beam.distributions import _get_dE_from_dt, bigaussian_arrays
+    ring = Ring(6911.5, 1 / 18**2, 26e9, Proton(), 3)
+    rf = RFStation(ring, [4620], [4.5e6], [0.0])
+    centre = (rf.phi_s[0] - rf.phi_rf[0, 0]) / rf.omega_rf[0, 0]
+    dt0, dE0 = bigaussian_arrays(n, 0.4e-9, _get_dE_from_dt(ring, rf, 0.4e-9), centre, 7)
+    intensity = 2e6 * n  # the charge per macro-particle of the golden runs
+    beam = Beam(ring, n, intensity, dt=dt0, dE=dE0)
+    prof = Profile(beam, CutOptions(cut_left=centre - 1.25e-9, cut_right=centre + 1.25e-9,
+                                    n_slices=512))
+    iv = InducedVoltageFreq(beam, prof, [Resonators(5e6, 1e9, 1.0)])
+    tiv = TotalInducedVoltage(beam, prof, [iv])
+    fused = FusedTracker(RingAndRFTracker(rf, beam), prof, tiv, kernel=kernel,
+                         turns_per_graph=2)
+    fused.track(3)
+    fused.check()
+    odt, odE, oprof, _ = o.track_oracle(
+        dt0, dE0, ring, rf, (prof.cut_left, prof.cut_right), prof.bin_centers, 512, 3,
+        impedance=(iv.n_fft, iv.total_impedance.cpu().numpy()), intensity=intensity)
+    # normwise against the bunch's scale: a handful of particles can all sit
+    # near dE = 0, where a per-particle relative error means nothing
+    dt_scale = max(np.max(np.abs(odt)), 1e-9)
+    dE_scale = max(np.max(np.abs(odE)), 2e7)
+    assert np.max(np.abs(beam.dt.cpu().numpy() - odt)) / dt_scale < 1e-12
+    assert np.max(np.abs(beam.dE.cpu().numpy() - odE)) / dE_scale < 1e-12
+    np.testing.assert_array_equal(fused.profile_tensor().cpu().numpy(), oprof[-1])
+
+
+def test_fused_mixed_precision_bunch_statistics(cuda):
+    """F32P64 (dE float32, RF phase and drift in float64) vs the FP64
+    oracle after 200 turns: relative error of the rms bunch length and
+    energy spread within 1e-5 (the chosen form's bar)."""
+    import cpu_oracle as o
+    from blond_b200.beam.distributions import _get_dE_from_dt, bigaussian_arrays
+    n, turns = 200000, 200
+    ring = Ring(6911.5, 1 / 18**2, 26e9, Proton(), turns)
+    rf = RFStation(ring, [4620], [4.5e6], [0.0])
+    centre = (rf.phi_s[0] - rf.phi_rf[0, 0]) / rf.omega_rf[0, 0]
+    dt0, dE0 = bigaussian_arrays(n, 0.4e-9, _get_dE_from_dt(ring, rf, 0.4e-9), centre, 0)
+    beam = Beam(ring, n, 1e10, dt=dt0, dE=dE0)
+    prof = Profile(beam, CutOptions(cut_left=centre - 1.25e-9, cut_right=centre + 1.25e-9,
+                                    n_slices=1024))
+    iv = InducedVoltageFreq(beam, prof, [Resonators(5e6, 1e9, 1.0)])
+    tiv = TotalInducedVoltage(beam, prof, [iv])
+    fused = FusedTracker(RingAndRFTracker(rf, beam), prof, tiv, precision="f32p64")
+    fused.track(turns)
+    fused.sync()
+    odt, odE, _, _ = o.track_oracle(
+        dt0, dE0, ring, rf, (prof.cut_left, prof.cut_right), prof.bin_centers, 1024, turns,
+        impedance=(iv.n_fft, iv.total_impedance.cpu().numpy()), intensity=1e10)
+    dt, dE = beam.dt.cpu().numpy(), beam.dE.cpu().numpy()
+    inwin = lambda x: x[(odt > prof.cut_left) & (odt < prof.cut_right)]  # noqa: E731
+    for a, b in ((dt, odt), (dE, odE)):
+        assert abs(np.std(inwin(a)) / np.std(inwin(b)) - 1) < 1e-5
+
