@@ -25,8 +25,10 @@ def golden(name):
 
 def normwise(a, b):
     """max|a-b| / max|b| -- the parity measure for coordinates and voltages."""
-    a = np.asarray(a, dtype=np.float64)
-    b = np.asarray(b, dtype=np.float64)
+    a, b = np.asarray(a), np.asarray(b)
+    # complex arrays (spectra, impedances) are compared as complex numbers
+    t = np.complex128 if (np.iscomplexobj(a) or np.iscomplexobj(b)) else np.float64
+    a, b = a.astype(t), b.astype(t)
     den = np.max(np.abs(b))
     return float(np.max(np.abs(a - b)) / (den if den > 0 else 1.0))
 
