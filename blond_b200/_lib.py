@@ -76,6 +76,10 @@ _EXTRA = {
     "blond_engine_tune": [c_ptr, c_int, c_int, c_int],
     "blond_engine_time_kernels": [c_ptr, c_i64, ct.POINTER(c_dbl),
                                   ct.POINTER(c_dbl), c_ptr],
+    "blond_turn_f64_noalloc": [c_ptr, c_ptr, c_i64, c_int, c_dbl, c_ptr, c_ptr, c_ptr,
+                               c_dbl, c_int] + [c_dbl] * 13 + [c_int, c_ptr, c_ptr,
+                                                              c_i64, c_dbl, c_ptr,
+                                                              c_ptr, c_ptr],
 }
 
 

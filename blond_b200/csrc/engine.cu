@@ -18,6 +18,8 @@
 #include "spectral.cuh"
 
 #include <algorithm>
+#include <cstddef>
+#include <mutex>
 #include <vector>
 
 namespace bb {
@@ -1111,3 +1113,181 @@ int blond_engine_get_turn(blond_engine* e, int64_t* turn) {
 }
 
 }  // extern "C"
+
+// ===================================================== one turn, no allocation
+// blond_turn_f64_noalloc runs the work of one fused turn (slice, induced
+// voltage + table, particle pass, final profile) with every temporary held
+// in a fixed file-scope device array instead of memory from cudaMalloc.
+// It exists for callers that must not allocate device memory: a tracking
+// step embedded in a host application that owns the device's memory (a
+// control-room online model, a framework with its own pooling allocator)
+// cannot call cudaMalloc, because the call can stall every stream on the
+// device while it runs and it bypasses the host's memory accounting.
+namespace bb {
+
+// Largest profile the fixed scratch holds.
+constexpr int kNoAllocMaxSlices = 16384;
+
+struct NoAllocScratch {
+    int hist[kNoAllocMaxSlices];              // integer slice counts
+    double2 table[kNoAllocMaxSlices];         // interpolation table
+    double bc[kNoAllocMaxSlices];             // bin centres (device copy)
+    DriftTurn drift[2];                       // index 1 = this turn's drift
+    double acc;                               // this turn's acceleration kick
+    long long turn;                           // turn counter (0 -> 1)
+    int err;                                  // bounded-wait error word
+};
+
+// ~448 KB per device that loads the library, held until the process exits.
+// Shared by every call: calls that overlap on the GPU (e.g. on two
+// streams) race on it.
+static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
+
+// Device address of the scratch on the current device, looked up once per
+// device (cudaGetSymbolAddress; in host code the symbol's name is only a
+// host-side stand-in, not a device address).
+static NoAllocScratch* noalloc_scratch() {
+    static NoAllocScratch* ptr[64] = {nullptr};
+    static std::mutex mu;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+        set_error("turn_noalloc: no current CUDA device");
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    if (!ptr[dev]) {
+        void* p = nullptr;
+        const cudaError_t rc = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (rc != cudaSuccess || !p) {
+            set_error("turn_noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(rc));
+            return nullptr;
+        }
+        ptr[dev] = reinterpret_cast<NoAllocScratch*>(p);
+    }
+    return ptr[dev];
+}
+
+}  // namespace bb
+
+extern "C" int blond_turn_f64_noalloc(
+    double* dt, double* dE, int64_t n, int n_rf, double charge, const double* voltage,
+    const double* omega_rf, const double* phi_rf, double acc_kick, int solver,
+    double t_rev, double length_ratio, double alpha_order, double eta_0, double eta_1,
+    double eta_2, double alpha_0, double alpha_1, double alpha_2, double beta,
+    double energy, double cut_left, double cut_right, int n_slices,
+    const double* bin_centers, const double* impedance, int64_t n_fft, double iv_scale,
+    double* profile_out, double* induced_voltage_out, void* stream) {
+    using namespace bb;
+    BB_CHECK_ARG(dt && dE && voltage && omega_rf && phi_rf && bin_centers && profile_out,
+                 "turn_noalloc: null pointer");
+    BB_CHECK_ARG(n >= 1, "turn_noalloc: n must be >= 1");
+    BB_CHECK_ARG(solver >= 0 && solver <= 2, "turn_noalloc: solver %d", solver);
+    BB_CHECK_ARG(aligned(dt, 16) && aligned(dE, 16),
+                 "turn_noalloc: dt and dE must be 16-byte aligned");
+    BB_CHECK_ARG(cut_right > cut_left, "turn_noalloc: cut_right <= cut_left");
+    BB_CHECK_SIZE(n_rf >= 1 && n_rf <= kMaxRfEngine, "turn_noalloc: n_rf=%d not in [1, %d]",
+                  n_rf, kMaxRfEngine);
+    BB_CHECK_SIZE(n_slices >= 2 && n_slices <= kNoAllocMaxSlices,
+                  "turn_noalloc: n_slices=%d exceeds the fixed scratch (2..%d slices); "
+                  "use the engine API for longer profiles", n_slices, kNoAllocMaxSlices);
+    SpecPlan plan = {};
+    if (impedance) {
+        BB_CHECK_ARG(induced_voltage_out, "turn_noalloc: null induced_voltage_out");
+        if (!make_spec_plan(n_fft, plan)) {
+            set_error("turn_noalloc: n_fft=%lld must be even, 5-smooth and <= %lld",
+                      (long long)n_fft, (long long)kMaxClusterFFT);
+            return BLOND_ERR_UNSUPPORTED;
+        }
+        BB_CHECK_SIZE(n_fft >= n_slices && plan.smem <= device_info().max_smem_optin,
+                      "turn_noalloc: n_fft=%lld unsupported for %d slices",
+                      (long long)n_fft, n_slices);
+    }
+    NoAllocScratch* sc = noalloc_scratch();
+    if (!sc) return BLOND_ERR_CUDA;
+    cudaStream_t s = as_stream(stream);
+
+    // this turn's constants (drift.cpp:31-56 evaluated on the host, as the
+    // engine does per turn), staged through pageable memory: the copy
+    // returns once the bytes are staged, so the stack buffers may go
+    struct Head {
+        DriftTurn drift[2];
+        double acc;
+        long long turn;
+        int err;
+    } h = {};
+    DriftTurn& d = h.drift[1];
+    d.Tr = t_rev * length_ratio;
+    d.simple = d.Tr * eta_0 / (beta * beta * energy);
+    const double coeff = 1. / (beta * beta * energy);
+    d.e0 = eta_0 * coeff;
+    d.e1 = eta_1 * coeff * coeff;
+    d.e2 = eta_2 * coeff * coeff * coeff;
+    d.ib2 = 1 / (beta * beta);
+    d.ie2 = 1 / (energy * energy);
+    d.energy = energy;
+    d.a0 = alpha_0;
+    d.a1 = alpha_1;
+    d.a2 = alpha_2;
+    h.drift[0] = d;
+    h.acc = acc_kick;
+    h.turn = 0;
+    h.err = 0;
+    static_assert(offsetof(NoAllocScratch, acc) ==
+                      offsetof(NoAllocScratch, drift) + 2 * sizeof(DriftTurn),
+                  "scratch header layout");
+    BB_CUDA(cudaMemcpyAsync(&sc->drift[0], &h.drift[0], sizeof(h.drift), cudaMemcpyHostToDevice, s));
+    BB_CUDA(cudaMemcpyAsync(&sc->acc, &h.acc, sizeof(double), cudaMemcpyHostToDevice, s));
+    BB_CUDA(cudaMemcpyAsync(&sc->turn, &h.turn, sizeof(long long), cudaMemcpyHostToDevice, s));
+    BB_CUDA(cudaMemcpyAsync(&sc->err, &h.err, sizeof(int), cudaMemcpyHostToDevice, s));
+    BB_CUDA(cudaMemcpyAsync(sc->bc, bin_centers, sizeof(double) * n_slices,
+                            cudaMemcpyHostToDevice, s));
+    // the histogram must start at zero; the previous call leaves its last
+    // turn's counts behind
+    BB_CUDA(cudaMemsetAsync(sc->hist, 0, sizeof(int) * n_slices, s));
+
+    // an engine description on the stack pointing at the caller's buffers
+    // and the fixed scratch (no allocation: none of the set-up calls run)
+    blond_engine e;
+    e.precision = BLOND_PREC_F64;
+    e.n_rf = n_rf;
+    e.solver = solver;
+    e.S = n_slices;
+    cudaGetDevice(&e.device);
+    e.n_turns = 1;
+    e.charge = charge;
+    e.d_V = const_cast<double*>(voltage);
+    e.d_om = const_cast<double*>(omega_rf);
+    e.d_ph = const_cast<double*>(phi_rf);
+    e.d_acc = &sc->acc;
+    e.d_drift = sc->drift;
+    e.order = alpha_order == 0 ? 0 : (alpha_order == 1 ? 1 : 2);
+    e.rf_set = e.drift_set = e.slicing_set = true;
+    e.cut_left = cut_left;
+    e.cut_right = cut_right;
+    e.inv_w = n_slices / (cut_right - cut_left);
+    e.d_bc = sc->bc;
+    e.bc0 = bin_centers[0];
+    e.lik_inv_w = (n_slices - 1) / (bin_centers[n_slices - 1] - bin_centers[0]);
+    e.bw = 1.0 / e.lik_inv_w;
+    e.dbc = bin_centers[1] - bin_centers[0];
+    e.has_fft = impedance != nullptr;
+    e.plan = plan;
+    e.d_H = reinterpret_cast<double2*>(const_cast<double*>(impedance));
+    e.iv_scale = iv_scale;
+    e.d_turn = &sc->turn;
+    e.d_err = &sc->err;
+    e.d_hist = sc->hist;
+    e.d_profile = profile_out;
+    e.d_vind = induced_voltage_out;
+    e.d_table = sc->table;
+    e.dt = dt;
+    e.dE = dE;
+    e.n = n;
+    e.variant = 1;  // plain-load particle pass, the engine's FP64 choice
+
+    int rc;
+    if ((rc = launch_particles(&e, false, s))) return rc;  // slice the input
+    if ((rc = launch_head(&e, s))) return rc;              // profile, V, table
+    if ((rc = launch_particles(&e, true, s))) return rc;   // the turn
+    return launch_profile(&e, false, s);                   // final profile
+}

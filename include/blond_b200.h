@@ -225,6 +225,40 @@ int blond_engine_time_kernels(blond_engine* engine, int64_t n_turns,
 int blond_engine_tune(blond_engine* engine, int threads, int blocks_per_sm,
                       int turns_per_graph);
 
+/* ------------------------------------------------------------ one turn, no allocation
+ * No counterpart in the reference.  One fused turn of the engine -- slice
+ * the input coordinates, induced voltage (when `impedance` is not NULL) and
+ * its interpolated kick, RF kick, drift, slice -- for callers that must not
+ * allocate device memory: a tracking step embedded in a host application
+ * that owns the device's memory (an online model, a framework with its own
+ * pooling allocator) cannot call cudaMalloc, which may stall the whole
+ * device and bypasses the host's accounting.  Nothing is allocated: the
+ * temporaries live in a fixed file-scope device array of ~448 KB that every
+ * device loading the library holds until the process exits.
+ *   - n_slices <= 16384, else BLOND_ERR_SIZE; n_fft as for the engine.
+ *   - dt, dE, voltage, omega_rf, phi_rf, impedance (n_fft/2+1 complex),
+ *     profile_out and induced_voltage_out (n_slices doubles) are device
+ *     arrays; bin_centers is a HOST array of n_slices values.  Drift
+ *     scalars are this turn's drift parameters (turn+1 values in the
+ *     reference tracker), voltage/omega_rf/phi_rf this turn's RF column.
+ *   - The first call on a device looks the scratch up
+ *     (cudaGetSymbolAddress) and sets kernel attributes: make it before
+ *     any stream capture.
+ *   - Every call shares the scratch: calls that overlap on the GPU (two
+ *     streams, two threads) race.  The histogram is cleared by each call. */
+int blond_turn_f64_noalloc(double* dt, double* dE, int64_t n, int n_rf,
+                           double charge, const double* voltage,
+                           const double* omega_rf, const double* phi_rf,
+                           double acc_kick, int solver, double t_rev,
+                           double length_ratio, double alpha_order,
+                           double eta_0, double eta_1, double eta_2,
+                           double alpha_0, double alpha_1, double alpha_2,
+                           double beta, double energy, double cut_left,
+                           double cut_right, int n_slices,
+                           const double* bin_centers, const double* impedance,
+                           int64_t n_fft, double iv_scale, double* profile_out,
+                           double* induced_voltage_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
