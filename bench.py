@@ -66,11 +66,11 @@ def machine(n_turns: int):
     return ring, rf
 
 
-def host_bunch(ring, rf, n: int):
+def host_bunch(ring, rf, n: int, seed: int = 0):
     from blond_b200.beam.distributions import _get_dE_from_dt, bigaussian_arrays
     sdE = _get_dE_from_dt(ring, rf, 0.4e-9)
     centre = (rf.phi_s[0] - rf.phi_rf[0, 0]) / rf.omega_rf[0, 0]
-    dt, dE = bigaussian_arrays(n, 0.4e-9, sdE, centre, 0)
+    dt, dE = bigaussian_arrays(n, 0.4e-9, sdE, centre, seed)
     return dt, dE, centre
 
 
@@ -204,7 +204,11 @@ def barrier(world):
 
 
 # ----------------------------------------------------------------- our arm
-def build_fused(n, S, n_turns, precision, kernel="auto"):
+def build_fused(n, S, n_turns, precision, kernel="auto", seed=0, group=None):
+    """One beam of n macro-particles per GPU.  With a process group the GPUs
+    hold shards of ONE beam (seed = rank: independent samples of the same
+    bunch) whose histogram is summed every turn; the charge per
+    macro-particle (1e10 / 1e7) is the same in every configuration."""
     import torch
     from blond_b200.beam.beam import Beam
     from blond_b200.beam.profile import CutOptions, Profile
@@ -213,15 +217,15 @@ def build_fused(n, S, n_turns, precision, kernel="auto"):
     from blond_b200.impedances.impedance_sources import Resonators
     from blond_b200.trackers.tracker import RingAndRFTracker
     ring, rf = machine(n_turns)
-    dt, dE, centre = host_bunch(ring, rf, n)
-    beam = Beam(ring, n, 1e10, dt=dt, dE=dE, dtype=torch.float64)
+    dt, dE, centre = host_bunch(ring, rf, n, seed)
+    beam = Beam(ring, n, 1e10 * n / 1e7, dt=dt, dE=dE, dtype=torch.float64)
     cl, cr, _ = window(centre, S)
     prof = Profile(beam, CutOptions(cut_left=cl, cut_right=cr, n_slices=S))
     iv = InducedVoltageFreq(beam, prof, [Resonators(5e6, 1e9, 1.0)])
     tiv = TotalInducedVoltage(beam, prof, [iv])
     tracker = RingAndRFTracker(rf, beam)
     fused = FusedTracker(tracker, prof, tiv, precision=precision, turns_per_graph=50,
-                         kernel=kernel)
+                         kernel=kernel, process_group=group)
     return fused, beam, iv.n_fft
 
 
@@ -245,9 +249,15 @@ def run_ours(args, world, rank, local):
     kt = min(K, 20)
     E = args.e2e_steps
     total = W + K + kt + E + 4
-    fused, beam, n_fft = build_fused(n, S, total, args.precision, args.kernel)
+    group = None
+    if world > 1:
+        import torch.distributed as dist
+        group = dist.group.WORLD
+    fused, beam, n_fft = build_fused(n, S, total, args.precision, args.kernel, seed=rank,
+                                     group=group)
     fused.track(W)
-    fused.prepare()  # graph capture/upload outside the timed region
+    if group is None:
+        fused.prepare()  # graph capture/upload outside the timed region
     torch.cuda.synchronize()
     barrier(world)
     clocks = ClockSampler(local) if rank == 0 else None
@@ -290,7 +300,9 @@ def run_ours(args, world, rank, local):
         "config": {"workload": WORKLOAD, "particles": n, "slices": S, "n_fft": n_fft,
                    "intensity": 1e10, "turns_per_graph": 50,
                    "l2": f"inputs larger than L2: {alg_bytes // 2 / 1e6:.0f} MB of dt/dE read per turn",
-                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+                   "parallelism": (f"dp{world}: one beam of {world} x {n:.0e} particles, "
+                                   "int32 histogram all-reduce (NCCL) per turn")
+                   if world > 1 else "1 GPU"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": _traffic(args.precision, n),
                      "kernel": f"particle_kernel{'_tma' if fused.kernel == 'tma' else ''} "

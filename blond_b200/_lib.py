@@ -70,6 +70,8 @@ _EXTRA = {
     "blond_engine_prepare": [c_ptr, c_ptr],
     "blond_engine_check": [c_ptr, c_ptr],
     "blond_engine_set_kernel": [c_ptr, c_int],
+    "blond_engine_bind_histogram": [c_ptr, c_ptr],
+    "blond_engine_step": [c_ptr, c_int, c_ptr],
     "blond_engine_get_profile": [c_ptr, c_ptr, c_ptr],
     "blond_engine_get_induced_voltage": [c_ptr, c_ptr, c_ptr],
     "blond_engine_get_turn": [c_ptr, ct.POINTER(c_i64)],

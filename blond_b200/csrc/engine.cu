@@ -506,7 +506,8 @@ struct blond_engine {
     long long* d_turn = nullptr;
     int* d_err = nullptr;  // set by a kernel whose bounded wait gave up
     long long host_turn = 0;
-    int* d_hist = nullptr;
+    int* d_hist = nullptr;    // the histogram in use (own or caller-bound)
+    int* own_hist = nullptr;  // the one engine_create allocated
     double* d_profile = nullptr;
     double* d_vind = nullptr;
     void* d_table = nullptr;
@@ -761,6 +762,7 @@ int blond_engine_create(blond_engine** out, int precision, int n_rf, int solver,
         cudaMemset(e->d_turn, 0, sizeof(long long));
         cudaMemset(e->d_err, 0, sizeof(int));
         cudaMemset(e->d_hist, 0, sizeof(int) * n_slices);
+        e->own_hist = e->d_hist;
         cudaMemset(e->d_profile, 0, sizeof(double) * n_slices);
         cudaMemset(e->d_vind, 0, sizeof(double) * n_slices);
         cudaMemset(e->d_table, 0, sizeof(double2) * n_slices);
@@ -789,7 +791,7 @@ int blond_engine_destroy(blond_engine* e) {
     for (void* p : {(void*)e->d_V, (void*)e->d_om, (void*)e->d_ph, (void*)e->d_acc,
                     (void*)e->d_drift, (void*)e->d_bc, (void*)e->d_H, (void*)e->d_tw,
                     (void*)e->d_ind,
-                    (void*)e->d_turn, (void*)e->d_err, (void*)e->d_hist, (void*)e->d_profile,
+                    (void*)e->d_turn, (void*)e->d_err, (void*)e->own_hist, (void*)e->d_profile,
                     (void*)e->d_vind, e->d_table})
         free_ptr(p);
     delete e;
@@ -948,6 +950,28 @@ int blond_engine_slice(blond_engine* e, void* stream) {
     int rc = launch_particles(e, false, s);
     if (rc) return rc;
     return launch_profile(e, false, s);
+}
+
+int blond_engine_bind_histogram(blond_engine* e, int* hist) {
+    BB_CHECK_ARG(e, "engine_bind_histogram: null engine");
+    BB_CHECK_ARG(aligned(hist, 4), "engine_bind_histogram: misaligned histogram");
+    e->d_hist = hist ? hist : e->own_hist;
+    e->graph_dirty = true;
+    return BLOND_OK;
+}
+
+int blond_engine_step(blond_engine* e, int part, void* stream) {
+    BB_CHECK_ARG(e && part >= 1 && part <= 3, "engine_step: part must be 1, 2 or 3");
+    int rc = check_ready(e);
+    if (rc) return rc;
+    cudaStream_t s = as_stream(stream);
+    if (part == 3) return launch_profile(e, false, s);
+    BB_CHECK_SIZE(e->host_turn < e->n_turns, "engine_step: turn %lld beyond the programme",
+                  (long long)e->host_turn);
+    if (part == 1) return launch_head(e, s);
+    if ((rc = launch_particles(e, true, s))) return rc;
+    e->host_turn += 1;
+    return BLOND_OK;
 }
 
 int blond_engine_set_kernel(blond_engine* e, int variant) {

@@ -74,10 +74,36 @@ def _stream():
     return ct.c_void_p(torch.cuda.current_stream().cuda_stream)
 
 
+def start_sharded(slice_local, reduce, refresh):
+    """Initial profile of a beam split over ranks: slice the local
+    particles, sum the histogram over the ranks, convert it."""
+    slice_local()
+    reduce()
+    refresh()
+
+
+def run_sharded_turns(n_turns, head, particles, reduce, refresh):
+    """The turn loop of one beam split over ranks (the reference's MPI
+    layout: Beam.split, beam/beam.py:626-697, and the per-turn histogram
+    all-reduce of Profile.reduce_histo, beam/profile.py:721-762).
+
+    Per turn, in this order on every rank (so every rank issues the same
+    collectives): head() -- profile from the summed histogram, induced
+    voltage, interpolation table; particles() -- the local particles'
+    induced kick, RF kick, drift and deposit; reduce() -- sum the histogram
+    over the ranks.  refresh() converts the final summed histogram."""
+    for _ in range(int(n_turns)):
+        head()
+        particles()
+        reduce()
+    refresh()
+
+
 class FusedTracker:
     def __init__(self, tracker, profile, total_induced_voltage=None,
                  precision: str = "f64", turns_per_graph: int = 50,
-                 threads: int = 0, blocks_per_sm: int = 0, kernel: str = "auto"):
+                 threads: int = 0, blocks_per_sm: int = 0, kernel: str = "auto",
+                 process_group=None):
         if precision not in PREC:
             raise ValueError(f"precision must be one of {list(PREC)}")
         if tracker.interpolation:
@@ -132,7 +158,21 @@ class FusedTracker:
         self.kernel = kernel
         self.eng.call("set_kernel", 0 if kernel == "tma" else 1)
         self.eng.call("set_turn", int(rf.counter[0]), _stream())
-        self.eng.call("slice", _stream())
+        # sharded: this rank holds a part of the beam; the int32 histogram is
+        # summed over `process_group` after every particle pass.  The beam's
+        # ratio (intensity / macro-particles) must be the whole beam's.
+        self.group = process_group
+        if process_group is None:
+            self.eng.call("slice", _stream())
+        else:
+            self.hist = torch.zeros(S, dtype=torch.int32, device="cuda")
+            self.eng.call("bind_histogram", ct.c_void_p(self.hist.data_ptr()))
+            start_sharded(lambda: self.eng.call("slice", _stream()), self._reduce,
+                          lambda: self.eng.call("step", 3, _stream()))
+
+    def _reduce(self):
+        import torch.distributed as dist
+        dist.all_reduce(self.hist, op=dist.ReduceOp.SUM, group=self.group)
 
     def _set_impedance(self, tiv, beam, rf):
         Z = None
@@ -164,7 +204,12 @@ class FusedTracker:
 
     def track(self, n_turns: int = 1):
         """Advance n_turns; updates the RF counter and beam energy fields."""
-        self.eng.call("run", int(n_turns), _stream())
+        if self.group is None:
+            self.eng.call("run", int(n_turns), _stream())
+        else:
+            run_sharded_turns(n_turns, lambda: self.eng.call("step", 1, _stream()),
+                              lambda: self.eng.call("step", 2, _stream()), self._reduce,
+                              lambda: self.eng.call("step", 3, _stream()))
         rf = self.rf
         rf.counter[0] += int(n_turns)
         t = rf.counter[0]

@@ -221,6 +221,19 @@ int blond_engine_get_turn(blond_engine* engine, int64_t* turn_host);
 int blond_engine_time_kernels(blond_engine* engine, int64_t n_turns,
                               double* head_ms, double* particles_ms,
                               void* stream);
+/* Sharded tracking (one beam split over several GPUs; the exchange is the
+ * reference's MPI Profile.reduce_histo, beam/profile.py:721-762): bind a caller-
+ * owned int32 histogram of n_slices counts (NULL restores the engine's
+ * own), then drive the turns step by step and sum the histogram over the
+ * ranks (e.g. an NCCL all-reduce) after every particle step:
+ *   slice; all-reduce; step(3)              -- initial profile
+ *   repeat: step(1); step(2); all-reduce    -- one turn
+ *   step(3)                                 -- profile of the final turn
+ * part 1 = head (profile, induced voltage, table; clears the histogram),
+ * part 2 = particle pass of the current turn (advances the turn),
+ * part 3 = profile <- histogram. */
+int blond_engine_bind_histogram(blond_engine* engine, int* hist);
+int blond_engine_step(blond_engine* engine, int part, void* stream);
 /* Grid size and block size of the particle kernel (0 = automatic). */
 int blond_engine_tune(blond_engine* engine, int threads, int blocks_per_sm,
                       int turns_per_graph);

@@ -228,3 +228,39 @@ def test_fused_mixed_precision_bunch_statistics(cuda):
     for a, b in ((dt, odt), (dE, odE)):
         assert abs(np.std(inwin(a)) / np.std(inwin(b)) - 1) < 1e-5
 
+
+
+def test_fused_sharded_api_with_one_rank_matches_unsharded(cuda):
+    """The sharded step-by-step path (caller-owned histogram, NCCL
+    all-reduce after every particle pass) on a one-rank process group gives
+    the graph-replayed path's result bit for bit."""
+    import datetime
+    import socket
+    import torch.distributed as dist
+    g = golden("track_full.npz")
+    results = []
+    for sharded in (False, True):
+        ring, rf, beam = build(g)
+        prof = make_profile(g, beam)
+        tiv = TotalInducedVoltage(beam, prof, impedance_objects("track_full.npz", beam, prof, rf))
+        group = None
+        if sharded:
+            with socket.socket() as s:
+                s.bind(("127.0.0.1", 0))
+                port = s.getsockname()[1]
+            dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0,
+                                    world_size=1, timeout=datetime.timedelta(seconds=60))
+            group = dist.group.WORLD
+        try:
+            fused = FusedTracker(RingAndRFTracker(rf, beam), prof, tiv, process_group=group,
+                                 turns_per_graph=4)
+            fused.track(int(g["n_turns"][0]))
+            fused.check()
+            results.append((beam.dt.cpu().numpy(), beam.dE.cpu().numpy(),
+                            fused.profile_tensor().cpu().numpy()))
+        finally:
+            if sharded:
+                dist.destroy_process_group()
+    for a, b in zip(*results):
+        np.testing.assert_array_equal(a, b)
+    np.testing.assert_array_equal(results[1][2], g["profiles"][-1])
