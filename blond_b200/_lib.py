@@ -70,6 +70,19 @@ _EXTRA = {
     "blond_engine_prepare": [c_ptr, c_ptr],
     "blond_engine_check": [c_ptr, c_ptr],
     "blond_engine_set_kernel": [c_ptr, c_int],
+    "blond_batch_create": [ct.POINTER(c_ptr), c_int, c_int, c_int, c_int, c_int],
+    "blond_batch_destroy": [c_ptr],
+    "blond_batch_set_rf": [c_ptr, c_i64, c_ptr, c_ptr, c_ptr, c_ptr, c_dbl],
+    "blond_batch_set_drift": [c_ptr, c_dbl, c_dbl] + [c_ptr] * 9,
+    "blond_batch_set_slicing": [c_ptr, c_ptr, c_ptr, c_ptr],
+    "blond_batch_set_impedance": [c_ptr, c_i64, c_ptr, c_ptr],
+    "blond_batch_bind_beams": [c_ptr, c_ptr, c_ptr, c_ptr],
+    "blond_batch_set_turn": [c_ptr, c_i64, c_ptr],
+    "blond_batch_slice": [c_ptr, c_ptr],
+    "blond_batch_run": [c_ptr, c_i64, c_ptr],
+    "blond_batch_tune": [c_ptr, c_int],
+    "blond_batch_get_profiles": [c_ptr, c_ptr, c_ptr],
+    "blond_batch_get_induced_voltages": [c_ptr, c_ptr, c_ptr],
     "blond_engine_bind_histogram": [c_ptr, c_ptr],
     "blond_engine_step": [c_ptr, c_int, c_ptr],
     "blond_engine_get_profile": [c_ptr, c_ptr, c_ptr],

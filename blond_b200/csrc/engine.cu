@@ -1315,3 +1315,574 @@ extern "C" int blond_turn_f64_noalloc(
     if ((rc = launch_particles(&e, true, s))) return rc;   // the turn
     return launch_profile(&e, false, s);                   // final profile
 }
+
+// ============================================================ batched beams
+// Many independent beams (ragged particle counts, own RF programme, slicing
+// window and impedance each) tracked together: ONE particle launch and ONE
+// head launch per turn for the whole batch.  Particles are concatenated;
+// a chunk table cuts every beam into pieces of at most kBatchChunk
+// particles, each piece processed by one block with its beam's constants in
+// shared memory and a private shared-memory histogram flushed to the beam's
+// global histogram.  The head kernel runs one cluster per beam.  Each beam
+// follows exactly the arithmetic of the single-beam engine (track_pair).
+namespace bb {
+
+constexpr int kBatchChunk = 32768;
+constexpr int kBatchThreads = 512;
+
+struct BatchArgs {
+    void* dt;
+    void* dE;
+    const long long* chunk_start;
+    const int* chunk_beam;
+    const int* chunk_count;
+    int n_chunks;
+    int n_rf;
+    double charge;
+    const double* V;  // [B][n_turns+1][n_rf]
+    const double* om;
+    const double* ph;
+    const double* acc;          // [B][n_turns]
+    const DriftTurn* drift;     // [B][n_turns+1]
+    int64_t n_turns;
+    int order;
+    const long long* turn;
+    int S;
+    const double* cut_left;     // [B]
+    const double* inv_w;        // [B]
+    const double* bc0;          // [B]
+    const double* lik_inv_w;    // [B]
+    const double* bw;           // [B]
+    int* hist;                  // [B][S]
+    const void* table;          // [B][S]
+};
+
+template <int PREC, int SOLVER, bool LIK, bool KICK>
+__global__ void __launch_bounds__(kBatchThreads, 2)
+particle_kernel_batch(const BatchArgs a) {
+    using E = typename Coord<PREC>::E;
+    extern __shared__ int sh[];
+    __shared__ TurnConsts c;
+    long long t = a.turn ? (*a.turn - 1) : 0;
+    if (t < 0) t = 0;
+    if (t >= a.n_turns) t = a.n_turns - 1;
+    double* dt = reinterpret_cast<double*>(a.dt);
+    E* dE = reinterpret_cast<E*>(a.dE);
+    const int S = a.S;
+    for (int ch = blockIdx.x; ch < a.n_chunks; ch += gridDim.x) {
+        const int b = a.chunk_beam[ch];
+        const long long start = a.chunk_start[ch];
+        const int count = a.chunk_count[ch];
+        if (KICK) {
+            const long long rb = (long long)b * (a.n_turns + 1);
+            for (int j = threadIdx.x; j < a.n_rf; j += blockDim.x) {
+                c.V[j] = a.V[(rb + t) * a.n_rf + j];
+                c.Vf[j] = (float)c.V[j];
+                c.om[j] = a.om[(rb + t) * a.n_rf + j];
+                c.ph[j] = a.ph[(rb + t) * a.n_rf + j];
+            }
+            if (threadIdx.x == 0) {
+                c.acc = a.acc[(long long)b * a.n_turns + t];
+                c.d = a.drift[rb + t + 1];
+            }
+        }
+        for (int k = threadIdx.x; k < S; k += blockDim.x) sh[k] = 0;
+        __syncthreads();
+        ParticleArgs pa = {};
+        pa.n_rf = a.n_rf;
+        pa.charge = a.charge;
+        pa.S = S;
+        pa.bc0 = a.bc0[b];
+        pa.lik_inv_w = a.lik_inv_w[b];
+        pa.bw = a.bw[b];
+        pa.table = LIK ? static_cast<const char*>(a.table) +
+                             (long long)b * S * (PREC == PREC_F64 ? 16 : 8)
+                       : nullptr;
+        const double cl = a.cut_left[b], iw = a.inv_w[b];
+        for (int i = threadIdx.x; i < count; i += 2 * blockDim.x) {
+            const int i2 = i + blockDim.x;
+            const bool two = i2 < count;
+            double t0 = dt[start + i], t1 = two ? dt[start + i2] : t0;
+            E e0 = dE[start + i], e1 = two ? dE[start + i2] : e0;
+            if (KICK) {
+                track_pair<PREC, SOLVER, LIK>(t0, t1, e0, e1, c, pa, a.order);
+                dt[start + i] = t0;
+                dE[start + i] = e0;
+                if (two) {
+                    dt[start + i2] = t1;
+                    dE[start + i2] = e1;
+                }
+            }
+            const int b0 = engine_bin(t0, cl, iw, S);
+            if (b0 >= 0) atomicAdd(&sh[b0], 1);
+            if (two) {
+                const int b1 = engine_bin(t1, cl, iw, S);
+                if (b1 >= 0) atomicAdd(&sh[b1], 1);
+            }
+        }
+        __syncthreads();
+        for (int k = threadIdx.x; k < S; k += blockDim.x) {
+            const int v = sh[k];
+            if (v) atomicAdd(&a.hist[(long long)b * S + k], v);
+        }
+        __syncthreads();  // shared histogram and constants are reused
+    }
+}
+
+}  // namespace bb
+
+struct blond_batch {
+    int precision = 0, B = 0, n_rf = 0, solver = 0, S = 0, device = 0;
+    int64_t n_turns = 0;
+    double charge = 1.0;
+    int order = 0;
+    double* d_V = nullptr;
+    double* d_om = nullptr;
+    double* d_ph = nullptr;
+    double* d_acc = nullptr;
+    bb::DriftTurn* d_drift = nullptr;
+    long long* d_chunk_start = nullptr;
+    int* d_chunk_beam = nullptr;
+    int* d_chunk_count = nullptr;
+    int n_chunks = 0;
+    double* d_cl = nullptr;
+    double* d_inv_w = nullptr;
+    double* d_bc0 = nullptr;
+    double* d_lik_inv_w = nullptr;
+    double* d_bw = nullptr;
+    double* d_bc = nullptr;
+    bool has_fft = false;
+    bb::SpecPlan plan = {};
+    double2* d_H = nullptr;
+    double* d_scale = nullptr;
+    double2* d_tw = nullptr;
+    int* d_hist = nullptr;
+    double* d_profile = nullptr;
+    double* d_vind = nullptr;
+    void* d_table = nullptr;
+    long long* d_turn = nullptr;
+    long long host_turn = 0;
+    void* dt = nullptr;
+    void* dE = nullptr;
+    int64_t n_total = 0;
+    bool rf_set = false, drift_set = false, slicing_set = false;
+    int turns_per_graph = 50;
+    cudaStream_t cap_stream = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    int graph_turns = 0;
+    bool graph_dirty = true;
+};
+
+namespace bb {
+
+static BatchArgs batch_args(blond_batch* q) {
+    BatchArgs a = {};
+    a.dt = q->dt;
+    a.dE = q->dE;
+    a.chunk_start = q->d_chunk_start;
+    a.chunk_beam = q->d_chunk_beam;
+    a.chunk_count = q->d_chunk_count;
+    a.n_chunks = q->n_chunks;
+    a.n_rf = q->n_rf;
+    a.charge = q->charge;
+    a.V = q->d_V;
+    a.om = q->d_om;
+    a.ph = q->d_ph;
+    a.acc = q->d_acc;
+    a.drift = q->d_drift;
+    a.n_turns = q->n_turns;
+    a.order = q->order;
+    a.turn = q->d_turn;
+    a.S = q->S;
+    a.cut_left = q->d_cl;
+    a.inv_w = q->d_inv_w;
+    a.bc0 = q->d_bc0;
+    a.lik_inv_w = q->d_lik_inv_w;
+    a.bw = q->d_bw;
+    a.hist = q->d_hist;
+    a.table = q->d_table;
+    return a;
+}
+
+template <int PREC, int SOLVER, bool LIK, bool KICK>
+static int launch_batch_t(blond_batch* q, cudaStream_t s, bool launch) {
+    static bool done[64] = {false};
+    auto k = particle_kernel_batch<PREC, SOLVER, LIK, KICK>;
+    int rc;
+    if ((rc = allow_max_smem(k, done))) return rc;
+    if (!launch) return BLOND_OK;
+    const int smem = (int)sizeof(int) * q->S;
+    const int grid = std::max(1, std::min(q->n_chunks, device_info().sm_count * 2));
+    k<<<grid, kBatchThreads, smem, s>>>(batch_args(q));
+    BB_LAUNCH_CHECK();
+    return BLOND_OK;
+}
+
+template <int PREC>
+static int launch_batch_p(blond_batch* q, bool kick, cudaStream_t s, bool launch) {
+    if (!kick) return launch_batch_t<PREC, 0, false, false>(q, s, launch);
+    const bool lik = q->has_fft;
+    switch (q->solver) {
+        case 0:
+            return lik ? launch_batch_t<PREC, 0, true, true>(q, s, launch)
+                       : launch_batch_t<PREC, 0, false, true>(q, s, launch);
+        case 1:
+            return lik ? launch_batch_t<PREC, 1, true, true>(q, s, launch)
+                       : launch_batch_t<PREC, 1, false, true>(q, s, launch);
+        default:
+            return lik ? launch_batch_t<PREC, 2, true, true>(q, s, launch)
+                       : launch_batch_t<PREC, 2, false, true>(q, s, launch);
+    }
+}
+
+static int launch_batch(blond_batch* q, bool kick, cudaStream_t s, bool launch = true) {
+    if (q->precision == BLOND_PREC_F64) return launch_batch_p<PREC_F64>(q, kick, s, launch);
+    return launch_batch_p<PREC_F32P64>(q, kick, s, launch);
+}
+
+static int launch_batch_profile(blond_batch* q, bool clear, cudaStream_t s) {
+    const int total = q->B * q->S;
+    const int threads = 256;
+    const int grid = std::min(1024, (total + threads - 1) / threads);
+    profile_kernel<<<grid, threads, 0, s>>>(q->d_hist, q->d_profile, total, clear ? 1 : 0,
+                                            clear ? q->d_turn : nullptr);
+    BB_LAUNCH_CHECK();
+    return BLOND_OK;
+}
+
+static int launch_batch_head(blond_batch* q, cudaStream_t s) {
+    if (!q->has_fft) return launch_batch_profile(q, true, s);
+    SpecParams P = {};
+    P.p = q->plan;
+    P.mode = SPEC_FORWARD | SPEC_MULTIPLY | SPEC_INVERSE;
+    P.in_i32 = q->d_hist;
+    P.n_in = q->S;
+    P.profile_out = q->d_profile;
+    P.H = q->d_H;
+    P.out = q->d_vind;
+    P.n_out = q->S;
+    P.table = q->d_table;
+    P.table_f32 = q->precision == BLOND_PREC_F32P64;
+    P.charge = q->charge;
+    P.bc = q->d_bc;
+    P.turn = q->d_turn;
+    P.bump_turn = 1;
+    P.twg = q->d_tw;
+    P.batch = q->B;
+    P.beam_scale = q->d_scale;
+    P.beam_inv_w = q->d_lik_inv_w;
+    return launch_spectral(P, s);
+}
+
+static int batch_ready(blond_batch* q) {
+    if (!q->rf_set || !q->drift_set || !q->slicing_set || !q->dt) {
+        set_error("batch: set_rf, set_drift, set_slicing and bind_beams must all be called "
+                  "before tracking");
+        return BLOND_ERR_STATE;
+    }
+    return BLOND_OK;
+}
+
+static int batch_turn(blond_batch* q, cudaStream_t s) {
+    int rc = launch_batch_head(q, s);
+    if (rc) return rc;
+    return launch_batch(q, true, s);
+}
+
+}  // namespace bb
+
+extern "C" {
+
+int blond_batch_create(blond_batch** out, int precision, int n_beams, int n_rf, int solver,
+                       int n_slices) {
+    using namespace bb;
+    BB_CHECK_ARG(out, "batch_create: null output");
+    BB_CHECK_ARG(precision == BLOND_PREC_F64 || precision == BLOND_PREC_F32P64,
+                 "batch_create: unknown precision %d", precision);
+    BB_CHECK_SIZE(n_beams >= 1, "batch_create: n_beams must be >= 1");
+    BB_CHECK_SIZE(n_rf >= 1 && n_rf <= kMaxRfEngine, "batch_create: n_rf=%d", n_rf);
+    BB_CHECK_ARG(solver >= 0 && solver <= 2, "batch_create: solver %d", solver);
+    const int max_s = (device_info().max_smem_optin - (int)sizeof(TurnConsts) - 1024) / 8;
+    BB_CHECK_SIZE(n_slices >= 2 && n_slices <= max_s, "batch_create: n_slices=%d not in [2, %d]",
+                  n_slices, max_s);
+    blond_batch* q = new blond_batch();
+    q->precision = precision;
+    q->B = n_beams;
+    q->n_rf = n_rf;
+    q->solver = solver;
+    q->S = n_slices;
+    cudaGetDevice(&q->device);
+    const size_t bs = (size_t)n_beams * n_slices;
+    int rc = BLOND_OK;
+    if (cudaMalloc(&q->d_turn, sizeof(long long)) != cudaSuccess ||
+        cudaMalloc(&q->d_hist, sizeof(int) * bs) != cudaSuccess ||
+        cudaMalloc(&q->d_profile, sizeof(double) * bs) != cudaSuccess ||
+        cudaMalloc(&q->d_vind, sizeof(double) * bs) != cudaSuccess ||
+        cudaMalloc(&q->d_table, sizeof(double2) * bs) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&q->cap_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        set_error("batch_create: allocation failed");
+        rc = BLOND_ERR_CUDA;
+    } else {
+        cudaMemset(q->d_turn, 0, sizeof(long long));
+        cudaMemset(q->d_hist, 0, sizeof(int) * bs);
+        cudaMemset(q->d_profile, 0, sizeof(double) * bs);
+        cudaMemset(q->d_vind, 0, sizeof(double) * bs);
+        cudaMemset(q->d_table, 0, sizeof(double2) * bs);
+        if (cudaDeviceSynchronize() != cudaSuccess) {
+            set_error("batch_create: device error");
+            rc = BLOND_ERR_CUDA;
+        }
+    }
+    if (rc) {
+        blond_batch_destroy(q);
+        return rc;
+    }
+    *out = q;
+    return BLOND_OK;
+}
+
+int blond_batch_destroy(blond_batch* q) {
+    using namespace bb;
+    if (!q) return BLOND_OK;
+    if (q->graph) cudaGraphExecDestroy(q->graph);
+    if (q->cap_stream) cudaStreamDestroy(q->cap_stream);
+    for (void* p : {(void*)q->d_V, (void*)q->d_om, (void*)q->d_ph, (void*)q->d_acc,
+                    (void*)q->d_drift, (void*)q->d_chunk_start, (void*)q->d_chunk_beam,
+                    (void*)q->d_chunk_count, (void*)q->d_cl, (void*)q->d_inv_w,
+                    (void*)q->d_bc0, (void*)q->d_lik_inv_w, (void*)q->d_bw, (void*)q->d_bc,
+                    (void*)q->d_H, (void*)q->d_scale, (void*)q->d_tw, (void*)q->d_hist,
+                    (void*)q->d_profile, (void*)q->d_vind, q->d_table, (void*)q->d_turn})
+        free_ptr(p);
+    delete q;
+    return BLOND_OK;
+}
+
+int blond_batch_set_rf(blond_batch* q, int64_t n_turns, const double* V, const double* om,
+                       const double* ph, const double* acc, double charge) {
+    using namespace bb;
+    BB_CHECK_ARG(q && V && om && ph && acc && n_turns >= 1, "batch_set_rf: bad argument");
+    const size_t cols = (size_t)q->B * (n_turns + 1) * q->n_rf;
+    int rc;
+    if ((rc = upload((void**)&q->d_V, V, sizeof(double) * cols))) return rc;
+    if ((rc = upload((void**)&q->d_om, om, sizeof(double) * cols))) return rc;
+    if ((rc = upload((void**)&q->d_ph, ph, sizeof(double) * cols))) return rc;
+    if ((rc = upload((void**)&q->d_acc, acc, sizeof(double) * q->B * n_turns))) return rc;
+    q->n_turns = n_turns;
+    q->charge = charge;
+    q->rf_set = true;
+    q->graph_dirty = true;
+    return BLOND_OK;
+}
+
+int blond_batch_set_drift(blond_batch* q, double length_ratio, double alpha_order,
+                          const double* t_rev, const double* eta_0, const double* eta_1,
+                          const double* eta_2, const double* alpha_0, const double* alpha_1,
+                          const double* alpha_2, const double* beta, const double* energy) {
+    using namespace bb;
+    BB_CHECK_ARG(q && t_rev && eta_0 && eta_1 && eta_2 && alpha_0 && alpha_1 && alpha_2 &&
+                     beta && energy && q->rf_set,
+                 "batch_set_drift: bad argument (set_rf first)");
+    const size_t nt = (size_t)q->n_turns + 1, total = nt * q->B;
+    std::vector<DriftTurn> h(total);
+    for (size_t i = 0; i < total; ++i) {
+        // drift.cpp:31-56, as blond_engine_set_drift
+        DriftTurn d = {};
+        d.Tr = t_rev[i] * length_ratio;
+        d.simple = d.Tr * eta_0[i] / (beta[i] * beta[i] * energy[i]);
+        const double coeff = 1. / (beta[i] * beta[i] * energy[i]);
+        d.e0 = eta_0[i] * coeff;
+        d.e1 = eta_1[i] * coeff * coeff;
+        d.e2 = eta_2[i] * coeff * coeff * coeff;
+        d.ib2 = 1 / (beta[i] * beta[i]);
+        d.ie2 = 1 / (energy[i] * energy[i]);
+        d.energy = energy[i];
+        d.a0 = alpha_0[i];
+        d.a1 = alpha_1[i];
+        d.a2 = alpha_2[i];
+        h[i] = d;
+    }
+    q->order = alpha_order == 0 ? 0 : (alpha_order == 1 ? 1 : 2);
+    int rc = upload((void**)&q->d_drift, h.data(), sizeof(DriftTurn) * total);
+    if (rc) return rc;
+    q->drift_set = true;
+    q->graph_dirty = true;
+    return BLOND_OK;
+}
+
+int blond_batch_set_slicing(blond_batch* q, const double* cut_left, const double* cut_right,
+                            const double* bc) {
+    using namespace bb;
+    BB_CHECK_ARG(q && cut_left && cut_right && bc, "batch_set_slicing: null pointer");
+    const int B = q->B, S = q->S;
+    std::vector<double> cl(B), iw(B), b0(B), liw(B), bw(B);
+    for (int b = 0; b < B; ++b) {
+        BB_CHECK_ARG(cut_right[b] > cut_left[b], "batch_set_slicing: beam %d cut_right <= "
+                     "cut_left", b);
+        const double* c = bc + (size_t)b * S;
+        cl[b] = cut_left[b];
+        iw[b] = S / (cut_right[b] - cut_left[b]);             // histogram.cpp:30
+        b0[b] = c[0];
+        liw[b] = (S - 1) / (c[S - 1] - c[0]);                 // linear_interp_kick.cpp:31-33
+        bw[b] = 1.0 / liw[b];
+    }
+    int rc;
+    if ((rc = upload((void**)&q->d_cl, cl.data(), sizeof(double) * B))) return rc;
+    if ((rc = upload((void**)&q->d_inv_w, iw.data(), sizeof(double) * B))) return rc;
+    if ((rc = upload((void**)&q->d_bc0, b0.data(), sizeof(double) * B))) return rc;
+    if ((rc = upload((void**)&q->d_lik_inv_w, liw.data(), sizeof(double) * B))) return rc;
+    if ((rc = upload((void**)&q->d_bw, bw.data(), sizeof(double) * B))) return rc;
+    if ((rc = upload((void**)&q->d_bc, bc, sizeof(double) * (size_t)B * S))) return rc;
+    q->slicing_set = true;
+    q->graph_dirty = true;
+    return BLOND_OK;
+}
+
+int blond_batch_set_impedance(blond_batch* q, int64_t n_fft, const double* Z,
+                              const double* scale) {
+    using namespace bb;
+    BB_CHECK_ARG(q && Z && scale, "batch_set_impedance: null pointer");
+    SpecPlan plan;
+    if (!make_spec_plan(n_fft, plan)) {
+        set_error("batch_set_impedance: n_fft=%lld must be even, 5-smooth and <= %lld",
+                  (long long)n_fft, (long long)kMaxClusterFFT);
+        return BLOND_ERR_UNSUPPORTED;
+    }
+    BB_CHECK_SIZE(n_fft >= q->S && plan.smem <= device_info().max_smem_optin,
+                  "batch_set_impedance: n_fft=%lld unsupported for %d slices",
+                  (long long)n_fft, q->S);
+    std::vector<double> sc(q->B);
+    for (int b = 0; b < q->B; ++b) sc[b] = -scale[b] / (double)plan.M;
+    int rc;
+    if ((rc = upload((void**)&q->d_H, Z, sizeof(double2) * (size_t)q->B * (n_fft / 2 + 1))))
+        return rc;
+    if ((rc = upload((void**)&q->d_scale, sc.data(), sizeof(double) * q->B))) return rc;
+    free_ptr(q->d_tw);
+    q->d_tw = nullptr;
+    if ((rc = make_spec_twiddles(plan, &q->d_tw))) return rc;
+    q->plan = plan;
+    q->has_fft = true;
+    q->graph_dirty = true;
+    return BLOND_OK;
+}
+
+int blond_batch_bind_beams(blond_batch* q, void* dt, void* dE, const int64_t* offsets) {
+    using namespace bb;
+    BB_CHECK_ARG(q && dt && dE && offsets, "batch_bind_beams: null pointer");
+    BB_CHECK_ARG(aligned(dt, 8) && aligned(dE, 8), "batch_bind_beams: misaligned arrays");
+    std::vector<long long> cs;
+    std::vector<int> cb, cc;
+    for (int b = 0; b < q->B; ++b) {
+        BB_CHECK_ARG(offsets[b + 1] >= offsets[b], "batch_bind_beams: offsets decrease");
+        for (int64_t s0 = offsets[b]; s0 < offsets[b + 1]; s0 += kBatchChunk) {
+            cs.push_back(s0);
+            cb.push_back(b);
+            cc.push_back((int)std::min<int64_t>(kBatchChunk, offsets[b + 1] - s0));
+        }
+    }
+    int rc;
+    q->n_chunks = (int)cs.size();
+    if (q->n_chunks) {
+        if ((rc = upload((void**)&q->d_chunk_start, cs.data(), sizeof(long long) * cs.size())))
+            return rc;
+        if ((rc = upload((void**)&q->d_chunk_beam, cb.data(), sizeof(int) * cb.size()))) return rc;
+        if ((rc = upload((void**)&q->d_chunk_count, cc.data(), sizeof(int) * cc.size())))
+            return rc;
+    }
+    q->dt = dt;
+    q->dE = dE;
+    q->n_total = offsets[q->B];
+    q->graph_dirty = true;
+    return BLOND_OK;
+}
+
+int blond_batch_set_turn(blond_batch* q, int64_t turn, void* stream) {
+    using namespace bb;
+    BB_CHECK_ARG(q && turn >= 0, "batch_set_turn: bad argument");
+    const long long t = turn;
+    BB_CUDA(cudaMemcpyAsync(q->d_turn, &t, sizeof(t), cudaMemcpyHostToDevice,
+                            as_stream(stream)));
+    BB_CUDA(cudaStreamSynchronize(as_stream(stream)));
+    q->host_turn = turn;
+    return BLOND_OK;
+}
+
+int blond_batch_slice(blond_batch* q, void* stream) {
+    using namespace bb;
+    BB_CHECK_ARG(q, "batch_slice: null batch");
+    int rc = batch_ready(q);
+    if (rc) return rc;
+    cudaStream_t s = as_stream(stream);
+    BB_CUDA(cudaMemsetAsync(q->d_hist, 0, sizeof(int) * (size_t)q->B * q->S, s));
+    if ((rc = launch_batch(q, false, s))) return rc;
+    return launch_batch_profile(q, false, s);
+}
+
+int blond_batch_run(blond_batch* q, int64_t n_turns, void* stream) {
+    using namespace bb;
+    BB_CHECK_ARG(q && n_turns >= 0, "batch_run: bad argument");
+    int rc = batch_ready(q);
+    if (rc) return rc;
+    BB_CHECK_SIZE(q->host_turn + n_turns <= q->n_turns,
+                  "batch_run: turns exceed the programme (%lld turns)", (long long)q->n_turns);
+    if (n_turns == 0) return BLOND_OK;
+    cudaStream_t s = as_stream(stream);
+    const int K = q->turns_per_graph;
+    int64_t done = 0;
+    if (n_turns >= K && K > 1) {
+        if (q->graph_dirty || !q->graph) {
+            if ((rc = launch_batch(q, true, s, false))) return rc;
+            if (q->has_fft && (rc = prepare_spectral())) return rc;
+            if (q->graph) cudaGraphExecDestroy(q->graph);
+            q->graph = nullptr;
+            cudaGraph_t g;
+            BB_CUDA(cudaStreamBeginCapture(q->cap_stream, cudaStreamCaptureModeThreadLocal));
+            int lrc = BLOND_OK;
+            for (int i = 0; i < K && lrc == BLOND_OK; ++i) lrc = batch_turn(q, q->cap_stream);
+            cudaError_t ce = cudaStreamEndCapture(q->cap_stream, &g);
+            if (lrc) return lrc;
+            if (ce != cudaSuccess) {
+                set_error("batch_run: graph capture failed: %s", cudaGetErrorString(ce));
+                return BLOND_ERR_CUDA;
+            }
+            ce = cudaGraphInstantiate(&q->graph, g, 0);
+            cudaGraphDestroy(g);
+            if (ce != cudaSuccess) {
+                set_error("batch_run: graph instantiation failed: %s", cudaGetErrorString(ce));
+                return BLOND_ERR_CUDA;
+            }
+            BB_CUDA(cudaGraphUpload(q->graph, s));
+            q->graph_turns = K;
+            q->graph_dirty = false;
+        }
+        for (; done + K <= n_turns; done += K) BB_CUDA(cudaGraphLaunch(q->graph, s));
+    }
+    for (; done < n_turns; ++done)
+        if ((rc = batch_turn(q, s))) return rc;
+    q->host_turn += n_turns;
+    return launch_batch_profile(q, false, s);
+}
+
+int blond_batch_tune(blond_batch* q, int turns_per_graph) {
+    BB_CHECK_ARG(q && turns_per_graph >= 0, "batch_tune: bad argument");
+    if (turns_per_graph) q->turns_per_graph = turns_per_graph;
+    q->graph_dirty = true;
+    return BLOND_OK;
+}
+
+int blond_batch_get_profiles(blond_batch* q, double* out, void* stream) {
+    using namespace bb;
+    BB_CHECK_ARG(q && out, "batch_get_profiles: null pointer");
+    BB_CUDA(cudaMemcpyAsync(out, q->d_profile, sizeof(double) * (size_t)q->B * q->S,
+                            cudaMemcpyDeviceToDevice, as_stream(stream)));
+    return BLOND_OK;
+}
+
+int blond_batch_get_induced_voltages(blond_batch* q, double* out, void* stream) {
+    using namespace bb;
+    BB_CHECK_ARG(q && out, "batch_get_induced_voltages: null pointer");
+    BB_CUDA(cudaMemcpyAsync(out, q->d_vind, sizeof(double) * (size_t)q->B * q->S,
+                            cudaMemcpyDeviceToDevice, as_stream(stream)));
+    return BLOND_OK;
+}
+
+}  // extern "C"

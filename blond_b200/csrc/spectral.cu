@@ -94,7 +94,7 @@ int launch_spectral(const SpecParams& P, cudaStream_t stream) {
     int rc = prepare_spectral();
     if (rc) return rc;
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(P.p.C, 1, 1);
+    cfg.gridDim = dim3(P.p.C * (P.batch > 0 ? P.batch : 1), 1, 1);
     cfg.blockDim = dim3(kSpecThreads, 1, 1);
     cfg.dynamicSmemBytes = P.p.smem;
     cfg.stream = stream;

@@ -94,6 +94,14 @@ struct SpecParams {
     // twiddle tables precomputed for this plan (make_spec_twiddles), or
     // nullptr to compute them in the kernel
     const double2* twg;
+    // batch of independent profiles: cluster q (blockIdx.x / C) handles
+    // profile q; in_i32 / profile_out / out / bc / table advance by n_in
+    // entries per profile, H by M + 1; beam_scale[q] and beam_inv_w[q]
+    // replace out_scale and inv_w when given.  No inductive term and no
+    // turn reads in batch mode (only the last cluster bumps the counter).
+    int batch;
+    const double* beam_scale;
+    const double* beam_inv_w;
 };
 
 // Device code below is compiled only in spectral.cu (which defines
@@ -304,6 +312,19 @@ spectral_kernel(const SpecParams P) {
     const SpecLayout lay = spec_layout(p);
     const int per = p.M / p.C;
     const int M = p.M, M1 = p.M1, M2 = p.M2, Bc = p.Bc, Br = p.Br, L = p.L;
+    // this cluster's profile (batch mode) and its arrays
+    const int beam = P.batch ? (int)(blockIdx.x / p.C) : 0;
+    const int64_t boff = (int64_t)beam * P.n_in;
+    int* const g_in_i32 = P.in_i32 ? P.in_i32 + boff : nullptr;
+    const double* const g_in_f64 = P.in_f64 ? P.in_f64 + boff : nullptr;
+    double* const g_profile = P.profile_out ? P.profile_out + boff : nullptr;
+    double* const g_out = P.out ? P.out + boff : nullptr;
+    const double* const g_bc = P.bc ? P.bc + boff : nullptr;
+    void* const g_table =
+        P.table ? static_cast<char*>(P.table) + boff * (P.table_f32 ? 8 : 16) : nullptr;
+    const double2* const g_H = P.H ? P.H + (int64_t)beam * (M + 1) : nullptr;
+    const double out_scale = P.beam_scale ? P.beam_scale[beam] : P.out_scale;
+    const double inv_w = P.beam_inv_w ? P.beam_inv_w[beam] : P.inv_w;
     double2* buf[3] = {reinterpret_cast<double2*>(sraw + lay.bufs),
                        reinterpret_cast<double2*>(sraw + lay.bufs) + per,
                        reinterpret_cast<double2*>(sraw + lay.bufs) + 2 * per};
@@ -335,15 +356,15 @@ spectral_kernel(const SpecParams P) {
         if (P.mode & SPEC_MULTIPLY) {
             for (int e = tid; e < per; e += nth) {
                 const int k = c * Br + e % Br + M1 * (e / Br);
-                cp_async16(&hk[e], &P.H[k]);
-                cp_async16(&hp[e], &P.H[k == 0 ? M : M - k]);
+                cp_async16(&hk[e], &g_H[k]);
+                cp_async16(&hp[e], &g_H[k == 0 ? M : M - k]);
             }
         }
-        if (inverse && P.table) {
+        if (inverse && g_table) {
             for (int e = tid; e < per; e += nth) {
                 const int64_t m = (int64_t)c * Bc + e % Bc + (int64_t)M2 * (e / Bc);
-                if (2 * m < P.n_out - 1) cp_async8(&bcs[2 * e], &P.bc[2 * m]);
-                if (2 * m + 1 < P.n_out - 1) cp_async8(&bcs[2 * e + 1], &P.bc[2 * m + 1]);
+                if (2 * m < P.n_out - 1) cp_async8(&bcs[2 * e], &g_bc[2 * m]);
+                if (2 * m + 1 < P.n_out - 1) cp_async8(&bcs[2 * e + 1], &g_bc[2 * m + 1]);
             }
         }
         asm volatile("cp.async.commit_group;" ::: "memory");
@@ -380,26 +401,26 @@ spectral_kernel(const SpecParams P) {
             const int64_t m = (int64_t)c * Bc + b + (int64_t)M2 * n1;
             double x0 = 0.0, x1 = 0.0;
             const int64_t i0 = 2 * m, i1 = 2 * m + 1;
-            if (P.in_i32) {
-                if (i0 < nlim) { x0 = (double)P.in_i32[i0]; P.in_i32[i0] = 0; }
-                if (i1 < nlim) { x1 = (double)P.in_i32[i1]; P.in_i32[i1] = 0; }
-                if (P.profile_out) {
-                    if (i0 < P.n_in) P.profile_out[i0] = x0;
-                    if (i1 < P.n_in) P.profile_out[i1] = x1;
+            if (g_in_i32) {
+                if (i0 < nlim) { x0 = (double)g_in_i32[i0]; g_in_i32[i0] = 0; }
+                if (i1 < nlim) { x1 = (double)g_in_i32[i1]; g_in_i32[i1] = 0; }
+                if (g_profile) {
+                    if (i0 < P.n_in) g_profile[i0] = x0;
+                    if (i1 < P.n_in) g_profile[i1] = x1;
                 }
             } else {
-                if (i0 < nlim) x0 = P.in_f64[i0];
-                if (i1 < nlim) x1 = P.in_f64[i1];
+                if (i0 < nlim) x0 = g_in_f64[i0];
+                if (i1 < nlim) x1 = g_in_f64[i1];
             }
             buf[0][n1 * Bc + b] = make_double2(x0, x1);
         }
         // histogram bins beyond the transform length (profile longer than
         // n_fft): converted and cleared but not transformed
-        if (P.in_i32 && c == 0) {
+        if (g_in_i32 && c == 0) {
             for (int64_t i = (int64_t)p.N + tid; i < P.n_in; i += nth) {
-                const double x = (double)P.in_i32[i];
-                P.in_i32[i] = 0;
-                if (P.profile_out) P.profile_out[i] = x;
+                const double x = (double)g_in_i32[i];
+                g_in_i32[i] = 0;
+                if (g_profile) g_profile[i] = x;
             }
         }
         wait_twiddles();
@@ -482,8 +503,8 @@ spectral_kernel(const SpecParams P) {
                 }
             }
             if (P.mode & SPEC_MULTIPLY) {
-                const double2 Hk = p.prefetch ? hk[e] : P.H[k];
-                const double2 Hp = p.prefetch ? hp[e] : P.H[k == 0 ? M : M - k];
+                const double2 Hk = p.prefetch ? hk[e] : g_H[k];
+                const double2 Hp = p.prefetch ? hp[e] : g_H[k == 0 ? M : M - k];
                 Yk = cmul(Yk, Hk);
                 Yp = cmul(Yp, Hp);
             }
@@ -549,14 +570,14 @@ spectral_kernel(const SpecParams P) {
     // ---- real output y[2m], y[2m+1] with m = c Bc + b + M2 m1
     const int64_t S = P.n_in;
     auto value = [&](int64_t n, double y) {
-        double v = y * P.out_scale;
+        double v = y * out_scale;
         if (P.ind_coeff) {
             // np.gradient(profile, dbc): central inside, one-sided at ends
             double g;
             if (S < 2) g = 0.0;
-            else if (n == 0) g = (P.profile_out[1] - P.profile_out[0]) / P.ind_dbc;
-            else if (n == S - 1) g = (P.profile_out[S - 1] - P.profile_out[S - 2]) / P.ind_dbc;
-            else g = (P.profile_out[n + 1] - P.profile_out[n - 1]) / (2.0 * P.ind_dbc);
+            else if (n == 0) g = (g_profile[1] - g_profile[0]) / P.ind_dbc;
+            else if (n == S - 1) g = (g_profile[S - 1] - g_profile[S - 2]) / P.ind_dbc;
+            else g = (g_profile[n + 1] - g_profile[n - 1]) / (2.0 * P.ind_dbc);
             v = v + ind * g;
         }
         return v;
@@ -566,9 +587,9 @@ spectral_kernel(const SpecParams P) {
         const int64_t m = (int64_t)c * Bc + b + (int64_t)M2 * m1;
         const double2 u = cres[m1 * Bc + b];
         const double v0 = value(2 * m, u.x), v1 = value(2 * m + 1, u.y);
-        if (2 * m < P.n_out) P.out[2 * m] = v0;
-        if (2 * m + 1 < P.n_out) P.out[2 * m + 1] = v1;
-        if (P.table) {
+        if (2 * m < P.n_out) g_out[2 * m] = v0;
+        if (2 * m + 1 < P.n_out) g_out[2 * m + 1] = v1;
+        if (g_table) {
             vloc[e] = v0;
             // v0 is V[2(m-1)+2] for the element before m: hand it to the
             // CTA that owns that element (first column of a CTA only)
@@ -582,8 +603,8 @@ spectral_kernel(const SpecParams P) {
     // reading the others' `rres` -- no CTA may exit before that
     cluster.sync();
     BB_PHASE(9);
-    if (!P.table && !P.bump_turn) return;
-    if (P.table) {
+    if (!g_table && !P.bump_turn) return;
+    if (g_table) {
         const int64_t nt = P.n_out - 1;
         for (int e = tid; e < per; e += nth) {
             const int b = e % Bc, m1 = e / Bc;
@@ -597,21 +618,21 @@ spectral_kernel(const SpecParams P) {
                 if (n >= nt) continue;
                 const double a0 = h == 0 ? v0 : v1;
                 const double a1 = h == 0 ? v1 : (b + 1 < Bc ? vloc[e + 1] : nbr[m1]);
-                const double bcn = p.prefetch ? bcs[2 * e + h] : P.bc[n];
+                const double bcn = p.prefetch ? bcs[2 * e + h] : g_bc[n];
                 if (!P.table_f32) {
                     // linear_interp_kick.cpp:44-47 with acc = 0
-                    const double slope = P.charge * (a1 - a0) * P.inv_w;
+                    const double slope = P.charge * (a1 - a0) * inv_w;
                     const double offset = P.charge * a0 - bcn * slope;
-                    reinterpret_cast<double2*>(P.table)[n] = make_double2(slope, offset);
+                    reinterpret_cast<double2*>(g_table)[n] = make_double2(slope, offset);
                 } else {
-                    reinterpret_cast<float2*>(P.table)[n] =
+                    reinterpret_cast<float2*>(g_table)[n] =
                         make_float2((float)(P.charge * a0),
-                                    (float)(P.charge * (a1 - a0) * P.inv_w));
+                                    (float)(P.charge * (a1 - a0) * inv_w));
                 }
             }
         }
     }
-    if (P.bump_turn && c == 0 && tid == 0) *P.turn = turn + 1;
+    if (P.bump_turn && beam == 0 && c == 0 && tid == 0) *P.turn = turn + 1;
     BB_PHASE(10);
 }
 

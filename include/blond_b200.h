@@ -238,6 +238,41 @@ int blond_engine_step(blond_engine* engine, int part, void* stream);
 int blond_engine_tune(blond_engine* engine, int threads, int blocks_per_sm,
                       int turns_per_graph);
 
+/* ------------------------------------------------------------ batched beams
+ * Many independent beams (one RingAndRFTracker + Profile +
+ * TotalInducedVoltage each in the reference) tracked together: one
+ * particle launch and one head launch per turn for the whole batch, each
+ * beam with its own particle count, RF programme, slicing window and
+ * impedance, and the single-beam engine's arithmetic.  Host arrays are
+ * beam-major: RF [B][n_turns+1][n_rf], acc [B][n_turns], drift arrays
+ * [B][n_turns+1], cuts [B], bin_centers [B][n_slices], impedance
+ * [B][n_fft/2+1] complex, scale [B] (= charge * e * ratio of each beam).
+ * dt/dE: device arrays of all beams concatenated, beam b occupying
+ * [offsets[b], offsets[b+1]) (host offsets). */
+typedef struct blond_batch blond_batch;
+int blond_batch_create(blond_batch** batch, int precision, int n_beams, int n_rf,
+                       int solver, int n_slices);
+int blond_batch_destroy(blond_batch* batch);
+int blond_batch_set_rf(blond_batch* batch, int64_t n_turns, const double* voltage,
+                       const double* omega_rf, const double* phi_rf,
+                       const double* acc_kick, double charge);
+int blond_batch_set_drift(blond_batch* batch, double length_ratio, double alpha_order,
+                          const double* t_rev, const double* eta_0, const double* eta_1,
+                          const double* eta_2, const double* alpha_0, const double* alpha_1,
+                          const double* alpha_2, const double* beta, const double* energy);
+int blond_batch_set_slicing(blond_batch* batch, const double* cut_left,
+                            const double* cut_right, const double* bin_centers);
+int blond_batch_set_impedance(blond_batch* batch, int64_t n_fft, const double* impedance,
+                              const double* scale);
+int blond_batch_bind_beams(blond_batch* batch, void* dt, void* dE, const int64_t* offsets);
+int blond_batch_set_turn(blond_batch* batch, int64_t turn, void* stream);
+int blond_batch_slice(blond_batch* batch, void* stream);
+int blond_batch_run(blond_batch* batch, int64_t n_turns, void* stream);
+int blond_batch_tune(blond_batch* batch, int turns_per_graph);
+/* device outputs of B * n_slices doubles (beam-major) */
+int blond_batch_get_profiles(blond_batch* batch, double* profiles, void* stream);
+int blond_batch_get_induced_voltages(blond_batch* batch, double* v, void* stream);
+
 /* ------------------------------------------------------------ one turn, no allocation
  * No counterpart in the reference.  One fused turn of the engine -- slice
  * the input coordinates, induced voltage (when `impedance` is not NULL) and
