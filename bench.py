@@ -53,6 +53,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--kernel", default="auto", choices=["auto", "tma", "plain"])
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3"],
+                    help="c2: the single-beam pipeline (default, the headline); "
+                         "c3: 256-beam double-RF batch")
+    ap.add_argument("--beams", type=int, default=256)
     return ap.parse_args()
 
 
@@ -377,8 +381,121 @@ def run_reference(args, world, rank):
     }
 
 
+C3_WORKLOAD = ("256 independent beams, double RF h=4620/18480 V2/V1=0.1 phi2=pi, "
+               "V1 ~ U(2,7) MV, N_b log-uniform in [1e5, 4e6], sigma_dt ~ U(0.2,0.5) ns, "
+               "512 slices, 3 resonators (R 2e5/1e5/5e4 Ohm, f_r 0.2/0.8/1.4 GHz, "
+               "Q log-uniform [100, 30000]), intensity 2e6 e per macro-particle")
+
+
+def c3_beams(n_beams, turns, seed=1234, scale_particles=1.0):
+    """The C3 scan: drop-in objects of every beam (seeded)."""
+    import torch
+    from blond_b200.beam.beam import Beam, Proton
+    from blond_b200.beam.distributions import _get_dE_from_dt, bigaussian_arrays
+    from blond_b200.beam.profile import CutOptions, Profile
+    from blond_b200.impedances.impedance import InducedVoltageFreq, TotalInducedVoltage
+    from blond_b200.impedances.impedance_sources import Resonators
+    from blond_b200.input_parameters.rf_parameters import RFStation
+    from blond_b200.input_parameters.ring import Ring
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n_beams):
+        n = int(round(np.exp(rng.uniform(np.log(1e5), np.log(4e6))) * scale_particles))
+        V1 = rng.uniform(2e6, 7e6)
+        sdt = rng.uniform(0.2e-9, 0.5e-9)
+        Q = np.exp(rng.uniform(np.log(100), np.log(30000), 3))
+        ring = Ring(6911.5, 1 / 18**2, 26e9, Proton(), turns)
+        rf = RFStation(ring, [4620, 4 * 4620], [V1, 0.1 * V1], [0.0, np.pi], n_rf=2)
+        centre = (rf.phi_s[0] - rf.phi_rf[0, 0]) / rf.omega_rf[0, 0]
+        dt, dE = bigaussian_arrays(n, sdt, _get_dE_from_dt(ring, rf, sdt), centre, seed + k)
+        beam = Beam(ring, n, 2e6 * n, dt=dt, dE=dE, dtype=torch.float64)
+        prof = Profile(beam, CutOptions(cut_left=centre - 1.25e-9,
+                                        cut_right=centre + 1.25e-9, n_slices=512))
+        iv = InducedVoltageFreq(beam, prof, [Resonators([2e5, 1e5, 5e4],
+                                                        [200e6, 800e6, 1.4e9], Q)])
+        out.append((rf, beam, prof, TotalInducedVoltage(beam, prof, [iv])))
+    return out
+
+
+def run_c3(args):
+    """Batched F32P64 and FP64 vs every beam through its own FP64 engine
+    (the unbatched plain path), with the F32P64 error per beam."""
+    import torch
+    from blond_b200.batch import BatchTracker
+    from blond_b200.engine import FusedTracker
+    from blond_b200.trackers.tracker import RingAndRFTracker
+    W, K = max(3, args.warmup), args.steps
+    beams = c3_beams(args.beams, 2 * (W + K) + 4)
+    n_total = sum(b.n_macroparticles for _, b, _, _ in beams)
+    res = {}
+    for prec in ("f32p64", "f64"):
+        bt = BatchTracker([(RingAndRFTracker(rf, b), p, t) for rf, b, p, t in beams],
+                          precision=prec)
+        bt.track(W)
+        bt.prepare()
+        ms = time_turns(bt, K)
+        res[prec] = (n_total * K / (ms * 1e-3), ms / K, bt)
+        for rf, _, _, _ in beams:
+            rf.counter[0] = 0
+    # F32P64 vs FP64 after W + K turns: rms bunch length / energy spread
+    errs = []
+    b32, b64 = res["f32p64"][2], res["f64"][2]
+    for k, (_, _, p, _) in enumerate(beams):
+        x = [t.double().cpu().numpy() for t in b64.coordinates(k)]
+        y = [t.double().cpu().numpy() for t in b32.coordinates(k)]
+        w = (x[0] > p.cut_left) & (x[0] < p.cut_right)
+        errs.append([abs(np.std(v[w]) / np.std(u[w]) - 1) for u, v in zip(x, y)])
+    errs = np.array(errs)
+    vals = {p: (res[p][0], res[p][1]) for p in res}
+    del b32, b64, res
+    torch.cuda.empty_cache()
+    # the unbatched plain path: every beam through its own FP64 engine
+    engines = [FusedTracker(RingAndRFTracker(rf, b), p, t, precision="f64",
+                            turns_per_graph=K) for rf, b, p, t in beams]
+    for e in engines:
+        e.track(W)
+        e.prepare()
+    torch.cuda.synchronize()
+    s = torch.cuda.current_stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(s)
+    for e in engines:
+        e.track(K)
+    b.record(s)
+    torch.cuda.synchronize()
+    ms_plain = a.elapsed_time(b)
+    plain = n_total * K / (ms_plain * 1e-3)
+    return vals, plain, ms_plain / K, errs, n_total
+
+
 def main():
     args = parse()
+    if args.workload == "c3" and args.impl == "ours":
+        W, K = max(3, args.warmup), args.steps
+        vals, plain, ms_plain, errs, n_total = run_c3(args)
+        print(json.dumps({
+            "metric": METRIC, "value": vals["f32p64"][0], "unit": UNIT, "n_gpus": 1,
+            "steps": K, "warmup": W, "ms_per_step": vals["f32p64"][1],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32p64", "data": "synthetic",
+            "config": {"workload": C3_WORKLOAD, "beams": args.beams,
+                       "particles_total": n_total, "slices": 512, "n_fft": 512},
+            "batched_f64": {"value": vals["f64"][0], "ms_per_step": vals["f64"][1]},
+            "unbatched_plain_f64": {"value": plain, "ms_per_step": ms_plain},
+            "speedup_f32p64_batched_vs_unbatched_f64": vals["f32p64"][0] / plain,
+            "f32p64_rel_err_after_turns": {
+                "turns": W + K,
+                "statistic": "in-window rms of dt and dE, per beam, F32P64 vs FP64 batch",
+                "sigma_dt_median": float(np.median(errs[:, 0])),
+                "sigma_dt_p90": float(np.percentile(errs[:, 0], 90)),
+                "sigma_dt_max": float(errs[:, 0].max()),
+                "sigma_dE_median": float(np.median(errs[:, 1])),
+                "sigma_dE_p90": float(np.percentile(errs[:, 1], 90)),
+                "sigma_dE_max": float(errs[:, 1].max()),
+                "beams_within_1e-5": int(np.sum(errs.max(axis=1) <= 1e-5))},
+            "gpu_launches": 2 * K,
+        }), flush=True)
+        return
     if args.impl == "reference":
         os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
         world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -80,6 +80,7 @@ _EXTRA = {
     "blond_batch_set_turn": [c_ptr, c_i64, c_ptr],
     "blond_batch_slice": [c_ptr, c_ptr],
     "blond_batch_run": [c_ptr, c_i64, c_ptr],
+    "blond_batch_prepare": [c_ptr, c_ptr],
     "blond_batch_tune": [c_ptr, c_int],
     "blond_batch_get_profiles": [c_ptr, c_ptr, c_ptr],
     "blond_batch_get_induced_voltages": [c_ptr, c_ptr, c_ptr],

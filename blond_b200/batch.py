@@ -129,6 +129,11 @@ class BatchTracker:
                 pass
             self.h = None
 
+    def prepare(self):
+        """Build and upload the CUDA graph now (else the first track() of at
+        least turns_per_graph turns builds it)."""
+        self._call("prepare", _stream())
+
     def track(self, n_turns: int = 1):
         self._call("run", int(n_turns), _stream())
         for rf, beam in zip(self.rfs, self.beams):

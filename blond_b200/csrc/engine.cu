@@ -1817,6 +1817,41 @@ int blond_batch_slice(blond_batch* q, void* stream) {
     return launch_batch_profile(q, false, s);
 }
 
+int blond_batch_prepare(blond_batch* q, void* stream) {
+    using namespace bb;
+    BB_CHECK_ARG(q, "batch_prepare: null batch");
+    int rc = batch_ready(q);
+    if (rc) return rc;
+    const int K = q->turns_per_graph;
+    if (K <= 1 || (!q->graph_dirty && q->graph)) return BLOND_OK;
+    cudaStream_t s = as_stream(stream);
+    // kernel attributes are set here, never inside the capture
+    if ((rc = launch_batch(q, true, s, false))) return rc;
+    if (q->has_fft && (rc = prepare_spectral())) return rc;
+    if (q->graph) cudaGraphExecDestroy(q->graph);
+    q->graph = nullptr;
+    cudaGraph_t g;
+    BB_CUDA(cudaStreamBeginCapture(q->cap_stream, cudaStreamCaptureModeThreadLocal));
+    int lrc = BLOND_OK;
+    for (int i = 0; i < K && lrc == BLOND_OK; ++i) lrc = batch_turn(q, q->cap_stream);
+    cudaError_t ce = cudaStreamEndCapture(q->cap_stream, &g);
+    if (lrc) return lrc;
+    if (ce != cudaSuccess) {
+        set_error("batch: graph capture failed: %s", cudaGetErrorString(ce));
+        return BLOND_ERR_CUDA;
+    }
+    ce = cudaGraphInstantiate(&q->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (ce != cudaSuccess) {
+        set_error("batch: graph instantiation failed: %s", cudaGetErrorString(ce));
+        return BLOND_ERR_CUDA;
+    }
+    BB_CUDA(cudaGraphUpload(q->graph, s));
+    q->graph_turns = K;
+    q->graph_dirty = false;
+    return BLOND_OK;
+}
+
 int blond_batch_run(blond_batch* q, int64_t n_turns, void* stream) {
     using namespace bb;
     BB_CHECK_ARG(q && n_turns >= 0, "batch_run: bad argument");
@@ -1829,31 +1864,7 @@ int blond_batch_run(blond_batch* q, int64_t n_turns, void* stream) {
     const int K = q->turns_per_graph;
     int64_t done = 0;
     if (n_turns >= K && K > 1) {
-        if (q->graph_dirty || !q->graph) {
-            if ((rc = launch_batch(q, true, s, false))) return rc;
-            if (q->has_fft && (rc = prepare_spectral())) return rc;
-            if (q->graph) cudaGraphExecDestroy(q->graph);
-            q->graph = nullptr;
-            cudaGraph_t g;
-            BB_CUDA(cudaStreamBeginCapture(q->cap_stream, cudaStreamCaptureModeThreadLocal));
-            int lrc = BLOND_OK;
-            for (int i = 0; i < K && lrc == BLOND_OK; ++i) lrc = batch_turn(q, q->cap_stream);
-            cudaError_t ce = cudaStreamEndCapture(q->cap_stream, &g);
-            if (lrc) return lrc;
-            if (ce != cudaSuccess) {
-                set_error("batch_run: graph capture failed: %s", cudaGetErrorString(ce));
-                return BLOND_ERR_CUDA;
-            }
-            ce = cudaGraphInstantiate(&q->graph, g, 0);
-            cudaGraphDestroy(g);
-            if (ce != cudaSuccess) {
-                set_error("batch_run: graph instantiation failed: %s", cudaGetErrorString(ce));
-                return BLOND_ERR_CUDA;
-            }
-            BB_CUDA(cudaGraphUpload(q->graph, s));
-            q->graph_turns = K;
-            q->graph_dirty = false;
-        }
+        if ((rc = blond_batch_prepare(q, stream))) return rc;
         for (; done + K <= n_turns; done += K) BB_CUDA(cudaGraphLaunch(q->graph, s));
     }
     for (; done < n_turns; ++done)

@@ -267,6 +267,8 @@ int blond_batch_set_impedance(blond_batch* batch, int64_t n_fft, const double* i
 int blond_batch_bind_beams(blond_batch* batch, void* dt, void* dE, const int64_t* offsets);
 int blond_batch_set_turn(blond_batch* batch, int64_t turn, void* stream);
 int blond_batch_slice(blond_batch* batch, void* stream);
+/* capture and upload the turn graph now (else the first long run does) */
+int blond_batch_prepare(blond_batch* batch, void* stream);
 int blond_batch_run(blond_batch* batch, int64_t n_turns, void* stream);
 int blond_batch_tune(blond_batch* batch, int turns_per_graph);
 /* device outputs of B * n_slices doubles (beam-major) */
