@@ -53,9 +53,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--kernel", default="auto", choices=["auto", "tma", "plain"])
-    ap.add_argument("--workload", default="c2", choices=["c2", "c3"],
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c5"],
                     help="c2: the single-beam pipeline (default, the headline); "
-                         "c3: 256-beam double-RF batch")
+                         "c3: 256-beam double-RF batch; c5: 1e8 particles, "
+                         "2^16 slices, 4 resonators + inductive Z/n")
     ap.add_argument("--beams", type=int, default=256)
     return ap.parse_args()
 
@@ -468,8 +469,99 @@ def run_c3(args):
     return vals, plain, ms_plain / K, errs, n_total
 
 
+C5_WORKLOAD = ("1e8 protons 26 GeV/c, double RF h=4620/18480 4.5/0.45 MV (phi 0/pi), "
+               "2^16 slices over 2.5 ns, "
+               "4 resonators (R 2e5/1e5/5e4/3e4 Ohm, f_r 0.2/0.8/1.4/2.0 GHz, "
+               "Q 100/1000/3000/30000) + inductive Im(Z)/n 0.1 Ohm, intensity 1e11")
+
+
+def build_c5(n, n_turns, precision, seed=0):
+    """The C5 pipeline: a long profile (2^16 slices, histogram deposited
+    straight into global memory) and a sum of five impedance sources."""
+    import torch
+    from blond_b200.beam.beam import Beam
+    from blond_b200.beam.profile import CutOptions, Profile
+    from blond_b200.engine import FusedTracker
+    from blond_b200.impedances.impedance import (InducedVoltageFreq, InductiveImpedance,
+                                                 TotalInducedVoltage)
+    from blond_b200.impedances.impedance_sources import Resonators
+    from blond_b200.trackers.tracker import RingAndRFTracker
+    from blond_b200.input_parameters.rf_parameters import RFStation
+    ring, _ = machine(n_turns)
+    rf = RFStation(ring, [4620, 4 * 4620], [4.5e6, 0.45e6], [0.0, np.pi], n_rf=2)
+    dt, dE, centre = host_bunch(ring, rf, n, seed)
+    beam = Beam(ring, n, 1e11, dt=dt, dE=dE, dtype=torch.float64)
+    del dt, dE
+    cl, cr, _ = window(centre, 65536)
+    prof = Profile(beam, CutOptions(cut_left=cl, cut_right=cr, n_slices=65536))
+    iv = InducedVoltageFreq(beam, prof, [Resonators([2e5, 1e5, 5e4, 3e4],
+                                                    [200e6, 800e6, 1.4e9, 2.0e9],
+                                                    [100.0, 1000.0, 3000.0, 30000.0])])
+    ind = InductiveImpedance(beam, prof, [0.1] * (n_turns + 1), rf)
+    tiv = TotalInducedVoltage(beam, prof, [iv, ind])
+    fused = FusedTracker(RingAndRFTracker(rf, beam), prof, tiv, precision=precision,
+                         turns_per_graph=50)
+    return fused, beam, prof, iv.n_fft
+
+
+def run_c5(args):
+    """F32P64 (the C5 precision) and FP64 on the same bunch; the F32P64
+    error is the in-window rms of dt and dE after the timed turns."""
+    import torch
+    W, K = max(3, args.warmup), args.steps
+    kt = min(K, 20)
+    n = int(args.particles) if args.particles != 1e7 else int(1e8)
+    res, coords = {}, {}
+    peak = _peaks().get("hbm_gbs") or 6650.0
+    for prec in ("f32p64", "f64"):
+        fused, beam, prof, n_fft = build_c5(n, W + K + kt + 4, prec)
+        fused.track(W)
+        fused.prepare()
+        torch.cuda.synchronize()
+        clocks = ClockSampler(0) if prec == "f32p64" else None
+        ms = time_turns(fused, K)
+        clk = clocks.stop() if clocks else None
+        fused.check()
+        w = (fused.dt > prof.cut_left) & (fused.dt < prof.cut_right)
+        coords[prec] = (fused.dt[w].std().item(), fused.dE.double()[w].std().item())
+        head_ms, part_ms = fused.time_kernels(kt)
+        ach = BYTES_PER_PARTICLE[prec] * n / (part_ms / kt * 1e-3) / 1e9
+        res[prec] = {"value": n * K / (ms * 1e-3), "ms_per_step": ms / K,
+                     "kernel_ms": part_ms / kt, "head_kernel_ms": head_ms / kt,
+                     "achieved_gbs": ach, "frac": ach / peak, "clocks": clk,
+                     "kernel": fused.kernel}
+        del fused, beam, prof
+        torch.cuda.empty_cache()
+    r = res["f32p64"]
+    return {
+        "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": 1,
+        "steps": K, "warmup": W, "ms_per_step": r["ms_per_step"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32p64", "data": "synthetic",
+        "config": {"workload": C5_WORKLOAD, "particles": n, "slices": 65536,
+                   "n_fft": n_fft, "l2": "inputs larger than L2"},
+        "roofline": {"bound": "hbm", "achieved": r["achieved_gbs"], "peak": peak,
+                     "unit": "GB/s", "frac": r["frac"], "traffic": None,
+                     "kernel": f"particle_kernel{'_tma' if r['kernel'] == 'tma' else ''} "
+                               "(global-memory histogram)",
+                     "kernel_ms": r["kernel_ms"], "head_kernel_ms": r["head_kernel_ms"],
+                     "bytes_per_particle": BYTES_PER_PARTICLE["f32p64"]},
+        "f64": {k: res["f64"][k] for k in ("value", "ms_per_step", "kernel_ms",
+                                            "head_kernel_ms", "achieved_gbs", "frac")},
+        "f32p64_rel_err_after_turns": {
+            "turns": W + K, "statistic": "in-window rms of dt and dE, F32P64 vs FP64",
+            "sigma_dt": abs(coords["f32p64"][0] / coords["f64"][0] - 1),
+            "sigma_dE": abs(coords["f32p64"][1] / coords["f64"][1] - 1)},
+        "gpu_launches": 2 * K,
+        "clocks": r["clocks"],
+    }
+
+
 def main():
     args = parse()
+    if args.workload == "c5" and args.impl == "ours":
+        print(json.dumps(run_c5(args)), flush=True)
+        return
     if args.workload == "c3" and args.impl == "ours":
         W, K = max(3, args.warmup), args.steps
         vals, plain, ms_plain, errs, n_total = run_c3(args)

@@ -56,6 +56,8 @@ struct ParticleArgs {
     // interpolation table (induced voltage)
     const void* table;
     double bc0, lik_inv_w, bw;
+    int global_hist;  // 1: deposit into `hist` directly (no shared copy)
+    int tma_stages;   // chunks in flight per block of the staged pass
 };
 
 enum { PREC_F64 = 0, PREC_F32P64 = 1 };
@@ -208,6 +210,47 @@ __device__ __forceinline__ void deposit(int* sh, int b, bool warp_agg, unsigned 
     }
 }
 
+// Block-private histogram layouts of the staged particle pass.
+//   HIST_AGG    one int per bin, warp-aggregated deposits (short profiles)
+//   HIST_I32    one int per bin
+//   HIST_PACKED two 16-bit counters per 32-bit word -- bin b < half in the
+//               low half of word b, bin b >= half in the high half of word
+//               b - half -- so a 2^16-slice profile fits in 128 KB.
+enum { HIST_AGG = 0, HIST_I32 = 1, HIST_PACKED = 2 };
+
+// Packed deposit.  A counter wraps after 65536 deposits of one block into
+// one bin; every wrap is seen by exactly one thread (from the old value its
+// atomic returns) and carried into the global histogram, so the counts stay
+// exact for any distribution.  A low counter's wrap also carries +1 into
+// the high counter of the word; the depositing thread takes that carry
+// back, and both the carry and its removal may wrap the high counter, which
+// is accounted the same way.  Between the carry and its removal the high
+// counter only ever holds extra carries (never fewer), so the accounting
+// needs no ordering between threads.
+__device__ __forceinline__ void deposit_packed(unsigned* sh, int half, int* gh, int b) {
+    if (b < 0) return;
+    if (b < half) {
+        const unsigned old = atomicAdd(&sh[b], 1u);
+        if ((old & 0xffffu) == 0xffffu) {
+            atomicAdd(&gh[b], 65536);
+            if ((old >> 16) == 0xffffu) atomicAdd(&gh[b + half], 65536);
+            const unsigned o2 = atomicSub(&sh[b], 0x10000u);
+            if ((o2 >> 16) == 0u) atomicAdd(&gh[b + half], -65536);
+        }
+    } else {
+        const unsigned old = atomicAdd(&sh[b - half], 0x10000u);
+        if ((old >> 16) == 0xffffu) atomicAdd(&gh[b], 65536);
+    }
+}
+
+template <int HIST>
+__device__ __forceinline__ void block_deposit(int* sh, int half, int* gh, int b) {
+    if (HIST == HIST_PACKED)
+        deposit_packed(reinterpret_cast<unsigned*>(sh), half, gh, b);
+    else
+        deposit(sh, b, HIST == HIST_AGG, 0xffffffffu);
+}
+
 // Flush the block-private histograms of one thread-block cluster: CTA r sums
 // bin range r of every CTA's shared histogram through distributed shared
 // memory and adds the sums to the global histogram, so a cluster of C
@@ -259,7 +302,11 @@ particle_kernel(const ParticleArgs a) {
             c.d = a.drift[t_idx + 1];
         }
     }
-    for (int k = threadIdx.x; k < a.S; k += blockDim.x) sh[k] = 0;
+    // profiles too long for a shared-memory copy deposit straight into
+    // the global histogram
+    int* const hd = a.global_hist ? a.hist : sh;
+    if (!a.global_hist)
+        for (int k = threadIdx.x; k < a.S; k += blockDim.x) sh[k] = 0;
     __syncthreads();
 
     double* dt = reinterpret_cast<double*>(a.dt);
@@ -284,8 +331,8 @@ particle_kernel(const ParticleArgs a) {
             b0 = engine_bin(tt.x, a.cut_left, a.inv_w, a.S);
             b1 = engine_bin(tt.y, a.cut_left, a.inv_w, a.S);
         }
-        deposit(sh, b0, WARP_AGG, 0xffffffffu);
-        deposit(sh, b1, WARP_AGG, 0xffffffffu);
+        deposit(hd, b0, WARP_AGG, 0xffffffffu);
+        deposit(hd, b1, WARP_AGG, 0xffffffffu);
     }
     // odd tail particle
     if ((a.n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
@@ -297,9 +344,9 @@ particle_kernel(const ParticleArgs a) {
             dE[a.n - 1] = e;
         }
         const int b = engine_bin(t, a.cut_left, a.inv_w, a.S);
-        if (b >= 0) atomicAdd(&sh[b], 1);
+        if (b >= 0) atomicAdd(&hd[b], 1);
     }
-    cluster_flush(sh, a.hist, a.S);
+    if (!a.global_hist) cluster_flush(sh, a.hist, a.S);
 }
 
 // ------------------------------------------------------ TMA-pipelined pass
@@ -356,7 +403,7 @@ __device__ __forceinline__ void mbar_wait_bounded(uint64_t* bar, uint32_t parity
         if (mbar_try_wait(bar, parity)) return;
 }
 
-template <int PREC, int SOLVER, bool LIK, bool WARP_AGG>
+template <int PREC, int SOLVER, bool LIK, int HIST>
 __global__ void __launch_bounds__(kTmaThreads, 1)
 particle_kernel_tma(const ParticleArgs a, int* err) {
     using E = typename Coord<PREC>::E;
@@ -365,9 +412,12 @@ particle_kernel_tma(const ParticleArgs a, int* err) {
     __shared__ TurnConsts c;
     __shared__ __align__(8) uint64_t full[kStages];
     int* sh = reinterpret_cast<int*>(dsm);
-    const size_t hist_bytes = ((size_t)a.S * sizeof(int) + 127) & ~(size_t)127;
+    const int half = (a.S + 1) / 2;
+    const int words = HIST == HIST_PACKED ? half : a.S;
+    const int nst = a.tma_stages;  // 2 .. kStages chunks in flight
+    const size_t hist_bytes = ((size_t)words * sizeof(int) + 127) & ~(size_t)127;
     double* st_dt = reinterpret_cast<double*>(dsm + hist_bytes);
-    E* st_dE = reinterpret_cast<E*>(dsm + hist_bytes + sizeof(double) * kTile * kStages);
+    E* st_dE = reinterpret_cast<E*>(dsm + hist_bytes + sizeof(double) * kTile * nst);
 
     long long t_idx = a.turn ? (*a.turn - 1) : 0;
     if (t_idx < 0) t_idx = 0;
@@ -381,10 +431,10 @@ particle_kernel_tma(const ParticleArgs a, int* err) {
     if (threadIdx.x == 0) {
         c.acc = a.acc[t_idx];
         c.d = a.drift[t_idx + 1];
-        for (int s = 0; s < kStages; ++s) mbar_init(&full[s], 1);
+        for (int s = 0; s < nst; ++s) mbar_init(&full[s], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    for (int k = threadIdx.x; k < a.S; k += blockDim.x) sh[k] = 0;
+    for (int k = threadIdx.x; k < words; k += blockDim.x) sh[k] = 0;
     __syncthreads();
 
     double* dt = reinterpret_cast<double*>(a.dt);
@@ -395,19 +445,19 @@ particle_kernel_tma(const ParticleArgs a, int* err) {
                                ? (nchunks - 1 - blockIdx.x) / gridDim.x + 1 : 0;
     const uint32_t bytes_dt = sizeof(double) * kTile, bytes_dE = sizeof(E) * kTile;
     auto issue = [&](long long i) {
-        const int s = (int)(i % kStages);
+        const int s = (int)(i % nst);
         const long long chunk = blockIdx.x + i * gridDim.x;
         mbar_expect_tx(&full[s], bytes_dt + bytes_dE);
         bulk_g2s(st_dt + (size_t)s * kTile, dt + chunk * kTile, bytes_dt, &full[s]);
         bulk_g2s(st_dE + (size_t)s * kTile, dE + chunk * kTile, bytes_dE, &full[s]);
     };
     if (threadIdx.x == 0)
-        for (long long i = 0; i < mine && i < kStages; ++i) issue(i);
+        for (long long i = 0; i < mine && i < nst; ++i) issue(i);
 
     const int order = a.order;
     for (long long i = 0; i < mine; ++i) {
-        const int s = (int)(i % kStages);
-        const bool got = mbar_wait_warp(&full[s], (uint32_t)((i / kStages) & 1), err);
+        const int s = (int)(i % nst);
+        const bool got = mbar_wait_warp(&full[s], (uint32_t)((i / nst) & 1), err);
         if (got) {
             const long long base = (blockIdx.x + i * gridDim.x) * (long long)kTile;
             const double2* sdt = reinterpret_cast<const double2*>(st_dt + (size_t)s * kTile);
@@ -420,24 +470,24 @@ particle_kernel_tma(const ParticleArgs a, int* err) {
                 track_pair<PREC, SOLVER, LIK>(tt.x, tt.y, ee.x, ee.y, c, a, order);
                 reinterpret_cast<double2*>(dt + base)[p] = tt;
                 reinterpret_cast<E2*>(dE + base)[p] = ee;
-                deposit(sh, engine_bin(tt.x, a.cut_left, a.inv_w, a.S), WARP_AGG, 0xffffffffu);
-                deposit(sh, engine_bin(tt.y, a.cut_left, a.inv_w, a.S), WARP_AGG, 0xffffffffu);
+                block_deposit<HIST>(sh, half, a.hist, engine_bin(tt.x, a.cut_left, a.inv_w, a.S));
+                block_deposit<HIST>(sh, half, a.hist, engine_bin(tt.y, a.cut_left, a.inv_w, a.S));
             }
         }
         // stage s fully consumed; the failure decision is block-uniform
         if (__syncthreads_or(!got)) {
-            // copies i .. min(mine, i + kStages) - 1 are in flight: give
+            // copies i .. min(mine, i + nst) - 1 are in flight: give
             // them a bounded chance to land before the block's shared
             // memory is released, then leave without flushing
             if (threadIdx.x == 0)
-                for (long long j = i; j < mine && j < i + kStages; ++j)
-                    mbar_wait_bounded(&full[j % kStages], (uint32_t)((j / kStages) & 1));
+                for (long long j = i; j < mine && j < i + nst; ++j)
+                    mbar_wait_bounded(&full[j % nst], (uint32_t)((j / nst) & 1));
             __syncthreads();
             return;
         }
-        if (threadIdx.x == 0 && i + kStages < mine) {
+        if (threadIdx.x == 0 && i + nst < mine) {
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            issue(i + kStages);
+            issue(i + nst);
         }
     }
     // remainder particles (fewer than one chunk): plain loads, last block
@@ -449,13 +499,25 @@ particle_kernel_tma(const ParticleArgs a, int* err) {
             dt[i] = t;
             dE[i] = e;
             const int b = engine_bin(t, a.cut_left, a.inv_w, a.S);
-            if (b >= 0) atomicAdd(&sh[b], 1);
+            if (HIST == HIST_PACKED)
+                deposit_packed(reinterpret_cast<unsigned*>(sh), half, a.hist, b);
+            else if (b >= 0)
+                atomicAdd(&sh[b], 1);
         }
     }
     __syncthreads();
-    for (int k = threadIdx.x; k < a.S; k += blockDim.x) {
-        const int v = sh[k];
-        if (v) atomicAdd(&a.hist[k], v);
+    if (HIST == HIST_PACKED) {
+        const unsigned* shp = reinterpret_cast<const unsigned*>(sh);
+        for (int k = threadIdx.x; k < half; k += blockDim.x) {
+            const unsigned v = shp[k];
+            if (v & 0xffffu) atomicAdd(&a.hist[k], (int)(v & 0xffffu));
+            if ((v >> 16) && k + half < a.S) atomicAdd(&a.hist[k + half], (int)(v >> 16));
+        }
+    } else {
+        for (int k = threadIdx.x; k < a.S; k += blockDim.x) {
+            const int v = sh[k];
+            if (v) atomicAdd(&a.hist[k], v);
+        }
     }
 }
 
@@ -533,7 +595,15 @@ static void free_ptr(void* p) {
     if (p) cudaFree(p);
 }
 
-static int engine_smem(const blond_engine* e) { return (int)sizeof(int) * e->S; }
+// Largest profile whose histogram the particle kernel privatises in shared
+// memory; longer profiles deposit into the global histogram.
+static int smem_hist_limit() {
+    return (device_info().max_smem_optin - (int)sizeof(TurnConsts) - 1024) / 4;
+}
+static bool global_hist(const blond_engine* e) { return e->S > smem_hist_limit(); }
+static int engine_smem(const blond_engine* e) {
+    return global_hist(e) ? 0 : (int)sizeof(int) * e->S;
+}
 
 // Raise a kernel's dynamic shared memory limit to the device's opt-in
 // maximum, once per device.  Done outside stream capture (engine_run calls
@@ -552,40 +622,81 @@ static int allow_max_smem(K kernel, bool* done) {
     return BLOND_OK;
 }
 
+// Layout of the staged pass for a profile of S slices: the histogram mode
+// and the number of chunks in flight that fit beside it in shared memory
+// (0: not even two fit, the plain pass runs instead).  One int per bin is
+// kept while it leaves room for kStages chunks (or as many as the packed
+// layout would); beyond that the packed 16-bit layout halves the
+// histogram.
+struct TmaPlan {
+    int mode = HIST_I32;
+    int stages = 0;
+    size_t bytes = 0;
+};
+
 template <int PREC>
-static size_t tma_smem(int S) {
+static TmaPlan tma_plan(int S) {
     using E = typename Coord<PREC>::E;
-    const size_t hist = ((size_t)S * sizeof(int) + 127) & ~(size_t)127;
-    return hist + (size_t)kStages * kTile * (sizeof(double) + sizeof(E));
+    const size_t stage = (size_t)kTile * (sizeof(double) + sizeof(E));
+    // static shared memory of the kernel (TurnConsts, barriers) + margin
+    const size_t reserve = sizeof(TurnConsts) + sizeof(uint64_t) * kStages + 256;
+    const size_t limit = (size_t)device_info().max_smem_optin - reserve;
+    auto fit = [&](size_t words, int* st) {
+        const size_t hist = (words * sizeof(int) + 127) & ~(size_t)127;
+        *st = hist + 2 * stage > limit
+                  ? 0 : (int)std::min<size_t>(kStages, (limit - hist) / stage);
+        return hist;
+    };
+    int st_i = 0, st_p = 0;
+    const size_t h_i = fit((size_t)S, &st_i);
+    const size_t h_p = fit((size_t)(S + 1) / 2, &st_p);
+    TmaPlan p;
+    if (st_i >= 2 && st_i >= std::min(kStages, st_p)) {
+        p.mode = S <= 2048 ? HIST_AGG : HIST_I32;
+        p.stages = st_i;
+        p.bytes = h_i + (size_t)st_i * stage;
+    } else if (st_p >= 2) {
+        p.mode = HIST_PACKED;
+        p.stages = st_p;
+        p.bytes = h_p + (size_t)st_p * stage;
+    }
+    return p;
+}
+
+template <int PREC, int SOLVER, bool LIK, int HIST>
+static int launch_tma(blond_engine* e, ParticleArgs a, const TmaPlan& p, cudaStream_t s,
+                      bool launch) {
+    static bool done[64] = {false};
+    auto k = particle_kernel_tma<PREC, SOLVER, LIK, HIST>;
+    int rc;
+    if ((rc = allow_max_smem(k, done))) return rc;
+    a.tma_stages = p.stages;
+    const long long nchunks = e->n / kTile;
+    const int grid = (int)std::max<long long>(
+        1, std::min<long long>(nchunks, device_info().sm_count));
+    if (launch) k<<<grid, kTmaThreads, p.bytes, s>>>(a, e->d_err);
+    BB_LAUNCH_CHECK();
+    return BLOND_OK;
 }
 
 template <int PREC, int SOLVER, bool LIK, bool KICK>
 static int launch_particles_t(blond_engine* e, const ParticleArgs& a, cudaStream_t s,
                               bool launch) {
     static bool done_agg[64] = {false}, done_plain[64] = {false};
-    static bool done_tma_agg[64] = {false}, done_tma[64] = {false};
     const int smem = engine_smem(e);
     const bool agg = e->S <= 2048;
     int rc;
-    if (KICK && e->variant == 0) {
-        const size_t tsm = tma_smem<PREC>(e->S);
-        auto k_agg = particle_kernel_tma<PREC, SOLVER, LIK, true>;
-        auto k_pl = particle_kernel_tma<PREC, SOLVER, LIK, false>;
-        cudaFuncAttributes fa;
-        BB_CUDA(cudaFuncGetAttributes(&fa, agg ? k_agg : k_pl));
-        if (tsm + fa.sharedSizeBytes <= (size_t)device_info().max_smem_optin) {
-            const long long nchunks = e->n / kTile;
-            const int grid = (int)std::max<long long>(
-                1, std::min<long long>(nchunks, device_info().sm_count));
-            if (agg) {
-                if ((rc = allow_max_smem(k_agg, done_tma_agg))) return rc;
-                if (launch) k_agg<<<grid, kTmaThreads, tsm, s>>>(a, e->d_err);
-            } else {
-                if ((rc = allow_max_smem(k_pl, done_tma))) return rc;
-                if (launch) k_pl<<<grid, kTmaThreads, tsm, s>>>(a, e->d_err);
+    if (KICK) {
+        // the staged pass when asked for, and for profiles whose int
+        // histogram does not fit beside the plain pass (packed layout
+        // instead of global-memory atomics)
+        const TmaPlan p = tma_plan<PREC>(e->S);
+        if (p.stages && (e->variant == 0 || global_hist(e))) {
+            switch (p.mode) {
+                case HIST_AGG: return launch_tma<PREC, SOLVER, LIK, HIST_AGG>(e, a, p, s, launch);
+                case HIST_I32: return launch_tma<PREC, SOLVER, LIK, HIST_I32>(e, a, p, s, launch);
+                default: return launch_tma<PREC, SOLVER, LIK, HIST_PACKED>(e, a, p, s, launch);
             }
-            BB_LAUNCH_CHECK();
-            return BLOND_OK;
         }
         // profile too long for the staged copy: plain loads below
     }
@@ -654,6 +765,7 @@ static ParticleArgs particle_args(blond_engine* e) {
     a.bc0 = e->bc0;
     a.lik_inv_w = e->lik_inv_w;
     a.bw = e->bw;
+    a.global_hist = global_hist(e) ? 1 : 0;
     return a;
 }
 
@@ -738,7 +850,8 @@ int blond_engine_create(blond_engine** out, int precision, int n_rf, int solver,
     BB_CHECK_SIZE(n_rf >= 1 && n_rf <= kMaxRfEngine, "engine_create: n_rf=%d not in [1, %d]",
                   n_rf, kMaxRfEngine);
     BB_CHECK_ARG(solver >= 0 && solver <= 2, "engine_create: solver %d", solver);
-    const int max_s = (device_info().max_smem_optin - (int)sizeof(TurnConsts) - 1024) / 4;
+    // beyond smem_hist_limit() slices the histogram lives in global memory
+    const int max_s = 1 << 22;
     BB_CHECK_SIZE(n_slices >= 2 && n_slices <= max_s,
                   "engine_create: n_slices=%d not in [2, %d]", n_slices, max_s);
     blond_engine* e = new blond_engine();

@@ -264,3 +264,106 @@ def test_fused_sharded_api_with_one_rank_matches_unsharded(cuda):
     for a, b in zip(*results):
         np.testing.assert_array_equal(a, b)
     np.testing.assert_array_equal(results[1][2], g["profiles"][-1])
+
+
+def _long_profile_case(precision, inductive, turns, n=300001, S=65536):
+    """Double RF, four resonators (+ inductive Z/n = 0.1 Ohm) on 2^16
+    slices: a profile too long for a shared-memory histogram, so the
+    particle kernel deposits into the global one."""
+    import cpu_oracle as o
+    from blond_b200.beam.distributions import _get_dE_from_dt, bigaussian_arrays
+    ring = Ring(6911.5, 1 / 18**2, 26e9, Proton(), turns)
+    rf = RFStation(ring, [4620, 4 * 4620], [4.5e6, 0.45e6], [0.0, np.pi], n_rf=2)
+    centre = (rf.phi_s[0] - rf.phi_rf[0, 0]) / rf.omega_rf[0, 0]
+    with pytest.warns(UserWarning):
+        sdE = _get_dE_from_dt(ring, rf, 0.4e-9)
+    dt0, dE0 = bigaussian_arrays(n, 0.4e-9, sdE, centre, 5)
+    beam = Beam(ring, n, 1e11, dt=dt0, dE=dE0)
+    prof = Profile(beam, CutOptions(cut_left=centre - 1.25e-9, cut_right=centre + 1.25e-9,
+                                    n_slices=S))
+    iv = InducedVoltageFreq(beam, prof, [Resonators([2e5, 1e5, 5e4, 3e4],
+                                                    [200e6, 800e6, 1.4e9, 2.0e9],
+                                                    [100.0, 1000.0, 3000.0, 30000.0])])
+    objs = [iv]
+    if inductive:
+        objs.append(InductiveImpedance(beam, prof, [0.1] * (turns + 1), rf))
+    tiv = TotalInducedVoltage(beam, prof, objs)
+    fused = FusedTracker(RingAndRFTracker(rf, beam), prof, tiv, precision=precision)
+    fused.track(turns)
+    fused.sync()
+    ref = o.track_oracle(
+        dt0, dE0, ring, rf, (prof.cut_left, prof.cut_right), prof.bin_centers, S, turns,
+        impedance=(iv.n_fft, iv.total_impedance.cpu().numpy()), intensity=1e11,
+        inductive=[0.1] * (turns + 1) if inductive else None)
+    return fused, beam, ref
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32p64"])
+def test_fused_2e16_slices_global_histogram(cuda, precision):
+    """Three turns on 2^16 slices (FFT length 65536) against the oracle:
+    FP64 to 1e-12 with exact counts; F32P64 counts may move by a few
+    particles."""
+    fused, beam, (odt, odE, oprof, ovind) = _long_profile_case(precision, False, 3)
+    dt, dE = beam.dt.cpu().numpy(), beam.dE.cpu().numpy()
+    got = fused.profile_tensor().cpu().numpy()
+    if precision == "f64":
+        assert normwise(dt, odt) < 1e-12 and normwise(dE, odE) < 1e-12
+        np.testing.assert_array_equal(got, oprof[-1])
+        assert normwise(fused.induced_voltage_tensor().cpu().numpy(), ovind[-1]) < 1e-10
+    else:
+        # bins are 38 fs wide: the float32 energy moves ~1e-3 of the
+        # particles into a neighbouring bin
+        assert normwise(dt, odt) < 1e-7
+        inwin = (odt > fused.profile.cut_left) & (odt < fused.profile.cut_right)
+        for a, b in ((dt, odt), (dE, odE)):
+            assert abs(np.std(a[inwin]) / np.std(b[inwin]) - 1) < 1e-5
+        assert got.sum() == oprof[-1].sum()
+        assert np.abs(got - oprof[-1]).sum() <= 0.01 * len(dt)
+
+
+def test_fused_2e16_slices_inductive(cuda):
+    """One FP64 turn of the same machine with the inductive term added.
+    With ~5 macro-particles per bin the derivative of the profile makes
+    |V_ind| ~1e8 V and interpolation slopes ~5e21 V/s; the reference's
+    kick form dE += dt*slope + (qV - bc*slope) (linear_interp_kick.cpp)
+    then cancels terms of max|bc*slope| ~1e13 eV, so one ulp of the induced
+    voltage moves dE by ~1e-3 eV.  The bar is therefore a few ulps of that
+    term, |dE - dE_oracle| <= 4e-15 max|bc*slope|."""
+    fused, beam, (odt, odE, oprof, ovind) = _long_profile_case("f64", True, 1)
+    vind = fused.induced_voltage_tensor().cpu().numpy()
+    assert normwise(vind, ovind[-1]) < 1e-12
+    np.testing.assert_array_equal(fused.profile_tensor().cpu().numpy(), oprof[-1])
+    bc = np.asarray(fused.profile.bin_centers)
+    slope = np.diff(ovind[-1]) * (len(bc) - 1) / (bc[-1] - bc[0])
+    bound = 4e-15 * np.abs(bc[:-1] * slope).max()
+    assert np.abs(beam.dE.cpu().numpy() - odE).max() <= bound
+    assert normwise(beam.dt.cpu().numpy(), odt) < 1e-10
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32p64"])
+def test_packed_histogram_counter_wraps(cuda, precision):
+    """2^16 slices take the packed 16-bit block histogram.  5e7 frozen
+    particles (no RF voltage, dE = 0: the coordinates never move), 45% in
+    bin 100 and 45% in bin 100 + 2^15 -- the two counters of one shared
+    word -- so every block wraps both counters more than once, and the
+    low counter's carries run into the high one.  The profile must still
+    be the exact histogram."""
+    import cpu_oracle as o
+    n, S, turns = 50_000_000, 65536, 2
+    ring = Ring(6911.5, 1 / 18**2, 26e9, Proton(), turns)
+    rf = RFStation(ring, [4620], [0.0], [0.0])
+    cl, cr = 0.0, 2.5e-9
+    w = (cr - cl) / S
+    rng = np.random.default_rng(7)
+    k = rng.choice(3, size=n, p=[0.45, 0.45, 0.10])
+    dt = np.where(k == 0, cl + 100.5 * w, cl + (100.5 + S // 2) * w)
+    dt = np.where(k == 2, rng.uniform(cl, cr, n), dt)
+    beam = Beam(ring, n, 1e11, dt=dt, dE=np.zeros(n))
+    prof = Profile(beam, CutOptions(cut_left=cl, cut_right=cr, n_slices=S))
+    fused = FusedTracker(RingAndRFTracker(rf, beam), prof, precision=precision)
+    fused.track(turns)
+    got = fused.profile_tensor().cpu().numpy()
+    want = o.histogram(dt, cl, cr, S)
+    assert got[100] > 2e7 and got[100 + S // 2] > 2e7
+    np.testing.assert_array_equal(got, want)
+    np.testing.assert_array_equal(fused.dt.cpu().numpy(), dt)
