@@ -96,6 +96,15 @@ _EXTRA = {
                                c_dbl, c_int] + [c_dbl] * 13 + [c_int, c_ptr, c_ptr,
                                                               c_i64, c_dbl, c_ptr,
                                                               c_ptr, c_ptr],
+    "blond_adjoint_deposit": [c_ptr, c_i64, c_int, c_dbl, c_dbl, c_ptr, c_ptr],
+    "blond_adjoint_forward_turn": [c_int, c_ptr, c_ptr, c_ptr, c_ptr, c_i64, c_int,
+                                   c_ptr, c_ptr, c_ptr, c_dbl, c_dbl, c_dbl, c_ptr,
+                                   c_int, c_dbl, c_dbl, c_ptr, c_ptr],
+    "blond_adjoint_backward_turn": [c_ptr, c_ptr, c_i64, c_ptr, c_ptr, c_ptr, c_int,
+                                    c_int, c_ptr, c_ptr, c_ptr, c_dbl, c_dbl, c_ptr,
+                                    c_int, c_dbl, c_dbl, c_ptr, c_ptr, c_ptr],
+    "blond_adjoint_spectral": [c_int, c_ptr, c_int, c_ptr, c_i64, c_dbl, c_ptr, c_ptr,
+                               c_ptr, c_ptr],
 }
 
 

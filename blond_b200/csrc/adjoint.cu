@@ -1,0 +1,471 @@
+// Differentiable N-turn map and its hand-written adjoint.
+//
+// One turn t of the forward map, in the reference main loop's order
+// (blond/impedances/impedance.py:113-146 then blond/trackers/tracker.py:
+// 521-615: induced voltage of the turn-start profile, linear_interp_kick,
+// RF kick, drift):
+//
+//   p_t      = CIC(dt_t)                          profile (counts)
+//   V_t      = -s irfft(Z rfft(p_t, n_fft))[:S]   induced voltage, s = q e ratio
+//   dE'      = dE_t + q interp(V_t; dt_t) + q sum_j V_j sin(w_j dt_t + phi_j) + acc_t
+//   dt_t+1   = dt_t + c_t dE',  dE_t+1 = dE'       simple drift, c_t from turn t+1
+//
+// CIC is cloud-in-cell deposition on the profile's bin centres
+// bc_k = bc_0 + k w: a particle at f = (dt - bc_0)/w gives 1 - u to bin
+// floor(f) and u = f - floor(f) to the next, so the profile is continuous
+// and piecewise linear in every dt.  (The reference's smooth_histogram,
+// blond/cpp_routines/histogram.cpp:75-132, moves a whole particle by two
+// bins where it crosses a bin centre, so its profile has no useful
+// derivative.)  interp(V; dt) = V_k (1 - u) + V_k+1 u on the same grid is
+// the function of linear_interp_kick.cpp:44-62, written without the
+// slope/offset cancellation.
+//
+// The adjoint of one turn, lambda = dL/d(state), runs backwards:
+//
+//   lambda_dt    += (lambda_p_t+1[k+1] - lambda_p_t+1[k]) / w   at dt_t+1
+//   lambda_dE'    = lambda_dE + c_t lambda_dt
+//   lambda_dt    += lambda_dE' q (sum_j V_j w_j cos(.) + (V_k+1 - V_k) / w)
+//   dL/dV_j,t    += sum_i lambda_dE' q sin(.)
+//   dL/dphi_j,t  += sum_i lambda_dE' q V_j cos(.)
+//   lambda_V[k]  += lambda_dE' q (1 - u),  lambda_V[k+1] += lambda_dE' q u
+//   lambda_dE     = lambda_dE'
+//
+// followed by lambda_p_t = A^T lambda_V (the same spectral kernel with
+// conj(Z): the transpose of a circular convolution is the correlation)
+// and the accumulation G += P_t conj(rfft(lambda_V)) from which the host
+// forms dL/dZ and, by the chain rule, dL/d(R_s, f_r, Q).  Everything on the
+// adjoint side runs in FP64; the forward keeps the engine's FP64 or
+// F32P64 (float dE, FP64 phase and drift) arithmetic.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "../../include/blond_b200.h"
+#include "common.cuh"
+#include "spectral.cuh"
+
+namespace bb {
+
+constexpr int kAdjThreads = 256;
+constexpr int kAdjMaxRf = 4;
+
+struct AdjTurn {
+    int64_t n;
+    int n_rf;
+    const double* V;   // this turn's n_rf amplitudes, frequencies, phases
+    const double* om;
+    const double* ph;
+    double acc, charge, drift_c;
+    const double* vind;  // S induced voltages of this turn, or nullptr
+    int S;
+    double bc0, inv_w;   // bin centres bc0 + k / inv_w
+    int smem_hist;       // 1: block-private histograms in shared memory
+    int fix_bits;        // fixed-point units per particle: 2^fix_bits
+};
+
+template <int PREC> struct AdjE;
+template <> struct AdjE<BLOND_PREC_F64> { using E = double; };
+template <> struct AdjE<BLOND_PREC_F32P64> { using E = float; };
+
+__device__ __forceinline__ double adj_reduce_2pi(double x) {
+    const double inv2pi = 0.15915494309189533577;
+    const double twopi = 6.28318530717958647692;
+    return fma(-rint(x * inv2pi), twopi, x);
+}
+
+// Cloud-in-cell deposit of a unit weight at dt, in fixed point with 2^b
+// units per particle: the weights are w1 = round(u 2^b) and w0 = 2^b - w1,
+// accumulated with integer atomics, so every particle deposits exactly one
+// unit and the profile does not depend on the order of the atomics (a run
+// repeats bit for bit, which finite-difference checks of the map rely
+// on).  b = min(52, 62 - ceil(log2(n + 1))) keeps n units below 2^63.
+typedef unsigned long long u64;
+
+inline int fixed_bits(int64_t n) {
+    int lg = 0;
+    while (lg < 63 && (1ull << lg) < (u64)n + 1) ++lg;
+    return std::min(52, 62 - lg);
+}
+
+__device__ __forceinline__ void cic_deposit(u64* h, int S, double t, double bc0,
+                                            double inv_w, int bits) {
+    const double f = (t - bc0) * inv_w;
+    if (!(f > -1.0 && f < (double)S)) return;  // also drops NaN
+    const double fl = floor(f);
+    const int j = (int)fl;
+    const u64 w1 = (u64)llrint(ldexp(f - fl, bits));
+    const u64 w0 = (1ull << bits) - w1;
+    if (j >= 0 && w0) atomicAdd(&h[j], w0);
+    if (j + 1 < S && w1) atomicAdd(&h[j + 1], w1);
+}
+
+__device__ __forceinline__ void zero_shared(u64* h, int S) {
+    for (int k = threadIdx.x; k < S; k += blockDim.x) h[k] = 0ull;
+}
+__device__ __forceinline__ void flush_shared(const u64* h, u64* g, int S) {
+    for (int k = threadIdx.x; k < S; k += blockDim.x)
+        if (h[k]) atomicAdd(&g[k], h[k]);
+}
+__device__ __forceinline__ void zero_shared(double* h, int S) {
+    for (int k = threadIdx.x; k < S; k += blockDim.x) h[k] = 0.0;
+}
+__device__ __forceinline__ void flush_shared(const double* h, double* g, int S) {
+    for (int k = threadIdx.x; k < S; k += blockDim.x)
+        if (h[k] != 0.0) atomicAdd(&g[k], h[k]);
+}
+
+// The profile array is accumulated in place as fixed point (its zero bit
+// pattern is 0.0) and converted to counts afterwards.
+__global__ void fixed_to_counts_kernel(double* p, int S, int bits) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < S; k += gridDim.x * blockDim.x)
+        p[k] = ldexp((double)reinterpret_cast<const u64*>(p)[k], -bits);
+}
+
+__global__ void __launch_bounds__(kAdjThreads)
+adj_deposit_kernel(const double* __restrict__ dt, int64_t n, int S, double bc0, double inv_w,
+                   int smem_hist, int bits, u64* __restrict__ prof) {
+    extern __shared__ u64 shq[];
+    u64* sh = shq;
+    u64* h = smem_hist ? sh : prof;
+    if (smem_hist) zero_shared(sh, S);
+    __syncthreads();
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        cic_deposit(h, S, dt[i], bc0, inv_w, bits);
+    __syncthreads();
+    if (smem_hist) flush_shared(sh, prof, S);
+}
+
+template <int PREC>
+__global__ void __launch_bounds__(kAdjThreads)
+adj_forward_kernel(const AdjTurn T, const double* __restrict__ dt_in,
+                   const void* __restrict__ dE_in, double* __restrict__ dt_out,
+                   void* __restrict__ dE_out, u64* __restrict__ prof_out) {
+    using E = typename AdjE<PREC>::E;
+    extern __shared__ u64 shf[];
+    u64* sh = shf;
+    __shared__ double sV[kAdjMaxRf], sOm[kAdjMaxRf], sPh[kAdjMaxRf];
+    if (threadIdx.x < T.n_rf) {
+        sV[threadIdx.x] = T.V[threadIdx.x];
+        sOm[threadIdx.x] = T.om[threadIdx.x];
+        sPh[threadIdx.x] = T.ph[threadIdx.x];
+    }
+    const bool dep = prof_out != nullptr;
+    u64* h = T.smem_hist ? sh : prof_out;
+    if (dep && T.smem_hist) zero_shared(sh, T.S);
+    __syncthreads();
+    const E* dEi = static_cast<const E*>(dE_in);
+    E* dEo = static_cast<E*>(dE_out);
+    const double q = T.charge;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < T.n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        double t = dt_in[i];
+        E e = dEi[i];
+        if (T.vind) {
+            const double f = (t - T.bc0) * T.inv_w;
+            if (f >= 0.0 && f < (double)(T.S - 1)) {
+                const double fl = floor(f);
+                const int k = (int)fl;
+                const double u = f - fl;
+                e += (E)(q * (T.vind[k] * (1.0 - u) + T.vind[k + 1] * u));
+            }
+        }
+        if (PREC == BLOND_PREC_F64) {
+            double s = 0.0;
+#pragma unroll
+            for (int j = 0; j < kAdjMaxRf; ++j)
+                if (j < T.n_rf) s += sV[j] * sin(fma(sOm[j], t, sPh[j]));
+            e += (E)(q * s + T.acc);
+        } else {
+            float s = 0.0f;
+#pragma unroll
+            for (int j = 0; j < kAdjMaxRf; ++j)
+                if (j < T.n_rf)
+                    s += (float)sV[j] * sinf((float)adj_reduce_2pi(fma(sOm[j], t, sPh[j])));
+            e += (E)q * s + (E)T.acc;
+        }
+        t = t + T.drift_c * (double)e;
+        dt_out[i] = t;
+        dEo[i] = e;
+        if (dep) cic_deposit(h, T.S, t, T.bc0, T.inv_w, T.fix_bits);
+    }
+    if (dep && T.smem_hist) {
+        __syncthreads();
+        flush_shared(sh, prof_out, T.S);
+    }
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// One backward turn (kick = 1), or only the deposit adjoint of a profile
+// at dt_next (kick = 0).  Shared memory: lambda_p_next copy, then the
+// block's lambda_V accumulator (S doubles each, when smem_hist).
+__global__ void __launch_bounds__(kAdjThreads)
+adj_backward_kernel(const AdjTurn T, int kick, const double* __restrict__ dt,
+                    const double* __restrict__ dt_next, const double* __restrict__ lam_p_next,
+                    double* __restrict__ lam_dt, double* __restrict__ lam_dE,
+                    double* __restrict__ lam_v, double* __restrict__ grad_rf) {
+    extern __shared__ double sh[];
+    __shared__ double sV[kAdjMaxRf], sOm[kAdjMaxRf], sPh[kAdjMaxRf];
+    __shared__ double red[kAdjThreads / 32][2 * kAdjMaxRf];
+    const int S = T.S;
+    const bool sm = T.smem_hist != 0;
+    double* lp = sm ? sh : const_cast<double*>(lam_p_next);
+    double* lv = sm ? sh + S : lam_v;
+    if (kick && threadIdx.x < T.n_rf) {
+        sV[threadIdx.x] = T.V[threadIdx.x];
+        sOm[threadIdx.x] = T.om[threadIdx.x];
+        sPh[threadIdx.x] = T.ph[threadIdx.x];
+    }
+    if (sm) {
+        for (int k = threadIdx.x; k < S; k += blockDim.x) {
+            sh[k] = lam_p_next ? lam_p_next[k] : 0.0;
+            sh[S + k] = 0.0;
+        }
+    }
+    __syncthreads();
+    const double q = T.charge;
+    double gv[kAdjMaxRf], gp[kAdjMaxRf];
+#pragma unroll
+    for (int j = 0; j < kAdjMaxRf; ++j) gv[j] = gp[j] = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < T.n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        double ldt = lam_dt[i];
+        double ldE = lam_dE[i];
+        if (lam_p_next) {
+            const double f = (dt_next[i] - T.bc0) * T.inv_w;
+            if (f > -1.0 && f < (double)S) {
+                const int j = (int)floor(f);
+                const double a = j >= 0 ? lp[j] : 0.0;
+                const double b = j + 1 < S ? lp[j + 1] : 0.0;
+                ldt += (b - a) * T.inv_w;
+            }
+        }
+        if (kick) {
+            const double t = dt[i];
+            const double lE = ldE + T.drift_c * ldt;
+            double dg = 0.0;
+#pragma unroll
+            for (int j = 0; j < kAdjMaxRf; ++j) {
+                if (j < T.n_rf) {
+                    double s, c;
+                    sincos(adj_reduce_2pi(fma(sOm[j], t, sPh[j])), &s, &c);
+                    dg += sV[j] * sOm[j] * c;
+                    gv[j] += lE * s;
+                    gp[j] += lE * sV[j] * c;
+                }
+            }
+            dg *= q;
+            if (T.vind) {
+                const double f = (t - T.bc0) * T.inv_w;
+                if (f >= 0.0 && f < (double)(S - 1)) {
+                    const double fl = floor(f);
+                    const int k = (int)fl;
+                    const double u = f - fl;
+                    dg += q * (T.vind[k + 1] - T.vind[k]) * T.inv_w;
+                    atomicAdd(&lv[k], lE * q * (1.0 - u));
+                    atomicAdd(&lv[k + 1], lE * q * u);
+                }
+            }
+            ldt += lE * dg;
+            ldE = lE;
+        }
+        lam_dt[i] = ldt;
+        lam_dE[i] = ldE;
+    }
+    if (kick) {
+        // programme gradients: warp sums, then one atomic per block and value
+        const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+        for (int j = 0; j < kAdjMaxRf; ++j) {
+            const double a = warp_sum(gv[j]), b = warp_sum(gp[j]);
+            if (lane == 0) {
+                red[w][j] = a;
+                red[w][kAdjMaxRf + j] = b;
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x < 2 * T.n_rf) {
+            const int j = threadIdx.x < T.n_rf ? threadIdx.x : kAdjMaxRf + threadIdx.x - T.n_rf;
+            double s = 0.0;
+            for (int r = 0; r < (int)(blockDim.x >> 5); ++r) s += red[r][j];
+            atomicAdd(&grad_rf[threadIdx.x], q * s);
+        }
+        if (sm) flush_shared(lv, lam_v, S);
+    }
+}
+
+static int adj_smem_limit() { return (device_info().max_smem_optin - 4096) / 16; }
+
+template <typename K>
+static int adj_allow_smem(K kernel, bool* done) {
+    const DeviceInfo& d = device_info();
+    if (!done[d.device & 63]) {
+        cudaFuncAttributes fa;
+        BB_CUDA(cudaFuncGetAttributes(&fa, kernel));
+        BB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     d.max_smem_optin - (int)fa.sharedSizeBytes));
+        done[d.device & 63] = true;
+    }
+    return BLOND_OK;
+}
+
+}  // namespace bb
+
+using namespace bb;
+
+extern "C" {
+
+int blond_adjoint_deposit(const double* dt, int64_t n, int n_slices, double bin_center0,
+                          double inv_bin_width, double* profile, void* stream) {
+    BB_CHECK_ARG(n >= 0 && n_slices >= 1, "adjoint_deposit: bad size");
+    BB_CHECK_ARG(profile && (n == 0 || dt), "adjoint_deposit: null pointer");
+    if (n == 0) return BLOND_OK;
+    static bool done[64] = {false};
+    int rc;
+    if ((rc = adj_allow_smem(adj_deposit_kernel, done))) return rc;
+    const int sm = n_slices <= adj_smem_limit() ? 1 : 0;
+    const int grid = particle_grid(n, kAdjThreads, 4);
+    cudaStream_t s = as_stream(stream);
+    adj_deposit_kernel<<<grid, kAdjThreads, sm ? sizeof(u64) * n_slices : 0, s>>>(
+        dt, n, n_slices, bin_center0, inv_bin_width, sm, fixed_bits(n),
+        reinterpret_cast<u64*>(profile));
+    BB_LAUNCH_CHECK();
+    fixed_to_counts_kernel<<<(n_slices + 255) / 256, 256, 0, s>>>(profile, n_slices,
+                                                                  fixed_bits(n));
+    BB_LAUNCH_CHECK();
+    return BLOND_OK;
+}
+
+int blond_adjoint_forward_turn(int precision, const double* dt_in, const void* dE_in,
+                               double* dt_out, void* dE_out, int64_t n, int n_rf,
+                               const double* voltage, const double* omega_rf,
+                               const double* phi_rf, double acc_kick, double charge,
+                               double drift_coeff, const double* induced_voltage,
+                               int n_slices, double bin_center0, double inv_bin_width,
+                               double* profile_out, void* stream) {
+    BB_CHECK_ARG(precision == BLOND_PREC_F64 || precision == BLOND_PREC_F32P64,
+                 "adjoint_forward_turn: unknown precision %d", precision);
+    BB_CHECK_SIZE(n_rf >= 0 && n_rf <= kAdjMaxRf, "adjoint_forward_turn: n_rf=%d not in "
+                  "[0, %d]", n_rf, kAdjMaxRf);
+    BB_CHECK_ARG(n >= 0 && n_slices >= 2, "adjoint_forward_turn: bad size");
+    BB_CHECK_ARG((n == 0 || (dt_in && dE_in && dt_out && dE_out)) &&
+                     (n_rf == 0 || (voltage && omega_rf && phi_rf)),
+                 "adjoint_forward_turn: null pointer");
+    if (n == 0) return BLOND_OK;
+    AdjTurn T = {};
+    T.n = n;
+    T.n_rf = n_rf;
+    T.V = voltage;
+    T.om = omega_rf;
+    T.ph = phi_rf;
+    T.acc = acc_kick;
+    T.charge = charge;
+    T.drift_c = drift_coeff;
+    T.vind = induced_voltage;
+    T.S = n_slices;
+    T.bc0 = bin_center0;
+    T.inv_w = inv_bin_width;
+    T.smem_hist = n_slices <= adj_smem_limit() ? 1 : 0;
+    T.fix_bits = fixed_bits(n);
+    const size_t smem = profile_out && T.smem_hist ? sizeof(u64) * n_slices : 0;
+    const int grid = particle_grid(n, kAdjThreads, 4);
+    cudaStream_t s = as_stream(stream);
+    int rc;
+    if (precision == BLOND_PREC_F64) {
+        static bool done[64] = {false};
+        if ((rc = adj_allow_smem(adj_forward_kernel<BLOND_PREC_F64>, done))) return rc;
+        adj_forward_kernel<BLOND_PREC_F64><<<grid, kAdjThreads, smem, s>>>(
+            T, dt_in, dE_in, dt_out, dE_out, reinterpret_cast<u64*>(profile_out));
+    } else {
+        static bool done[64] = {false};
+        if ((rc = adj_allow_smem(adj_forward_kernel<BLOND_PREC_F32P64>, done))) return rc;
+        adj_forward_kernel<BLOND_PREC_F32P64><<<grid, kAdjThreads, smem, s>>>(
+            T, dt_in, dE_in, dt_out, dE_out, reinterpret_cast<u64*>(profile_out));
+    }
+    BB_LAUNCH_CHECK();
+    if (profile_out) {
+        fixed_to_counts_kernel<<<(n_slices + 255) / 256, 256, 0, s>>>(profile_out, n_slices,
+                                                                      T.fix_bits);
+        BB_LAUNCH_CHECK();
+    }
+    return BLOND_OK;
+}
+
+int blond_adjoint_backward_turn(const double* dt, const double* dt_next, int64_t n,
+                                double* lam_dt, double* lam_dE, const double* lam_p_next,
+                                int kick, int n_rf, const double* voltage,
+                                const double* omega_rf, const double* phi_rf, double charge,
+                                double drift_coeff, const double* induced_voltage,
+                                int n_slices, double bin_center0, double inv_bin_width,
+                                double* lam_v, double* grad_rf, void* stream) {
+    BB_CHECK_SIZE(n_rf >= 0 && n_rf <= kAdjMaxRf, "adjoint_backward_turn: n_rf=%d not in "
+                  "[0, %d]", n_rf, kAdjMaxRf);
+    BB_CHECK_ARG(n >= 0 && n_slices >= 2, "adjoint_backward_turn: bad size");
+    BB_CHECK_ARG(n == 0 || (lam_dt && lam_dE), "adjoint_backward_turn: null adjoint");
+    BB_CHECK_ARG(!lam_p_next || dt_next, "adjoint_backward_turn: lam_p_next needs dt_next");
+    BB_CHECK_ARG(!kick || ((n == 0 || dt) && grad_rf && (!induced_voltage || lam_v) &&
+                           (n_rf == 0 || (voltage && omega_rf && phi_rf))),
+                 "adjoint_backward_turn: null pointer");
+    if (n == 0) return BLOND_OK;
+    AdjTurn T = {};
+    T.n = n;
+    T.n_rf = n_rf;
+    T.V = voltage;
+    T.om = omega_rf;
+    T.ph = phi_rf;
+    T.charge = charge;
+    T.drift_c = drift_coeff;
+    T.vind = kick ? induced_voltage : nullptr;
+    T.S = n_slices;
+    T.bc0 = bin_center0;
+    T.inv_w = inv_bin_width;
+    T.smem_hist = n_slices <= adj_smem_limit() ? 1 : 0;
+    static bool done[64] = {false};
+    int rc;
+    if ((rc = adj_allow_smem(adj_backward_kernel, done))) return rc;
+    const size_t smem = T.smem_hist ? 2 * sizeof(double) * n_slices : 0;
+    const int grid = particle_grid(n, kAdjThreads, 4);
+    adj_backward_kernel<<<grid, kAdjThreads, smem, as_stream(stream)>>>(
+        T, kick, dt, dt_next, lam_p_next, lam_dt, lam_dE, lam_v, grad_rf);
+    BB_LAUNCH_CHECK();
+    return BLOND_OK;
+}
+
+int blond_adjoint_spectral(int mode, const double* x, int n_slices, const double* impedance,
+                           int64_t n_fft, double scale, double* y, double* spectrum,
+                           double* accum, void* stream) {
+    BB_CHECK_ARG(mode == 0 || mode == 1, "adjoint_spectral: mode must be 0 or 1");
+    BB_CHECK_ARG(x && impedance && y && n_slices >= 1, "adjoint_spectral: bad argument");
+    BB_CHECK_ARG(mode == 0 || (spectrum && accum), "adjoint_spectral: mode 1 needs the "
+                 "stored spectrum and the accumulator");
+    SpecParams P = {};
+    if (!make_spec_plan(n_fft, P.p)) {
+        set_error("adjoint_spectral: n_fft=%lld is not an even 5-smooth length <= %lld",
+                  (long long)n_fft, (long long)kMaxClusterFFT);
+        return BLOND_ERR_UNSUPPORTED;
+    }
+    P.mode = SPEC_FORWARD | SPEC_MULTIPLY | SPEC_INVERSE;
+    P.in_f64 = x;
+    P.n_in = n_slices;
+    P.H = reinterpret_cast<const double2*>(impedance);
+    P.out = y;
+    P.n_out = n_slices < n_fft ? n_slices : n_fft;
+    P.out_scale = -scale / (double)P.p.M;
+    if (mode == 0 && spectrum) {
+        P.mode |= SPEC_OUT_SPECTRUM;
+        P.spec_out = reinterpret_cast<double2*>(spectrum);
+    }
+    if (mode == 1) {
+        P.mode |= SPEC_ACCUM;
+        P.acc_a = reinterpret_cast<const double2*>(spectrum);
+        P.acc_g = reinterpret_cast<double2*>(accum);
+    }
+    return launch_spectral(P, as_stream(stream));
+}
+
+}  // extern "C"

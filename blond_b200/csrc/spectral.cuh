@@ -63,6 +63,7 @@ enum : int {
     SPEC_OUT_SPECTRUM = 4,// write the N/2+1 spectrum of the real input
     SPEC_IN_SPECTRUM = 8, // input is an N/2+1 spectrum (irfft only)
     SPEC_MULTIPLY = 16,   // multiply the spectrum by H before inverting
+    SPEC_ACCUM = 32,      // acc_g[k] += acc_a[k] * conj(X[k]) over the spectrum
 };
 
 struct SpecParams {
@@ -102,6 +103,11 @@ struct SpecParams {
     int batch;
     const double* beam_scale;
     const double* beam_inv_w;
+    // SPEC_ACCUM (M + 1 values each): the adjoint of the induced voltage
+    // with respect to the impedance needs sum_turns P_t[k] conj(L_t[k]),
+    // P_t the profile spectrum and L_t the spectrum of this input
+    const double2* acc_a;
+    double2* acc_g;
 };
 
 // Device code below is compiled only in spectral.cu (which defines
@@ -500,6 +506,10 @@ spectral_kernel(const SpecParams P) {
                     // every k < M is owned once; X[M] comes from k == 0
                     P.spec_out[k] = Yk;
                     if (k == 0) P.spec_out[M] = Yp;
+                }
+                if (P.mode & SPEC_ACCUM) {
+                    P.acc_g[k] = cadd(P.acc_g[k], cmul(P.acc_a[k], cconj(Yk)));
+                    if (k == 0) P.acc_g[M] = cadd(P.acc_g[M], cmul(P.acc_a[M], cconj(Yp)));
                 }
             }
             if (P.mode & SPEC_MULTIPLY) {

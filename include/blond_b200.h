@@ -309,6 +309,59 @@ int blond_turn_f64_noalloc(double* dt, double* dE, int64_t n, int n_rf,
                            int64_t n_fft, double iv_scale, double* profile_out,
                            double* induced_voltage_out, void* stream);
 
+/* ------------------------------------------------------------ adjoint segment
+ * No counterpart in the reference (it has no derivatives).  The building
+ * blocks of a differentiable N-turn map -- profile by cloud-in-cell
+ * deposition, induced voltage, interpolated kick, RF kick, simple drift --
+ * and of its adjoint, driven turn by turn by a host that checkpoints the
+ * coordinates every K turns (blond_b200/adjoint.py).  Coordinates are
+ * device arrays: dt double, dE double (BLOND_PREC_F64) or float
+ * (BLOND_PREC_F32P64); adjoints are double.  The bin grid is the profile's
+ * bin centres bin_center0 + k / inv_bin_width, k < n_slices; cloud-in-cell
+ * gives a particle at f = (dt - bin_center0) * inv_bin_width the weight
+ * 1 - (f - floor f) in bin floor f and the rest in the next bin.
+ * voltage / omega_rf / phi_rf point at this turn's n_rf (<= 4) device
+ * values; drift_coeff = t_rev length_ratio eta_0 / (beta^2 E) of turn + 1. */
+
+/* profile (n_slices zeros on entry) = cloud-in-cell deposit of dt, with
+ * weights rounded to multiples of 2^-b, b = min(52, 62 - ceil(log2(n+1))),
+ * so that every run gives the same bits (integer accumulation, independent
+ * of the order of the atomics) */
+int blond_adjoint_deposit(const double* dt, int64_t n, int n_slices, double bin_center0,
+                          double inv_bin_width, double* profile, void* stream);
+/* one forward turn: induced_voltage (n_slices values, or NULL) kick,
+ * RF kick, drift, then profile_out (zeros on entry, or NULL: none) = the
+ * deposit of the new dt as above; dt_out / dE_out may alias dt_in / dE_in */
+int blond_adjoint_forward_turn(int precision, const double* dt_in, const void* dE_in,
+                               double* dt_out, void* dE_out, int64_t n, int n_rf,
+                               const double* voltage, const double* omega_rf,
+                               const double* phi_rf, double acc_kick, double charge,
+                               double drift_coeff, const double* induced_voltage,
+                               int n_slices, double bin_center0, double inv_bin_width,
+                               double* profile_out, void* stream);
+/* one backward turn.  On entry lam_dt / lam_dE hold dL/d(dt, dE) at turn
+ * t+1 and lam_p_next dL/d(profile at turn t+1) (deposited at dt_next, or
+ * NULL); on exit they hold dL/d(dt, dE) at turn t excluding the turn-t
+ * profile.  lam_v += dL/d(induced voltage of turn t); grad_rf[j] +=
+ * dL/dV_j and grad_rf[n_rf + j] += dL/dphi_j of this turn.  kick = 0 only
+ * adds the deposit adjoint of lam_p_next at dt_next. */
+int blond_adjoint_backward_turn(const double* dt, const double* dt_next, int64_t n,
+                                double* lam_dt, double* lam_dE, const double* lam_p_next,
+                                int kick, int n_rf, const double* voltage,
+                                const double* omega_rf, const double* phi_rf, double charge,
+                                double drift_coeff, const double* induced_voltage,
+                                int n_slices, double bin_center0, double inv_bin_width,
+                                double* lam_v, double* grad_rf, void* stream);
+/* mode 0: y = -scale irfft(Z rfft(x, n_fft))[:n_slices] (the induced
+ *         voltage), spectrum (n_fft/2+1 complex, or NULL) = rfft(x, n_fft);
+ * mode 1: the transpose, with impedance = conj(Z):
+ *         y = -scale irfft(conj(Z) rfft(x))[:n_slices], and
+ *         accum[k] += spectrum[k] conj(rfft(x)[k]).
+ * Cluster transform lengths only (even 5-smooth n_fft <= 131072). */
+int blond_adjoint_spectral(int mode, const double* x, int n_slices, const double* impedance,
+                           int64_t n_fft, double scale, double* y, double* spectrum,
+                           double* accum, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
