@@ -53,9 +53,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--kernel", default="auto", choices=["auto", "tma", "plain"])
-    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c5"],
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5"],
                     help="c2: the single-beam pipeline (default, the headline); "
-                         "c3: 256-beam double-RF batch; c5: 1e8 particles, "
+                         "c3: 256-beam double-RF batch; c4: adjoint gradient; "
+                         "c5: 1e8 particles, "
                          "2^16 slices, 4 resonators + inductive Z/n")
     ap.add_argument("--beams", type=int, default=256)
     return ap.parse_args()
@@ -304,6 +305,7 @@ def run_ours(args, world, rank, local):
         "dtype": args.precision, "data": "synthetic",
         "config": {"workload": WORKLOAD, "particles": n, "slices": S, "n_fft": n_fft,
                    "intensity": 1e10, "turns_per_graph": 50,
+                   "autotuned": fused.tuned,
                    "l2": f"inputs larger than L2: {alg_bytes // 2 / 1e6:.0f} MB of dt/dE read per turn",
                    "parallelism": (f"dp{world}: one beam of {world} x {n:.0e} particles, "
                                    "int32 histogram all-reduce (NCCL) per turn")
@@ -333,7 +335,8 @@ def run_ours(args, world, rank, local):
         ach32 = BYTES_PER_PARTICLE["f32p64"] * n / (p32 / kt * 1e-3) / 1e9
         out["mixed_precision"] = {"dtype": "f32p64", "value": n * K / (ms32 * 1e-3),
                                   "ms_per_step": ms32 / K, "kernel_ms": p32 / kt,
-                                  "achieved_gbs": ach32, "frac": ach32 / peak}
+                                  "achieved_gbs": ach32, "frac": ach32 / peak,
+                                  "autotuned": fm.tuned}
         del fm, bm_
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, turns, kind, cores, sec = cpu_reference(n, S, None, args.cpu_seconds)
@@ -529,7 +532,7 @@ def run_c5(args):
         res[prec] = {"value": n * K / (ms * 1e-3), "ms_per_step": ms / K,
                      "kernel_ms": part_ms / kt, "head_kernel_ms": head_ms / kt,
                      "achieved_gbs": ach, "frac": ach / peak, "clocks": clk,
-                     "kernel": fused.kernel}
+                     "kernel": fused.kernel, "autotuned": fused.tuned}
         del fused, beam, prof
         torch.cuda.empty_cache()
     r = res["f32p64"]
@@ -545,7 +548,8 @@ def run_c5(args):
                      "kernel": f"particle_kernel{'_tma' if r['kernel'] == 'tma' else ''} "
                                "(global-memory histogram)",
                      "kernel_ms": r["kernel_ms"], "head_kernel_ms": r["head_kernel_ms"],
-                     "bytes_per_particle": BYTES_PER_PARTICLE["f32p64"]},
+                     "bytes_per_particle": BYTES_PER_PARTICLE["f32p64"],
+                     "autotuned": r["autotuned"]},
         "f64": {k: res["f64"][k] for k in ("value", "ms_per_step", "kernel_ms",
                                             "head_kernel_ms", "achieved_gbs", "frac")},
         "f32p64_rel_err_after_turns": {
@@ -557,8 +561,81 @@ def run_c5(args):
     }
 
 
+C4_WORKLOAD = ("adjoint: 2e6 protons 26 GeV/c, h=4620 4.5 MV, 1024 slices over 2.5 ns "
+               "(cloud-in-cell), broadband resonator 1 MOhm/1 GHz/Q=1 at intensity 3e9, "
+               "500 turns, checkpoints every 50; loss = RMS bunch length^2 (ns^2) + L2 "
+               "profile mismatch to a 0.35 ns Gaussian; gradients w.r.t. V[500], "
+               "phi[500], R_s, f_r, Q")
+
+
+def run_c4(args):
+    """Gradient throughput (forward + backward, particle-turns/s counted
+    once per turn of the map) in F32P64 and FP64, and the F32P64 gradient
+    against the FP64 one."""
+    import torch
+    from blond_b200.adjoint import AdjointTracker, bunch_loss, gaussian_target
+    n, S, T = 2_000_000, 1024, 500
+    ring, rf = machine(T)
+    dt0, dE0, centre = host_bunch(ring, rf, n, seed=3)
+    cl, cr = centre - 1.25e-9, centre + 1.25e-9
+    W, K = max(3, min(args.warmup, 3)), max(1, min(args.steps, 5))
+    out, grads = {}, {}
+    for prec in ("f32p64", "f64"):
+        tr = AdjointTracker(ring, rf, n, 3e9, cl, cr, S, T, precision=prec,
+                            checkpoint_every=50)
+        target = gaussian_target(S, cl, cr, centre, 0.35e-9)
+        dtt = torch.tensor(dt0, device="cuda")
+        dEt = torch.tensor(dE0, device="cuda")
+
+        def step():
+            V = torch.full((T, 1), 4.5e6, dtype=torch.float64, device="cuda",
+                           requires_grad=True)
+            P = torch.zeros(T, 1, dtype=torch.float64, device="cuda", requires_grad=True)
+            R, fr, Q = (torch.tensor([x], dtype=torch.float64, device="cuda",
+                                     requires_grad=True) for x in (1e6, 1e9, 1.0))
+            _, _, p = tr(dtt, dEt, V, P, tr.impedance(R, fr, Q))
+            L = bunch_loss(p, target, tr.bin_centers())
+            L.backward()
+            return [x.grad for x in (V, P, R, fr, Q)]
+
+        for _ in range(W):
+            step()
+        torch.cuda.synchronize()
+        s = torch.cuda.current_stream()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s)
+        for _ in range(K):
+            g = step()
+        b.record(s)
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / K
+        grads[prec] = [x.detach().cpu().numpy().ravel() for x in g]
+        out[prec] = {"ms_per_gradient": ms, "value": n * T / (ms * 1e-3)}
+        del tr
+        torch.cuda.empty_cache()
+    names = ("V", "phi", "R_s", "f_r", "Q")
+    err = {k: float(np.abs(a_ - b_).max() / np.abs(b_).max())
+           for k, a_, b_ in zip(names, grads["f32p64"], grads["f64"])}
+    r = out["f32p64"]
+    return {
+        "metric": "particle-turns/s of the gradient (forward + adjoint) on 1 B200",
+        "value": r["value"], "unit": UNIT, "n_gpus": 1, "steps": K, "warmup": W,
+        "ms_per_step": r["ms_per_gradient"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32p64", "data": "synthetic",
+        "config": {"workload": C4_WORKLOAD, "particles": n, "slices": S, "turns": T},
+        "f64": out["f64"],
+        "f32p64_gradient_vs_f64": {"statistic": "max|g32 - g64| / max|g64| per parameter "
+                                                "after 500 turns", **err},
+        "fd_check": "tests/test_gpu_adjoint.py: FP64 adjoint vs central differences "
+                    "of the FP64 forward within 1e-4 at this size",
+    }
+
+
 def main():
     args = parse()
+    if args.workload == "c4" and args.impl == "ours":
+        print(json.dumps(run_c4(args)), flush=True)
+        return
     if args.workload == "c5" and args.impl == "ours":
         print(json.dumps(run_c5(args)), flush=True)
         return

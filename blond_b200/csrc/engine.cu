@@ -98,7 +98,7 @@ __device__ __forceinline__ void track_one(double& t,
                 } else {
                     const float2 tb = __ldg(reinterpret_cast<const float2*>(a.table) + k);
                     const float x = (float)(t - (a.bc0 + (double)k * a.bw));
-                    e += tb.x + tb.y * x;
+                    e += __fmaf_rn(tb.y, x, tb.x);
                 }
             }
         }
@@ -138,6 +138,7 @@ __device__ __forceinline__ void track_pair(double& t0, double& t1,
     using TB = typename Vec2<E>::type;
     bool in0 = false, in1 = false;
     TB tb0, tb1;
+    float x0f = 0.0f, x1f = 0.0f;  // F32P64: offsets from the slice centre
     if (LIK) {
         const double f0 = floor((t0 - a.bc0) * a.lik_inv_w);
         const double f1 = floor((t1 - a.bc0) * a.lik_inv_w);
@@ -148,8 +149,8 @@ __device__ __forceinline__ void track_pair(double& t0, double& t1,
         tb1 = __ldg(reinterpret_cast<const TB*>(a.table) + k1);
         if (PREC == PREC_F32P64) {
             // offsets from the slice centre, needed before t changes
-            tb0.y = tb0.y * (float)(t0 - (a.bc0 + (double)k0 * a.bw));
-            tb1.y = tb1.y * (float)(t1 - (a.bc0 + (double)k1 * a.bw));
+            x0f = (float)(t0 - (a.bc0 + (double)k0 * a.bw));
+            x1f = (float)(t1 - (a.bc0 + (double)k1 * a.bw));
         }
     }
     E s0, s1;
@@ -175,8 +176,8 @@ __device__ __forceinline__ void track_pair(double& t0, double& t1,
             if (in0) e0 += t0 * tb0.x + tb0.y;
             if (in1) e1 += t1 * tb1.x + tb1.y;
         } else {
-            if (in0) e0 += tb0.x + tb0.y;
-            if (in1) e1 += tb1.x + tb1.y;
+            if (in0) e0 += __fmaf_rn(tb0.y, x0f, tb0.x);
+            if (in1) e1 += __fmaf_rn(tb1.y, x1f, tb1.x);
         }
     }
     const E q = (E)a.charge, acc = (E)c.acc;
@@ -582,6 +583,7 @@ struct blond_engine {
     int blocks_per_sm = 2;
     int turns_per_graph = 50;
     int variant = 0;  // 0: TMA-pipelined particle pass, 1: plain loads
+    int hist_mode = -1;  // -1 automatic, else HIST_AGG/I32/PACKED/GLOBAL
     // graph cache
     cudaStream_t cap_stream = nullptr;
     cudaGraphExec_t graph = nullptr;
@@ -601,8 +603,21 @@ static int smem_hist_limit() {
     return (device_info().max_smem_optin - (int)sizeof(TurnConsts) - 1024) / 4;
 }
 static bool global_hist(const blond_engine* e) { return e->S > smem_hist_limit(); }
+
+// Histogram layout of the plain pass: straight into global memory when
+// asked for or when one int per bin does not fit in shared memory, else
+// block-private, warp-aggregated when asked for or for short profiles.
+enum { HIST_GLOBAL = 3 };
+static bool plain_global(const blond_engine* e) {
+    return global_hist(e) || e->hist_mode == HIST_GLOBAL;
+}
+static bool plain_agg(const blond_engine* e) {
+    if (e->hist_mode == HIST_AGG) return true;
+    if (e->hist_mode == HIST_I32) return false;
+    return e->S <= 2048;
+}
 static int engine_smem(const blond_engine* e) {
-    return global_hist(e) ? 0 : (int)sizeof(int) * e->S;
+    return plain_global(e) ? 0 : (int)sizeof(int) * e->S;
 }
 
 // Raise a kernel's dynamic shared memory limit to the device's opt-in
@@ -635,7 +650,7 @@ struct TmaPlan {
 };
 
 template <int PREC>
-static TmaPlan tma_plan(int S) {
+static TmaPlan tma_plan(int S, int forced) {
     using E = typename Coord<PREC>::E;
     const size_t stage = (size_t)kTile * (sizeof(double) + sizeof(E));
     // static shared memory of the kernel (TurnConsts, barriers) + margin
@@ -651,6 +666,23 @@ static TmaPlan tma_plan(int S) {
     const size_t h_i = fit((size_t)S, &st_i);
     const size_t h_p = fit((size_t)(S + 1) / 2, &st_p);
     TmaPlan p;
+    if (forced == HIST_GLOBAL) return p;
+    if (forced == HIST_AGG || forced == HIST_I32) {
+        if (st_i >= 2) {
+            p.mode = forced;
+            p.stages = st_i;
+            p.bytes = h_i + (size_t)st_i * stage;
+        }
+        return p;
+    }
+    if (forced == HIST_PACKED) {
+        if (st_p >= 2) {
+            p.mode = HIST_PACKED;
+            p.stages = st_p;
+            p.bytes = h_p + (size_t)st_p * stage;
+        }
+        return p;
+    }
     if (st_i >= 2 && st_i >= std::min(kStages, st_p)) {
         p.mode = S <= 2048 ? HIST_AGG : HIST_I32;
         p.stages = st_i;
@@ -684,14 +716,16 @@ static int launch_particles_t(blond_engine* e, const ParticleArgs& a, cudaStream
                               bool launch) {
     static bool done_agg[64] = {false}, done_plain[64] = {false};
     const int smem = engine_smem(e);
-    const bool agg = e->S <= 2048;
+    const bool agg = plain_agg(e);
     int rc;
     if (KICK) {
-        // the staged pass when asked for, and for profiles whose int
-        // histogram does not fit beside the plain pass (packed layout
-        // instead of global-memory atomics)
-        const TmaPlan p = tma_plan<PREC>(e->S);
-        if (p.stages && (e->variant == 0 || global_hist(e))) {
+        // the staged pass when asked for (variant 0 or the packed layout),
+        // and by default for profiles whose int histogram does not fit
+        // beside the plain pass (packed layout instead of global atomics)
+        const TmaPlan p = tma_plan<PREC>(e->S, e->hist_mode);
+        const bool want = e->variant == 0 || e->hist_mode == HIST_PACKED ||
+                          (e->hist_mode < 0 && global_hist(e));
+        if (p.stages && want) {
             switch (p.mode) {
                 case HIST_AGG: return launch_tma<PREC, SOLVER, LIK, HIST_AGG>(e, a, p, s, launch);
                 case HIST_I32: return launch_tma<PREC, SOLVER, LIK, HIST_I32>(e, a, p, s, launch);
@@ -765,7 +799,7 @@ static ParticleArgs particle_args(blond_engine* e) {
     a.bc0 = e->bc0;
     a.lik_inv_w = e->lik_inv_w;
     a.bw = e->bw;
-    a.global_hist = global_hist(e) ? 1 : 0;
+    a.global_hist = plain_global(e) ? 1 : 0;
     return a;
 }
 
@@ -1120,6 +1154,134 @@ int blond_engine_tune(blond_engine* e, int threads, int blocks_per_sm, int turns
     if (turns_per_graph) e->turns_per_graph = turns_per_graph;
     e->graph_dirty = true;
     return BLOND_OK;
+}
+
+int blond_engine_set_histogram(blond_engine* e, int mode) {
+    BB_CHECK_ARG(e && mode >= -1 && mode <= HIST_GLOBAL,
+                 "engine_set_histogram: mode must be -1 (automatic) .. 3");
+    e->hist_mode = mode;
+    e->graph_dirty = true;
+    return BLOND_OK;
+}
+
+// Autotuner of the particle pass.  Every feasible configuration -- plain
+// pass with 256 or 512 threads and 1, 2 or 4 blocks per SM (the
+// grid-stride loop gives each thread n / (grid x threads) particles),
+// each histogram layout that fits; staged pass with each layout that fits
+// -- is timed on the bound beam with CUDA events (one warm-up and `reps`
+// launches each) and the fastest is kept.  The coordinates and the
+// histogram are snapshotted first and restored afterwards, so tuning does
+// not change the state of the run.
+int blond_engine_autotune(blond_engine* e, int reps, void* stream, int* config,
+                          double* best_ms) {
+    BB_CHECK_ARG(e && config && best_ms && reps >= 1 && reps <= 10,
+                 "engine_autotune: bad argument (reps in 1..10)");
+    int rc = check_ready(e);
+    if (rc) return rc;
+    cudaStream_t s = as_stream(stream);
+    cudaStreamCaptureStatus cs;
+    BB_CUDA(cudaStreamIsCapturing(s, &cs));
+    BB_CHECK_ARG(cs == cudaStreamCaptureStatusNone,
+                 "engine_autotune: the stream is being captured");
+    const size_t esz = e->precision == BLOND_PREC_F64 ? sizeof(double) : sizeof(float);
+    const size_t n = (size_t)e->n;
+    void *sdt = nullptr, *sdE = nullptr, *shist = nullptr;
+    if (cudaMalloc(&sdt, 8 * n) != cudaSuccess || cudaMalloc(&sdE, esz * n) != cudaSuccess ||
+        cudaMalloc(&shist, sizeof(int) * (size_t)e->S) != cudaSuccess) {
+        free_ptr(sdt);
+        free_ptr(sdE);
+        free_ptr(shist);
+        cudaGetLastError();
+        set_error("engine_autotune: cannot allocate the snapshot (%zu bytes)",
+                  (8 + esz) * n);
+        return BLOND_ERR_CUDA;
+    }
+    BB_CUDA(cudaMemcpyAsync(sdt, e->dt, 8 * n, cudaMemcpyDeviceToDevice, s));
+    BB_CUDA(cudaMemcpyAsync(sdE, e->dE, esz * n, cudaMemcpyDeviceToDevice, s));
+    BB_CUDA(cudaMemcpyAsync(shist, e->d_hist, sizeof(int) * e->S, cudaMemcpyDeviceToDevice,
+                            s));
+    struct Cand { int variant, threads, bps, hist; };
+    std::vector<Cand> cands;
+    std::vector<int> plain_modes;
+    if (global_hist(e)) plain_modes = {HIST_GLOBAL};
+    else if (e->S <= 2048) plain_modes = {HIST_AGG, HIST_I32, HIST_GLOBAL};
+    else plain_modes = {HIST_I32, HIST_GLOBAL};
+    for (int threads : {256, 512})
+        for (int bps : {1, 2, 4})
+            for (int h : plain_modes) cands.push_back({1, threads, bps, h});
+    const bool f64 = e->precision == BLOND_PREC_F64;
+    for (int h : {HIST_AGG, HIST_I32, HIST_PACKED}) {
+        if (h == HIST_AGG && e->S > 2048) continue;
+        if (h == HIST_I32 && e->S <= 2048) continue;
+        const TmaPlan p = f64 ? tma_plan<PREC_F64>(e->S, h) : tma_plan<PREC_F32P64>(e->S, h);
+        if (p.stages) cands.push_back({0, kTmaThreads, 1, h});
+    }
+    const Cand old = {e->variant, e->threads, e->blocks_per_sm, e->hist_mode};
+    cudaEvent_t a = nullptr, b = nullptr;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    double best = 1e30;
+    Cand win = old;
+    for (const Cand& c : cands) {
+        e->variant = c.variant;
+        e->hist_mode = c.hist;
+        if (c.variant == 1) {
+            e->threads = c.threads;
+            e->blocks_per_sm = c.bps;
+        }
+        if (launch_particles(e, true, s, false)) {
+            cudaGetLastError();
+            continue;
+        }
+        cudaMemsetAsync(e->d_hist, 0, sizeof(int) * e->S, s);
+        if ((rc = launch_particles(e, true, s))) break;
+        cudaEventRecord(a, s);
+        for (int r = 0; r < reps && rc == BLOND_OK; ++r) rc = launch_particles(e, true, s);
+        cudaEventRecord(b, s);
+        if (rc) break;
+        if (cudaEventSynchronize(b) != cudaSuccess) {
+            rc = BLOND_ERR_CUDA;
+            break;
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, a, b);
+        if (ms / reps < best) {
+            best = ms / reps;
+            win = c;
+            if (c.variant == 0) {
+                win.threads = old.threads;
+                win.bps = old.bps;
+            }
+        }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    // restore the state of the run
+    cudaMemcpyAsync(e->dt, sdt, 8 * n, cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(e->dE, sdE, esz * n, cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(e->d_hist, shist, sizeof(int) * e->S, cudaMemcpyDeviceToDevice, s);
+    const cudaError_t ce = cudaStreamSynchronize(s);
+    free_ptr(sdt);
+    free_ptr(sdE);
+    free_ptr(shist);
+    if (rc == BLOND_OK && ce != cudaSuccess) {
+        set_error("engine_autotune: %s", cudaGetErrorString(ce));
+        rc = BLOND_ERR_CUDA;
+    }
+    if (rc == BLOND_OK) rc = blond_engine_check(e, stream);
+    const Cand& use = rc == BLOND_OK && best < 1e30 ? win : old;
+    e->variant = use.variant;
+    e->threads = use.threads;
+    e->blocks_per_sm = use.bps;
+    e->hist_mode = use.hist;
+    e->graph_dirty = true;
+    config[0] = use.variant;
+    config[1] = use.variant == 0 ? kTmaThreads : use.threads;
+    config[2] = use.variant == 0 ? 1 : use.bps;
+    config[3] = use.hist;
+    config[4] = (int)cands.size();
+    *best_ms = best < 1e30 ? best : 0.0;
+    return rc;
 }
 
 // Capture (once per configuration) the graph of turns_per_graph turns and

@@ -103,7 +103,7 @@ class FusedTracker:
     def __init__(self, tracker, profile, total_induced_voltage=None,
                  precision: str = "f64", turns_per_graph: int = 50,
                  threads: int = 0, blocks_per_sm: int = 0, kernel: str = "auto",
-                 process_group=None):
+                 process_group=None, tune: str | None = None):
         if precision not in PREC:
             raise ValueError(f"precision must be one of {list(PREC)}")
         if tracker.interpolation:
@@ -151,12 +151,23 @@ class FusedTracker:
         self.eng.call("tune", int(threads), int(blocks_per_sm), int(turns_per_graph))
         if kernel not in ("auto", "tma", "plain"):
             raise ValueError("kernel must be 'auto', 'tma' or 'plain'")
+        self.kernel_requested = kernel
         if kernel == "auto":
             # measured on the B200 (C2 workload): plain loads win for FP64
             # (87 vs 107 us), the bulk-copy pipeline ties or wins for F32P64
             kernel = "plain" if precision == "f64" else "tma"
         self.kernel = kernel
         self.eng.call("set_kernel", 0 if kernel == "tma" else 1)
+        # the autotuner picks block size, grid (particles per thread),
+        # histogram layout and staged vs plain pass on the first track() or
+        # prepare(), unless the caller fixed any of them
+        if tune is None:
+            tune = "auto" if (self.kernel_requested == "auto" and not threads
+                              and not blocks_per_sm) else "fixed"
+        if tune not in ("auto", "fixed"):
+            raise ValueError("tune must be 'auto' or 'fixed'")
+        self.tune_mode = tune
+        self.tuned = None
         self.eng.call("set_turn", int(rf.counter[0]), _stream())
         # sharded: this rank holds a part of the beam; the int32 histogram is
         # summed over `process_group` after every particle pass.  The beam's
@@ -202,8 +213,28 @@ class FusedTracker:
         if hasattr(self, "_zn"):
             self.eng.call("set_inductive", _p(self._zn), float(self._ind_scale))
 
+    def autotune(self, reps: int = 3) -> dict:
+        """Run the engine's autotuner now (blond_engine_autotune): times
+        every feasible particle-pass configuration on this beam, keeps the
+        fastest and leaves the beam untouched.  Returns the choice."""
+        cfg = (ct.c_int * 5)()
+        ms = ct.c_double()
+        self.eng.call("autotune", int(reps), _stream(), cfg, ct.byref(ms))
+        names = {-1: "auto", 0: "smem-warp-aggregated", 1: "smem-int", 2: "smem-packed16",
+                 3: "global"}
+        self.tuned = {"kernel": "tma" if cfg[0] == 0 else "plain", "threads": cfg[1],
+                      "blocks_per_sm": cfg[2], "histogram": names.get(cfg[3], cfg[3]),
+                      "candidates": cfg[4], "particle_pass_ms": ms.value}
+        self.kernel = self.tuned["kernel"]
+        return self.tuned
+
+    def _maybe_tune(self):
+        if self.tune_mode == "auto" and self.tuned is None:
+            self.autotune()
+
     def track(self, n_turns: int = 1):
         """Advance n_turns; updates the RF counter and beam energy fields."""
+        self._maybe_tune()
         if self.group is None:
             self.eng.call("run", int(n_turns), _stream())
         else:
@@ -221,6 +252,7 @@ class FusedTracker:
     def prepare(self):
         """Build and upload the CUDA graph now (otherwise the first track()
         of at least turns_per_graph turns builds it)."""
+        self._maybe_tune()
         self.eng.call("prepare", _stream())
 
     def check(self):
@@ -230,6 +262,7 @@ class FusedTracker:
     def time_kernels(self, n_turns: int):
         """Track n_turns with CUDA events around each launch; returns the
         summed (head_ms, particles_ms).  Synchronises the current stream."""
+        self._maybe_tune()
         h, p = ct.c_double(), ct.c_double()
         self.eng.call("time_kernels", int(n_turns), ct.byref(h), ct.byref(p), _stream())
         self.rf.counter[0] += int(n_turns)

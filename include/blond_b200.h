@@ -237,6 +237,21 @@ int blond_engine_step(blond_engine* engine, int part, void* stream);
 /* Grid size and block size of the particle kernel (0 = automatic). */
 int blond_engine_tune(blond_engine* engine, int threads, int blocks_per_sm,
                       int turns_per_graph);
+/* Histogram layout of the particle pass: -1 automatic, 0 block-private
+ * ints with warp-aggregated deposits, 1 block-private ints, 2 block-private
+ * packed 16-bit counters (staged pass), 3 global-memory atomics (plain
+ * pass).  A layout that does not fit falls back to the automatic one. */
+int blond_engine_set_histogram(blond_engine* engine, int mode);
+/* Autotuner: times every feasible particle-pass configuration (plain pass:
+ * 256/512 threads x 1/2/4 blocks per SM x histogram layouts; staged pass:
+ * histogram layouts) on the bound beam, `reps` (1..10) launches each after
+ * one warm-up, keeps the fastest and restores the coordinates and the
+ * histogram.  config[5] receives {variant (0 staged, 1 plain), threads,
+ * blocks per SM, histogram layout, candidates timed}; best_ms the
+ * particle-pass time of the winner.  Not inside stream capture; allocates
+ * a snapshot of the coordinates for the duration of the call. */
+int blond_engine_autotune(blond_engine* engine, int reps, void* stream, int* config,
+                          double* best_ms);
 
 /* ------------------------------------------------------------ batched beams
  * Many independent beams (one RingAndRFTracker + Profile +

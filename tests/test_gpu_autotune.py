@@ -1,0 +1,69 @@
+"""The particle-pass autotuner and the histogram layouts it chooses from.
+
+Every configuration must give the reference's result bit for bit (the
+layouts only change where the counts are accumulated), and tuning must not
+move the beam: tracking after autotune() equals tracking without it.
+"""
+import numpy as np
+import pytest
+import torch
+
+from conftest import golden, normwise
+from test_gpu_tracking import build, impedance_objects, make_profile
+from blond_b200.engine import FusedTracker
+from blond_b200.impedances.impedance import TotalInducedVoltage
+from blond_b200.trackers.tracker import RingAndRFTracker
+
+pytestmark = pytest.mark.gpu
+
+
+def fused_for(name, **kw):
+    g = golden(name)
+    ring, rf, beam = build(g)
+    prof = make_profile(g, beam)
+    ivs = impedance_objects(name, beam, prof, rf)
+    tiv = TotalInducedVoltage(beam, prof, ivs) if ivs else None
+    return g, beam, FusedTracker(RingAndRFTracker(rf, beam), prof, tiv, **kw)
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32p64"])
+def test_autotune_leaves_the_beam_untouched(cuda, precision):
+    g, beam, fx = fused_for("track_full.npz", precision=precision, tune="fixed")
+    nt = int(g["n_turns"][0])
+    fx.track(nt)
+    ref = (fx.dt.cpu().numpy().copy(), fx.dE.cpu().numpy().copy(),
+           fx.profile_tensor().cpu().numpy())
+    g, beam, fa = fused_for("track_full.npz", precision=precision)
+    assert fa.tune_mode == "auto"
+    dt0 = fa.dt.cpu().numpy().copy()
+    cfg = fa.autotune(reps=2)
+    assert cfg["candidates"] > 0 and cfg["particle_pass_ms"] > 0
+    assert cfg["kernel"] in ("tma", "plain")
+    np.testing.assert_array_equal(fa.dt.cpu().numpy(), dt0)
+    fa.track(nt)
+    np.testing.assert_array_equal(fa.dt.cpu().numpy(), ref[0])
+    np.testing.assert_array_equal(fa.dE.cpu().numpy(), ref[1])
+    np.testing.assert_array_equal(fa.profile_tensor().cpu().numpy(), ref[2])
+    if precision == "f64":
+        assert normwise(beam.dt.cpu().numpy(), g["dt"]) < 1e-11
+
+
+@pytest.mark.parametrize("kernel", ["tma", "plain"])
+@pytest.mark.parametrize("hist", [-1, 0, 1, 2, 3])
+def test_every_histogram_layout_matches_reference(cuda, kernel, hist):
+    g, beam, f = fused_for("track_full.npz", precision="f64", kernel=kernel)
+    f.eng.call("set_histogram", hist)
+    nt = int(g["n_turns"][0])
+    f.track(nt)
+    assert normwise(beam.dt.cpu().numpy(), g["dt"]) < 1e-11
+    assert normwise(beam.dE.cpu().numpy(), g["dE"]) < 1e-11
+    np.testing.assert_array_equal(f.profile_tensor().cpu().numpy(), g["profiles"][-1])
+
+
+def test_autotuned_tracker_is_the_default(cuda):
+    g, beam, f = fused_for("track_rf.npz")
+    assert f.tuned is None
+    f.track(int(g["n_turns"][0]))
+    assert f.tuned is not None
+    assert normwise(beam.dt.cpu().numpy(), g["dt"]) < 1e-11
+    np.testing.assert_array_equal(f.profile_tensor().cpu().numpy(), g["profiles"][-1])
