@@ -20,6 +20,8 @@
 #include <algorithm>
 #include <cstddef>
 #include <mutex>
+#include <set>
+#include <utility>
 #include <vector>
 
 namespace bb {
@@ -273,20 +275,47 @@ __device__ __forceinline__ void cluster_flush(int* sh, int* hist, int S) {
     cl.sync();  // remote reads done before any CTA's shared memory goes away
 }
 
-constexpr int kEngineThreads = 512;
-// CTAs whose histograms are merged on chip before the global flush.  1: on
-// the C2 workload (64 KB histograms, 2 blocks/SM) clusters of 8 cost more
-// in lost co-scheduling than they save in atomics (142 vs 87 us measured).
-constexpr int kEngineCluster = 1;
+// Largest block of the plain pass; its launch bound (1024 threads, one
+// block per SM) caps registers at 64 per thread, the same as two blocks of
+// 512, so 256-, 512- and 1024-thread launches all use the same code.
+constexpr int kEngineThreads = 1024;
+
+// Per-thread asynchronous copies into shared memory (cp.async, 16 or 8
+// bytes): the prefetch ring of the plain pass.
+__device__ __forceinline__ void ring_copy16(void* smem, const void* gmem) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                     (uint32_t)__cvta_generic_to_shared(smem)), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void ring_copy8(void* smem, const void* gmem) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(
+                     (uint32_t)__cvta_generic_to_shared(smem)), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void ring_commit() {
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void ring_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Bytes of the plain pass's prefetch ring per thread and stage.
+template <int PREC>
+constexpr int ring_bytes() {
+    return 16 + (PREC == PREC_F64 ? 16 : 8);
+}
 
 // Pairs of particles per thread and iteration; pairs are read with one
-// 16-byte (dt) and one 16- or 8-byte (dE) load.
-template <int PREC, int SOLVER, bool LIK, bool KICK, bool WARP_AGG>
-__global__ void __launch_bounds__(kEngineThreads, 2)
+// 16-byte (dt) and one 16- or 8-byte (dE) load.  With NST > 0 the loads go
+// through a per-thread ring of NST shared-memory slots filled NST - 1
+// iterations ahead with cp.async: each thread then has NST - 1 pairs in
+// flight while it computes one, without extra registers and without any
+// block-wide barrier (a thread reads only the slots it filled itself).
+template <int PREC, int SOLVER, bool LIK, bool KICK, bool WARP_AGG, int NST>
+__global__ void __launch_bounds__(kEngineThreads, 1)
 particle_kernel(const ParticleArgs a) {
     using E = typename Coord<PREC>::E;
     using E2 = typename Vec2<E>::type;
-    extern __shared__ int sh[];
+    extern __shared__ __align__(16) int sh[];
     __shared__ TurnConsts c;
     long long t_idx = a.turn ? (*a.turn - 1) : 0;
     if (t_idx < 0) t_idx = 0;
@@ -317,23 +346,64 @@ particle_kernel(const ParticleArgs a) {
     const int order = a.order;
     // whole warps iterate together (needed by __match_any_sync)
     const int lane = threadIdx.x & 31;
-    for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31);
-         base < npairs; base += stride) {
-        const int64_t p = base + lane;
-        int b0 = -1, b1 = -1;
-        if (p < npairs) {
-            double2 tt = reinterpret_cast<const double2*>(dt)[p];
-            E2 ee = reinterpret_cast<const E2*>(dE)[p];
-            if (KICK) track_pair<PREC, SOLVER, LIK>(tt.x, tt.y, ee.x, ee.y, c, a, order);
-            if (KICK) {
+    int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31);
+    if (NST == 0) {
+        for (; base < npairs; base += stride) {
+            const int64_t p = base + lane;
+            int b0 = -1, b1 = -1;
+            if (p < npairs) {
+                double2 tt = reinterpret_cast<const double2*>(dt)[p];
+                E2 ee = reinterpret_cast<const E2*>(dE)[p];
+                if (KICK) track_pair<PREC, SOLVER, LIK>(tt.x, tt.y, ee.x, ee.y, c, a, order);
+                if (KICK) {
+                    reinterpret_cast<double2*>(dt)[p] = tt;
+                    reinterpret_cast<E2*>(dE)[p] = ee;
+                }
+                b0 = engine_bin(tt.x, a.cut_left, a.inv_w, a.S);
+                b1 = engine_bin(tt.y, a.cut_left, a.inv_w, a.S);
+            }
+            deposit(hd, b0, WARP_AGG, 0xffffffffu);
+            deposit(hd, b1, WARP_AGG, 0xffffffffu);
+        }
+    } else {
+        // the ring sits after the (16-byte aligned) histogram
+        const size_t hbytes = a.global_hist ? 0 : (((size_t)a.S * sizeof(int) + 15) & ~(size_t)15);
+        double2* rdt = reinterpret_cast<double2*>(reinterpret_cast<char*>(sh) + hbytes);
+        E2* rdE = reinterpret_cast<E2*>(rdt + (size_t)NST * blockDim.x);
+        const double2* gdt = reinterpret_cast<const double2*>(dt);
+        const E2* gdE = reinterpret_cast<const E2*>(dE);
+        auto fill = [&](int slot, int64_t p) {
+            if (p < npairs) {
+                ring_copy16(&rdt[slot * blockDim.x + threadIdx.x], &gdt[p]);
+                if (sizeof(E2) == 16) ring_copy16(&rdE[slot * blockDim.x + threadIdx.x], &gdE[p]);
+                else ring_copy8(&rdE[slot * blockDim.x + threadIdx.x], &gdE[p]);
+            }
+            ring_commit();  // one group per stage, empty past the end
+        };
+#pragma unroll
+        for (int s = 0; s < NST - 1; ++s) fill(s, base + s * stride + lane);
+        int slot = 0;
+        for (; base < npairs; base += stride) {
+            // stage it + NST - 1 goes into the slot this thread emptied in
+            // the previous iteration
+            fill(slot == 0 ? NST - 1 : slot - 1, base + (NST - 1) * stride + lane);
+            ring_wait<NST - 1>();  // groups complete in order: this stage landed
+            const int64_t p = base + lane;
+            int b0 = -1, b1 = -1;
+            if (p < npairs) {
+                double2 tt = rdt[slot * blockDim.x + threadIdx.x];
+                E2 ee = rdE[slot * blockDim.x + threadIdx.x];
+                track_pair<PREC, SOLVER, LIK>(tt.x, tt.y, ee.x, ee.y, c, a, order);
                 reinterpret_cast<double2*>(dt)[p] = tt;
                 reinterpret_cast<E2*>(dE)[p] = ee;
+                b0 = engine_bin(tt.x, a.cut_left, a.inv_w, a.S);
+                b1 = engine_bin(tt.y, a.cut_left, a.inv_w, a.S);
             }
-            b0 = engine_bin(tt.x, a.cut_left, a.inv_w, a.S);
-            b1 = engine_bin(tt.y, a.cut_left, a.inv_w, a.S);
+            deposit(hd, b0, WARP_AGG, 0xffffffffu);
+            deposit(hd, b1, WARP_AGG, 0xffffffffu);
+            slot = slot + 1 == NST ? 0 : slot + 1;
         }
-        deposit(hd, b0, WARP_AGG, 0xffffffffu);
-        deposit(hd, b1, WARP_AGG, 0xffffffffu);
+        ring_wait<0>();  // nothing may land in shared memory after the flush
     }
     // odd tail particle
     if ((a.n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
@@ -579,11 +649,13 @@ struct blond_engine {
     void* dE = nullptr;
     int64_t n = 0;
     // tuning
-    int threads = kEngineThreads;
+    int threads = 512;
     int blocks_per_sm = 2;
     int turns_per_graph = 50;
     int variant = 0;  // 0: TMA-pipelined particle pass, 1: plain loads
     int hist_mode = -1;  // -1 automatic, else HIST_AGG/I32/PACKED/GLOBAL
+    int ring = 0;        // plain pass: prefetch ring stages (0 = direct loads)
+    int cluster = 1;     // plain pass: blocks whose histograms merge on chip
     // graph cache
     cudaStream_t cap_stream = nullptr;
     cudaGraphExec_t graph = nullptr;
@@ -711,6 +783,50 @@ static int launch_tma(blond_engine* e, ParticleArgs a, const TmaPlan& p, cudaStr
     return BLOND_OK;
 }
 
+// Raise a kernel's dynamic shared memory limit to the opt-in maximum once
+// per (kernel, device).
+template <typename K>
+static int allow_smem_once(K kernel) {
+    static std::mutex mu;
+    static std::set<std::pair<const void*, int>> done;
+    const DeviceInfo& d = device_info();
+    const std::pair<const void*, int> key(reinterpret_cast<const void*>(kernel), d.device);
+    std::lock_guard<std::mutex> lock(mu);
+    if (done.count(key)) return BLOND_OK;
+    cudaFuncAttributes fa;
+    BB_CUDA(cudaFuncGetAttributes(&fa, kernel));
+    BB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 d.max_smem_optin - (int)fa.sharedSizeBytes));
+    done.insert(key);
+    return BLOND_OK;
+}
+
+// The plain pass for a histogram mode and prefetch ring depth (0, 2, 4).
+template <int PREC, int SOLVER, bool LIK, bool KICK>
+static auto plain_kernel(bool agg, int ring)
+    -> decltype(&particle_kernel<PREC, SOLVER, LIK, KICK, true, 0>) {
+    if constexpr (KICK) {
+        if (ring == 2)
+            return agg ? particle_kernel<PREC, SOLVER, LIK, KICK, true, 2>
+                       : particle_kernel<PREC, SOLVER, LIK, KICK, false, 2>;
+        if (ring == 4)
+            return agg ? particle_kernel<PREC, SOLVER, LIK, KICK, true, 4>
+                       : particle_kernel<PREC, SOLVER, LIK, KICK, false, 4>;
+    }
+    return agg ? particle_kernel<PREC, SOLVER, LIK, KICK, true, 0>
+               : particle_kernel<PREC, SOLVER, LIK, KICK, false, 0>;
+}
+
+// Dynamic shared memory of the plain pass: the histogram (16-byte aligned)
+// and the prefetch ring; -1 if that exceeds the opt-in limit.
+template <int PREC>
+static int plain_ring_smem(const blond_engine* e, int ring) {
+    const int h = engine_smem(e);
+    const int bytes = ring ? ((h + 15) & ~15) + ring * e->threads * ring_bytes<PREC>() : h;
+    const int limit = device_info().max_smem_optin - (int)sizeof(TurnConsts) - 1024;
+    return bytes <= limit ? bytes : -1;
+}
+
 template <int PREC, int SOLVER, bool LIK, bool KICK>
 static int launch_particles_t(blond_engine* e, const ParticleArgs& a, cudaStream_t s,
                               bool launch) {
@@ -735,23 +851,31 @@ static int launch_particles_t(blond_engine* e, const ParticleArgs& a, cudaStream
         // profile too long for the staged copy: plain loads below
     }
     int grid = particle_grid(e->n / 2 + 1, e->threads, e->blocks_per_sm);
-    grid = (grid + kEngineCluster - 1) / kEngineCluster * kEngineCluster;
-    auto k = agg ? particle_kernel<PREC, SOLVER, LIK, KICK, true>
-                 : particle_kernel<PREC, SOLVER, LIK, KICK, false>;
-    if ((rc = allow_max_smem(k, agg ? done_agg : done_plain))) return rc;
+    const int cl = plain_global(e) ? 1 : e->cluster;  // merging needs shared histograms
+    grid = (grid + cl - 1) / cl * cl;
+    const int ring = KICK ? e->ring : 0;
+    auto k = plain_kernel<PREC, SOLVER, LIK, KICK>(agg, ring);
+    (void)done_agg;
+    (void)done_plain;
+    if ((rc = allow_smem_once(k))) return rc;
+    const int smem_ring = plain_ring_smem<PREC>(e, ring);
+    if (smem_ring < 0) {
+        set_error("engine: prefetch ring of %d stages does not fit beside the histogram", ring);
+        return BLOND_ERR_SIZE;
+    }
     if (launch) {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(grid, 1, 1);
         cfg.blockDim = dim3(e->threads, 1, 1);
-        cfg.dynamicSmemBytes = smem;
+        cfg.dynamicSmemBytes = smem_ring;
         cfg.stream = s;
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeClusterDimension;
-        attr[0].val.clusterDim.x = kEngineCluster;
+        attr[0].val.clusterDim.x = cl;
         attr[0].val.clusterDim.y = 1;
         attr[0].val.clusterDim.z = 1;
         cfg.attrs = attr;
-        cfg.numAttrs = kEngineCluster > 1 ? 1 : 0;
+        cfg.numAttrs = cl > 1 ? 1 : 0;
         BB_CUDA(cudaLaunchKernelEx(&cfg, k, a));
     }
     BB_LAUNCH_CHECK();
@@ -1156,6 +1280,22 @@ int blond_engine_tune(blond_engine* e, int threads, int blocks_per_sm, int turns
     return BLOND_OK;
 }
 
+int blond_engine_set_cluster(blond_engine* e, int blocks) {
+    BB_CHECK_ARG(e && (blocks == 1 || blocks == 2 || blocks == 4 || blocks == 8),
+                 "engine_set_cluster: 1, 2, 4 or 8 blocks");
+    e->cluster = blocks;
+    e->graph_dirty = true;
+    return BLOND_OK;
+}
+
+int blond_engine_set_prefetch(blond_engine* e, int stages) {
+    BB_CHECK_ARG(e && (stages == 0 || stages == 2 || stages == 4),
+                 "engine_set_prefetch: stages must be 0, 2 or 4");
+    e->ring = stages;
+    e->graph_dirty = true;
+    return BLOND_OK;
+}
+
 int blond_engine_set_histogram(blond_engine* e, int mode) {
     BB_CHECK_ARG(e && mode >= -1 && mode <= HIST_GLOBAL,
                  "engine_set_histogram: mode must be -1 (automatic) .. 3");
@@ -1167,7 +1307,10 @@ int blond_engine_set_histogram(blond_engine* e, int mode) {
 // Autotuner of the particle pass.  Every feasible configuration -- plain
 // pass with 256 or 512 threads and 1, 2 or 4 blocks per SM (the
 // grid-stride loop gives each thread n / (grid x threads) particles),
-// each histogram layout that fits; staged pass with each layout that fits
+// each histogram layout and prefetch ring depth (0, 2, 4) that fits, and
+// block-private histograms merged in pairs through distributed shared
+// memory before the global flush (thread-block clusters of 2);
+// staged pass with each layout that fits
 // -- is timed on the bound beam with CUDA events (one warm-up and `reps`
 // launches each) and the fastest is kept.  The coordinates and the
 // histogram are snapshotted first and restored afterwards, so tuning does
@@ -1200,23 +1343,38 @@ int blond_engine_autotune(blond_engine* e, int reps, void* stream, int* config,
     BB_CUDA(cudaMemcpyAsync(sdE, e->dE, esz * n, cudaMemcpyDeviceToDevice, s));
     BB_CUDA(cudaMemcpyAsync(shist, e->d_hist, sizeof(int) * e->S, cudaMemcpyDeviceToDevice,
                             s));
-    struct Cand { int variant, threads, bps, hist; };
+    struct Cand { int variant, threads, bps, hist, ring, cluster; };
     std::vector<Cand> cands;
     std::vector<int> plain_modes;
     if (global_hist(e)) plain_modes = {HIST_GLOBAL};
     else if (e->S <= 2048) plain_modes = {HIST_AGG, HIST_I32, HIST_GLOBAL};
     else plain_modes = {HIST_I32, HIST_GLOBAL};
-    for (int threads : {256, 512})
-        for (int bps : {1, 2, 4})
-            for (int h : plain_modes) cands.push_back({1, threads, bps, h});
     const bool f64 = e->precision == BLOND_PREC_F64;
+    const int keep_threads = e->threads, keep_hist = e->hist_mode;
+    for (int threads : {256, 512, 1024})
+        for (int bps : {1, 2, 4})
+            // 64 registers a thread: at most 1024 threads resident per SM
+            if (threads * bps <= 1024)
+            for (int h : plain_modes)
+                for (int ring : {0, 2, 4})
+                    for (int cl : {1, 2}) {
+                        if (cl > 1 && (h == HIST_GLOBAL || ring == 4)) continue;
+                        e->threads = threads;
+                        e->hist_mode = h;
+                        const int sm = f64 ? plain_ring_smem<PREC_F64>(e, ring)
+                                           : plain_ring_smem<PREC_F32P64>(e, ring);
+                        if (sm >= 0) cands.push_back({1, threads, bps, h, ring, cl});
+                    }
+    e->threads = keep_threads;
+    e->hist_mode = keep_hist;
     for (int h : {HIST_AGG, HIST_I32, HIST_PACKED}) {
         if (h == HIST_AGG && e->S > 2048) continue;
         if (h == HIST_I32 && e->S <= 2048) continue;
         const TmaPlan p = f64 ? tma_plan<PREC_F64>(e->S, h) : tma_plan<PREC_F32P64>(e->S, h);
-        if (p.stages) cands.push_back({0, kTmaThreads, 1, h});
+        if (p.stages) cands.push_back({0, kTmaThreads, 1, h, 0, 1});
     }
-    const Cand old = {e->variant, e->threads, e->blocks_per_sm, e->hist_mode};
+    const Cand old = {e->variant, e->threads, e->blocks_per_sm, e->hist_mode, e->ring,
+                      e->cluster};
     cudaEvent_t a = nullptr, b = nullptr;
     cudaEventCreate(&a);
     cudaEventCreate(&b);
@@ -1225,6 +1383,8 @@ int blond_engine_autotune(blond_engine* e, int reps, void* stream, int* config,
     for (const Cand& c : cands) {
         e->variant = c.variant;
         e->hist_mode = c.hist;
+        e->ring = c.ring;
+        e->cluster = c.cluster;
         if (c.variant == 1) {
             e->threads = c.threads;
             e->blocks_per_sm = c.bps;
@@ -1274,12 +1434,16 @@ int blond_engine_autotune(blond_engine* e, int reps, void* stream, int* config,
     e->threads = use.threads;
     e->blocks_per_sm = use.bps;
     e->hist_mode = use.hist;
+    e->ring = use.ring;
+    e->cluster = use.cluster;
     e->graph_dirty = true;
     config[0] = use.variant;
     config[1] = use.variant == 0 ? kTmaThreads : use.threads;
     config[2] = use.variant == 0 ? 1 : use.bps;
     config[3] = use.hist;
-    config[4] = (int)cands.size();
+    config[4] = use.ring;
+    config[5] = use.cluster;
+    config[6] = (int)cands.size();
     *best_ms = best < 1e30 ? best : 0.0;
     return rc;
 }

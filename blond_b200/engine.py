@@ -217,14 +217,15 @@ class FusedTracker:
         """Run the engine's autotuner now (blond_engine_autotune): times
         every feasible particle-pass configuration on this beam, keeps the
         fastest and leaves the beam untouched.  Returns the choice."""
-        cfg = (ct.c_int * 5)()
+        cfg = (ct.c_int * 7)()
         ms = ct.c_double()
         self.eng.call("autotune", int(reps), _stream(), cfg, ct.byref(ms))
         names = {-1: "auto", 0: "smem-warp-aggregated", 1: "smem-int", 2: "smem-packed16",
                  3: "global"}
         self.tuned = {"kernel": "tma" if cfg[0] == 0 else "plain", "threads": cfg[1],
                       "blocks_per_sm": cfg[2], "histogram": names.get(cfg[3], cfg[3]),
-                      "candidates": cfg[4], "particle_pass_ms": ms.value}
+                      "prefetch_stages": cfg[4], "cluster": cfg[5], "candidates": cfg[6],
+                      "particle_pass_ms": ms.value}
         self.kernel = self.tuned["kernel"]
         return self.tuned
 

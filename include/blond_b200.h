@@ -242,12 +242,20 @@ int blond_engine_tune(blond_engine* engine, int threads, int blocks_per_sm,
  * packed 16-bit counters (staged pass), 3 global-memory atomics (plain
  * pass).  A layout that does not fit falls back to the automatic one. */
 int blond_engine_set_histogram(blond_engine* engine, int mode);
+/* Plain pass: depth of the per-thread cp.async prefetch ring (0 = direct
+ * loads, 2 or 4 stages). */
+int blond_engine_set_prefetch(blond_engine* engine, int stages);
+/* Plain pass: blocks (1, 2, 4, 8) of a thread-block cluster whose shared
+ * histograms are summed through distributed shared memory before one
+ * global flush per cluster. */
+int blond_engine_set_cluster(blond_engine* engine, int blocks);
 /* Autotuner: times every feasible particle-pass configuration (plain pass:
- * 256/512 threads x 1/2/4 blocks per SM x histogram layouts; staged pass:
- * histogram layouts) on the bound beam, `reps` (1..10) launches each after
- * one warm-up, keeps the fastest and restores the coordinates and the
- * histogram.  config[5] receives {variant (0 staged, 1 plain), threads,
- * blocks per SM, histogram layout, candidates timed}; best_ms the
+ * 256/512 threads x 1/2/4 blocks per SM x histogram layouts x prefetch
+ * ring 0/2/4 x clusters of 1/2; staged pass: histogram layouts) on the
+ * bound beam, `reps` (1..10) launches each after one warm-up, keeps the
+ * fastest and restores the coordinates and the histogram.  config[7]
+ * receives {variant (0 staged, 1 plain), threads, blocks per SM, histogram
+ * layout, ring stages, cluster blocks, candidates timed}; best_ms the
  * particle-pass time of the winner.  Not inside stream capture; allocates
  * a snapshot of the coordinates for the duration of the call. */
 int blond_engine_autotune(blond_engine* engine, int reps, void* stream, int* config,

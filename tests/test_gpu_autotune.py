@@ -67,3 +67,38 @@ def test_autotuned_tracker_is_the_default(cuda):
     assert f.tuned is not None
     assert normwise(beam.dt.cpu().numpy(), g["dt"]) < 1e-11
     np.testing.assert_array_equal(f.profile_tensor().cpu().numpy(), g["profiles"][-1])
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32p64"])
+@pytest.mark.parametrize("stages", [2, 4])
+@pytest.mark.parametrize("hist", [0, 1, 3])
+def test_prefetch_ring_matches_direct_loads(cuda, precision, stages, hist):
+    g, beam, fx = fused_for("track_full.npz", precision=precision, kernel="plain")
+    nt = int(g["n_turns"][0])
+    fx.track(nt)
+    ref = (fx.dt.cpu().numpy().copy(), fx.dE.cpu().numpy().copy(),
+           fx.profile_tensor().cpu().numpy())
+    g, beam, f = fused_for("track_full.npz", precision=precision, kernel="plain")
+    f.eng.call("set_prefetch", stages)
+    f.eng.call("set_histogram", hist)
+    f.track(nt)
+    np.testing.assert_array_equal(f.dt.cpu().numpy(), ref[0])
+    np.testing.assert_array_equal(f.dE.cpu().numpy(), ref[1])
+    np.testing.assert_array_equal(f.profile_tensor().cpu().numpy(), ref[2])
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32p64"])
+@pytest.mark.parametrize("cluster", [2, 4])
+@pytest.mark.parametrize("hist", [0, 1])
+def test_cluster_merged_histograms_match(cuda, precision, cluster, hist):
+    g, beam, fx = fused_for("track_full.npz", precision=precision, kernel="plain")
+    nt = int(g["n_turns"][0])
+    fx.track(nt)
+    ref = (fx.dt.cpu().numpy().copy(), fx.profile_tensor().cpu().numpy())
+    g, beam, f = fused_for("track_full.npz", precision=precision, kernel="plain")
+    f.eng.call("set_cluster", cluster)
+    f.eng.call("set_histogram", hist)
+    f.eng.call("set_prefetch", 2)
+    f.track(nt)
+    np.testing.assert_array_equal(f.dt.cpu().numpy(), ref[0])
+    np.testing.assert_array_equal(f.profile_tensor().cpu().numpy(), ref[1])
