@@ -656,6 +656,10 @@ struct blond_engine {
     int hist_mode = -1;  // -1 automatic, else HIST_AGG/I32/PACKED/GLOBAL
     int ring = 0;        // plain pass: prefetch ring stages (0 = direct loads)
     int cluster = 1;     // plain pass: blocks whose histograms merge on chip
+    // host-buffer pipeline (blond_engine_track_host): copy streams and one
+    // (in, done, out) event triple per chunk
+    cudaStream_t io_in = nullptr, io_out = nullptr;
+    std::vector<cudaEvent_t> io_ev;
     // graph cache
     cudaStream_t cap_stream = nullptr;
     cudaGraphExec_t graph = nullptr;
@@ -775,7 +779,7 @@ static int launch_tma(blond_engine* e, ParticleArgs a, const TmaPlan& p, cudaStr
     int rc;
     if ((rc = allow_max_smem(k, done))) return rc;
     a.tma_stages = p.stages;
-    const long long nchunks = e->n / kTile;
+    const long long nchunks = a.n / kTile;
     const int grid = (int)std::max<long long>(
         1, std::min<long long>(nchunks, device_info().sm_count));
     if (launch) k<<<grid, kTmaThreads, p.bytes, s>>>(a, e->d_err);
@@ -850,7 +854,7 @@ static int launch_particles_t(blond_engine* e, const ParticleArgs& a, cudaStream
         }
         // profile too long for the staged copy: plain loads below
     }
-    int grid = particle_grid(e->n / 2 + 1, e->threads, e->blocks_per_sm);
+    int grid = particle_grid(a.n / 2 + 1, e->threads, e->blocks_per_sm);
     const int cl = plain_global(e) ? 1 : e->cluster;  // merging needs shared histograms
     grid = (grid + cl - 1) / cl * cl;
     const int ring = KICK ? e->ring : 0;
@@ -933,6 +937,20 @@ static int launch_particles(blond_engine* e, bool kick, cudaStream_t s,
     if (e->precision == BLOND_PREC_F64)
         return launch_particles_p<PREC_F64>(e, a, kick, s, launch);
     return launch_particles_p<PREC_F32P64>(e, a, kick, s, launch);
+}
+
+// The particle pass over particles [off, off + cnt) of the bound beam (off
+// even, so pairs stay 16-byte aligned); deposits into the same histogram.
+static int launch_particles_range(blond_engine* e, int64_t off, int64_t cnt,
+                                  cudaStream_t s) {
+    ParticleArgs a = particle_args(e);
+    const size_t esz = e->precision == BLOND_PREC_F64 ? sizeof(double) : sizeof(float);
+    a.dt = static_cast<double*>(e->dt) + off;
+    a.dE = static_cast<char*>(e->dE) + esz * (size_t)off;
+    a.n = cnt;
+    if (e->precision == BLOND_PREC_F64)
+        return launch_particles_p<PREC_F64>(e, a, true, s, true);
+    return launch_particles_p<PREC_F32P64>(e, a, true, s, true);
 }
 
 static int launch_profile(blond_engine* e, bool clear, cudaStream_t s) {
@@ -1059,6 +1077,9 @@ int blond_engine_destroy(blond_engine* e) {
     if (!e) return BLOND_OK;
     if (e->graph) cudaGraphExecDestroy(e->graph);
     if (e->cap_stream) cudaStreamDestroy(e->cap_stream);
+    for (cudaEvent_t ev : e->io_ev) cudaEventDestroy(ev);
+    if (e->io_in) cudaStreamDestroy(e->io_in);
+    if (e->io_out) cudaStreamDestroy(e->io_out);
     for (void* p : {(void*)e->d_V, (void*)e->d_om, (void*)e->d_ph, (void*)e->d_acc,
                     (void*)e->d_drift, (void*)e->d_bc, (void*)e->d_H, (void*)e->d_tw,
                     (void*)e->d_ind,
@@ -1513,6 +1534,77 @@ int blond_engine_run(blond_engine* e, int64_t n_turns, void* stream) {
     // the profile of the final coordinates (the histogram stays for the
     // next turn's head)
     return launch_profile(e, false, s);
+}
+
+// Turns on coordinates that live in host memory.  Every turn copies the
+// beam in, runs the turn and copies it back, as a drop-in caller that keeps
+// its arrays on the host sees it; the copies are pipelined in chunks over
+// two copy streams (in and out directions concurrently) against the
+// particle pass: chunk c is computed while c + 1 arrives and c - 1 leaves.
+int blond_engine_track_host(blond_engine* e, double* host_dt, void* host_dE,
+                            int64_t n_turns, int chunks, void* stream) {
+    BB_CHECK_ARG(e && host_dt && host_dE && n_turns >= 0 && chunks >= 1 && chunks <= 256,
+                 "engine_track_host: bad argument (chunks in 1..256)");
+    int rc = check_ready(e);
+    if (rc) return rc;
+    BB_CHECK_SIZE(e->host_turn + n_turns <= e->n_turns,
+                  "engine_track_host: turns exceed the programme");
+    if (n_turns == 0) return BLOND_OK;
+    cudaStream_t s = as_stream(stream);
+    if (!e->io_in) {
+        BB_CUDA(cudaStreamCreateWithFlags(&e->io_in, cudaStreamNonBlocking));
+        BB_CUDA(cudaStreamCreateWithFlags(&e->io_out, cudaStreamNonBlocking));
+    }
+    while ((int)e->io_ev.size() < 3 * chunks + 1) {
+        cudaEvent_t ev;
+        BB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        e->io_ev.push_back(ev);
+    }
+    cudaEvent_t* ev_in = e->io_ev.data();
+    cudaEvent_t* ev_done = ev_in + chunks;
+    cudaEvent_t* ev_out = ev_done + chunks;
+    cudaEvent_t ev_start = e->io_ev[3 * chunks];
+    const int64_t n = e->n;
+    const size_t esz = e->precision == BLOND_PREC_F64 ? sizeof(double) : sizeof(float);
+    std::vector<int64_t> off((size_t)chunks + 1);
+    for (int c = 0; c < chunks; ++c) off[c] = (n * c / chunks) & ~(int64_t)1;
+    off[chunks] = n;
+    double* ddt = static_cast<double*>(e->dt);
+    char* ddE = static_cast<char*>(e->dE);
+    char* hdE = static_cast<char*>(host_dE);
+    // earlier work on the caller's stream touches the device coordinates
+    BB_CUDA(cudaEventRecord(ev_start, s));
+    BB_CUDA(cudaStreamWaitEvent(e->io_in, ev_start, 0));
+    for (int64_t t = 0; t < n_turns; ++t) {
+        for (int c = 0; c < chunks; ++c) {
+            const int64_t o = off[c], m = off[c + 1] - off[c];
+            // the previous turn's copy-out of this chunk has read it
+            if (t > 0) BB_CUDA(cudaStreamWaitEvent(e->io_in, ev_out[c], 0));
+            BB_CUDA(cudaMemcpyAsync(ddt + o, host_dt + o, sizeof(double) * m,
+                                    cudaMemcpyHostToDevice, e->io_in));
+            BB_CUDA(cudaMemcpyAsync(ddE + esz * o, hdE + esz * o, esz * m,
+                                    cudaMemcpyHostToDevice, e->io_in));
+            BB_CUDA(cudaEventRecord(ev_in[c], e->io_in));
+        }
+        if ((rc = launch_head(e, s))) return rc;
+        for (int c = 0; c < chunks; ++c) {
+            const int64_t o = off[c], m = off[c + 1] - off[c];
+            BB_CUDA(cudaStreamWaitEvent(s, ev_in[c], 0));
+            if (m > 0 && (rc = launch_particles_range(e, o, m, s))) return rc;
+            BB_CUDA(cudaEventRecord(ev_done[c], s));
+            BB_CUDA(cudaStreamWaitEvent(e->io_out, ev_done[c], 0));
+            BB_CUDA(cudaMemcpyAsync(host_dt + o, ddt + o, sizeof(double) * m,
+                                    cudaMemcpyDeviceToHost, e->io_out));
+            BB_CUDA(cudaMemcpyAsync(hdE + esz * o, ddE + esz * o, esz * m,
+                                    cudaMemcpyDeviceToHost, e->io_out));
+            BB_CUDA(cudaEventRecord(ev_out[c], e->io_out));
+        }
+    }
+    e->host_turn += n_turns;
+    if ((rc = launch_profile(e, false, s))) return rc;
+    // the caller's stream completes only after the last copy-out
+    BB_CUDA(cudaStreamWaitEvent(s, ev_out[chunks - 1], 0));
+    return BLOND_OK;
 }
 
 int blond_engine_time_kernels(blond_engine* e, int64_t n_turns, double* head_ms,

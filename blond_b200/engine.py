@@ -250,6 +250,31 @@ class FusedTracker:
         self.beam.energy = float(rf.energy[t])
         self.beam.momentum = float(rf.momentum[t])
 
+    def track_host(self, host_dt: torch.Tensor, host_dE: torch.Tensor, n_turns: int = 1,
+                   chunks: int = 16):
+        """Advance n_turns on coordinates held in (pinned) host tensors:
+        every turn copies them in, tracks and copies them back, pipelined in
+        chunks against the particle pass (blond_engine_track_host)."""
+        edt = torch.float64 if self.precision == "f64" else torch.float32
+        if host_dt.device.type != "cpu" or host_dE.device.type != "cpu":
+            raise ValueError("track_host takes host tensors")
+        if host_dt.dtype != torch.float64 or host_dE.dtype != edt:
+            raise TypeError(f"host arrays must be float64 dt and {edt} dE")
+        if host_dt.numel() != self.dt.numel() or host_dE.numel() != self.dE.numel():
+            raise ValueError("host arrays must hold the bound beam")
+        if not (host_dt.is_contiguous() and host_dE.is_contiguous()):
+            raise ValueError("host arrays must be contiguous")
+        self._maybe_tune()
+        self.eng.call("track_host", ct.c_void_p(host_dt.data_ptr()),
+                      ct.c_void_p(host_dE.data_ptr()), int(n_turns), int(chunks), _stream())
+        rf = self.rf
+        rf.counter[0] += int(n_turns)
+        t = rf.counter[0]
+        self.beam.beta = float(rf.beta[t])
+        self.beam.gamma = float(rf.gamma[t])
+        self.beam.energy = float(rf.energy[t])
+        self.beam.momentum = float(rf.momentum[t])
+
     def prepare(self):
         """Build and upload the CUDA graph now (otherwise the first track()
         of at least turns_per_graph turns builds it)."""

@@ -232,6 +232,14 @@ int blond_engine_time_kernels(blond_engine* engine, int64_t n_turns,
  * part 1 = head (profile, induced voltage, table; clears the histogram),
  * part 2 = particle pass of the current turn (advances the turn),
  * part 3 = profile <- histogram. */
+/* Turns on coordinates in HOST memory (host_dt doubles, host_dE of the
+ * engine's precision, n particles each; page-locked memory lets the copies
+ * overlap).  Each turn copies the beam to the bound device arrays, runs the
+ * turn and copies it back, in `chunks` pieces pipelined against the
+ * particle pass (in and out copies on two streams).  The caller's stream
+ * completes after the last copy. */
+int blond_engine_track_host(blond_engine* engine, double* host_dt, void* host_dE,
+                            int64_t n_turns, int chunks, void* stream);
 int blond_engine_bind_histogram(blond_engine* engine, int* hist);
 int blond_engine_step(blond_engine* engine, int part, void* stream);
 /* Grid size and block size of the particle kernel (0 = automatic). */

@@ -367,3 +367,37 @@ def test_packed_histogram_counter_wraps(cuda, precision):
     assert got[100] > 2e7 and got[100 + S // 2] > 2e7
     np.testing.assert_array_equal(got, want)
     np.testing.assert_array_equal(fused.dt.cpu().numpy(), dt)
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32p64"])
+@pytest.mark.parametrize("chunks", [1, 3, 7])
+def test_track_host_matches_device_tracking(cuda, precision, chunks):
+    """Turns on page-locked host arrays, copied in and out every turn in
+    chunks pipelined against the particle pass, give the device result bit
+    for bit."""
+    g = golden("track_full.npz")
+    nt = int(g["n_turns"][0])
+    out = []
+    for host in (False, True):
+        ring, rf, beam = build(g)
+        prof = make_profile(g, beam)
+        tiv = TotalInducedVoltage(beam, prof, impedance_objects("track_full.npz", beam, prof, rf))
+        f = FusedTracker(RingAndRFTracker(rf, beam), prof, tiv, precision=precision)
+        if host:
+            hdt = f.dt.cpu().pin_memory()
+            hdE = f.dE.cpu().pin_memory()
+            f.track_host(hdt, hdE, nt - 1, chunks=chunks)
+            f.track_host(hdt, hdE, 1, chunks=chunks)
+            torch.cuda.synchronize()
+            out.append((hdt.numpy().copy(), hdE.numpy().copy(),
+                        f.profile_tensor().cpu().numpy()))
+        else:
+            f.track(nt)
+            out.append((f.dt.cpu().numpy(), f.dE.cpu().numpy(),
+                        f.profile_tensor().cpu().numpy()))
+        assert rf.counter[0] == nt
+    for a, b in zip(out[0], out[1]):
+        np.testing.assert_array_equal(a, b)
+    if precision == "f64":
+        assert normwise(out[1][0], g["dt"]) < 1e-11
+        np.testing.assert_array_equal(out[1][2], g["profiles"][-1])
