@@ -60,6 +60,12 @@ def parse():
                          "c5: 1e8 particles, "
                          "2^16 slices, 4 resonators + inductive Z/n")
     ap.add_argument("--beams", type=int, default=256)
+    ap.add_argument("--tune", default="auto", choices=["auto", "fixed"],
+                    help="fixed: no autotuner; --threads/--blocks-per-sm/--prefetch "
+                         "give the particle pass's launch shape (profiling runs)")
+    ap.add_argument("--threads", type=int, default=1024)
+    ap.add_argument("--blocks-per-sm", type=int, default=1)
+    ap.add_argument("--prefetch", type=int, default=2, choices=[0, 2, 4])
     return ap.parse_args()
 
 
@@ -211,7 +217,7 @@ def barrier(world):
 
 
 # ----------------------------------------------------------------- our arm
-def build_fused(n, S, n_turns, precision, kernel="auto", seed=0, group=None):
+def build_fused(n, S, n_turns, precision, kernel="auto", seed=0, group=None, shape=None):
     """One beam of n macro-particles per GPU.  With a process group the GPUs
     hold shards of ONE beam (seed = rank: independent samples of the same
     bunch) whose histogram is summed every turn; the charge per
@@ -231,8 +237,15 @@ def build_fused(n, S, n_turns, precision, kernel="auto", seed=0, group=None):
     iv = InducedVoltageFreq(beam, prof, [Resonators(5e6, 1e9, 1.0)])
     tiv = TotalInducedVoltage(beam, prof, [iv])
     tracker = RingAndRFTracker(rf, beam)
-    fused = FusedTracker(tracker, prof, tiv, precision=precision, turns_per_graph=50,
-                         kernel=kernel, process_group=group)
+    if shape is None:
+        fused = FusedTracker(tracker, prof, tiv, precision=precision, turns_per_graph=50,
+                             kernel=kernel, process_group=group)
+    else:
+        threads, bps, ring = shape
+        fused = FusedTracker(tracker, prof, tiv, precision=precision, turns_per_graph=50,
+                             kernel="plain", threads=threads, blocks_per_sm=bps,
+                             process_group=group, tune="fixed")
+        fused.eng.call("set_prefetch", ring)
     return fused, beam, iv.n_fft
 
 
@@ -260,8 +273,10 @@ def run_ours(args, world, rank, local):
     if world > 1:
         import torch.distributed as dist
         group = dist.group.WORLD
+    shape = ((args.threads, args.blocks_per_sm, args.prefetch) if args.tune == "fixed"
+             else None)
     fused, beam, n_fft = build_fused(n, S, total, args.precision, args.kernel, seed=rank,
-                                     group=group)
+                                     group=group, shape=shape)
     fused.track(W)
     if group is None:
         fused.prepare()  # graph capture/upload outside the timed region
@@ -327,7 +342,7 @@ def run_ours(args, world, rank, local):
     if rank == 0 and world == 1 and not args.no_mixed and args.precision == "f64":
         del fused, beam
         torch.cuda.empty_cache()
-        fm, bm_, _ = build_fused(n, S, W + K + kt + 4, "f32p64", args.kernel)
+        fm, bm_, _ = build_fused(n, S, W + K + kt + 4, "f32p64", args.kernel, shape=shape)
         fm.track(W)
         fm.prepare()
         ms32 = time_turns(fm, K)
