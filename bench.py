@@ -403,7 +403,8 @@ def run_reference(args, world, rank):
 C3_WORKLOAD = ("256 independent beams, double RF h=4620/18480 V2/V1=0.1 phi2=pi, "
                "V1 ~ U(2,7) MV, N_b log-uniform in [1e5, 4e6], sigma_dt ~ U(0.2,0.5) ns, "
                "512 slices, 3 resonators (R 2e5/1e5/5e4 Ohm, f_r 0.2/0.8/1.4 GHz, "
-               "Q log-uniform [100, 30000]), intensity 2e6 e per macro-particle")
+               "Q log-uniform [100, 30000]), intensity 1e11 protons per beam")
+C3_INTENSITY = 1e11
 
 
 def c3_beams(n_beams, turns, seed=1234, scale_particles=1.0):
@@ -427,13 +428,19 @@ def c3_beams(n_beams, turns, seed=1234, scale_particles=1.0):
         rf = RFStation(ring, [4620, 4 * 4620], [V1, 0.1 * V1], [0.0, np.pi], n_rf=2)
         centre = (rf.phi_s[0] - rf.phi_rf[0, 0]) / rf.omega_rf[0, 0]
         dt, dE = bigaussian_arrays(n, sdt, _get_dE_from_dt(ring, rf, sdt), centre, seed + k)
-        beam = Beam(ring, n, 2e6 * n, dt=dt, dE=dE, dtype=torch.float64)
+        beam = Beam(ring, n, C3_INTENSITY, dt=dt, dE=dE, dtype=torch.float64)
         prof = Profile(beam, CutOptions(cut_left=centre - 1.25e-9,
                                         cut_right=centre + 1.25e-9, n_slices=512))
         iv = InducedVoltageFreq(beam, prof, [Resonators([2e5, 1e5, 5e4],
                                                         [200e6, 800e6, 1.4e9], Q)])
         out.append((rf, beam, prof, TotalInducedVoltage(beam, prof, [iv])))
     return out
+
+
+def ct_stream():
+    import ctypes
+    import torch
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
 
 
 def run_c3(args):
@@ -444,7 +451,8 @@ def run_c3(args):
     from blond_b200.engine import FusedTracker
     from blond_b200.trackers.tracker import RingAndRFTracker
     W, K = max(3, args.warmup), args.steps
-    beams = c3_beams(args.beams, 2 * (W + K) + 4)
+    T_err = max(1000, W + K)  # turns after which the precision is compared
+    beams = c3_beams(args.beams, T_err + W + K + 4)
     n_total = sum(b.n_macroparticles for _, b, _, _ in beams)
     res = {}
     for prec in ("f32p64", "f64"):
@@ -453,20 +461,36 @@ def run_c3(args):
         bt.track(W)
         bt.prepare()
         ms = time_turns(bt, K)
+        bt.track(T_err - W - K)  # untimed, to the comparison turn
         res[prec] = (n_total * K / (ms * 1e-3), ms / K, bt)
         for rf, _, _, _ in beams:
             rf.counter[0] = 0
-    # F32P64 vs FP64 after W + K turns: rms bunch length / energy spread
-    errs = []
+    # control: FP64 again from initial times moved by one ulp -- how far the
+    # dynamics alone separate two runs that differ by rounding
+    bp = BatchTracker([(RingAndRFTracker(rf, b), p, t) for rf, b, p, t in beams],
+                      precision="f64")
+    bp.dt.copy_(torch.nextafter(bp.dt, torch.full_like(bp.dt, float("inf"))))
+    bp._call("slice", ct_stream())
+    bp.track(T_err)
+    for rf, _, _, _ in beams:
+        rf.counter[0] = 0
+
+    # F32P64 (and the control) vs FP64 after W + K turns: rms bunch length /
+    # energy spread of the particles in the window
+    def rel_errs(other, ref):
+        out = []
+        for k, (_, _, p, _) in enumerate(beams):
+            x = [t.double().cpu().numpy() for t in ref.coordinates(k)]
+            y = [t.double().cpu().numpy() for t in other.coordinates(k)]
+            w = (x[0] > p.cut_left) & (x[0] < p.cut_right)
+            out.append([abs(np.std(v[w]) / np.std(u[w]) - 1) for u, v in zip(x, y)])
+        return np.array(out)
+
     b32, b64 = res["f32p64"][2], res["f64"][2]
-    for k, (_, _, p, _) in enumerate(beams):
-        x = [t.double().cpu().numpy() for t in b64.coordinates(k)]
-        y = [t.double().cpu().numpy() for t in b32.coordinates(k)]
-        w = (x[0] > p.cut_left) & (x[0] < p.cut_right)
-        errs.append([abs(np.std(v[w]) / np.std(u[w]) - 1) for u, v in zip(x, y)])
-    errs = np.array(errs)
+    errs = rel_errs(b32, b64)
+    floor = rel_errs(bp, b64)
     vals = {p: (res[p][0], res[p][1]) for p in res}
-    del b32, b64, res
+    del b32, b64, bp, res
     torch.cuda.empty_cache()
     # the unbatched plain path: every beam through its own FP64 engine
     engines = [FusedTracker(RingAndRFTracker(rf, b), p, t, precision="f64",
@@ -484,7 +508,7 @@ def run_c3(args):
     torch.cuda.synchronize()
     ms_plain = a.elapsed_time(b)
     plain = n_total * K / (ms_plain * 1e-3)
-    return vals, plain, ms_plain / K, errs, n_total
+    return vals, plain, ms_plain / K, errs, floor, n_total, T_err
 
 
 C5_WORKLOAD = ("1e8 protons 26 GeV/c, double RF h=4620/18480 4.5/0.45 MV (phi 0/pi), "
@@ -656,7 +680,7 @@ def main():
         return
     if args.workload == "c3" and args.impl == "ours":
         W, K = max(3, args.warmup), args.steps
-        vals, plain, ms_plain, errs, n_total = run_c3(args)
+        vals, plain, ms_plain, errs, floor, n_total, T_err = run_c3(args)
         print(json.dumps({
             "metric": METRIC, "value": vals["f32p64"][0], "unit": UNIT, "n_gpus": 1,
             "steps": K, "warmup": W, "ms_per_step": vals["f32p64"][1],
@@ -668,7 +692,7 @@ def main():
             "unbatched_plain_f64": {"value": plain, "ms_per_step": ms_plain},
             "speedup_f32p64_batched_vs_unbatched_f64": vals["f32p64"][0] / plain,
             "f32p64_rel_err_after_turns": {
-                "turns": W + K,
+                "turns": T_err,
                 "statistic": "in-window rms of dt and dE, per beam, F32P64 vs FP64 batch",
                 "sigma_dt_median": float(np.median(errs[:, 0])),
                 "sigma_dt_p90": float(np.percentile(errs[:, 0], 90)),
@@ -676,7 +700,16 @@ def main():
                 "sigma_dE_median": float(np.median(errs[:, 1])),
                 "sigma_dE_p90": float(np.percentile(errs[:, 1], 90)),
                 "sigma_dE_max": float(errs[:, 1].max()),
-                "beams_within_1e-5": int(np.sum(errs.max(axis=1) <= 1e-5))},
+                "beams_within_1e-5": int(np.sum(errs.max(axis=1) <= 1e-5)),
+                "control_fp64_one_ulp": {
+                    "statistic": "the same, FP64 from initial dt moved by one ulp vs FP64",
+                    "sigma_dt_median": float(np.median(floor[:, 0])),
+                    "sigma_dt_p90": float(np.percentile(floor[:, 0], 90)),
+                    "sigma_dE_median": float(np.median(floor[:, 1])),
+                    "sigma_dE_p90": float(np.percentile(floor[:, 1], 90)),
+                    "beams_within_1e-5": int(np.sum(floor.max(axis=1) <= 1e-5))},
+                "beams_f32p64_within_1e-5_or_control": int(np.sum(
+                    errs.max(axis=1) <= np.maximum(1e-5, 2 * floor.max(axis=1))))},
             "gpu_launches": 2 * K,
         }), flush=True)
         return
