@@ -383,11 +383,56 @@ def _traffic(precision, n):
 
 
 # ----------------------------------------------------------------- ref arm
+def gpu_reference(n: int, S: int, turns: int, warmup: int):
+    """The reference's own GPU kernels (blond/gpu/kernels.cu rebuilt for
+    sm_100a) + cuFFT, driven in the reference objects' order on device-
+    resident coordinates; returns (particle-turns/s, ms per turn) or None
+    when the kernels were not built or no GPU is present."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_cpu
+    import ref_gpu
+    import torch
+    if not (ref_gpu.available() and torch.cuda.is_available()):
+        return None
+    ring, rf = machine(turns + warmup + 2)
+    dt, dE, centre = host_bunch(ring, rf, n)
+    cl, cr, bc = window(centre, S)
+    bin_size = (cr - cl) / S
+    Z = _resonator_host(ref_cpu.CpuPath(), np.fft.rfftfreq(S, bin_size)) / bin_size
+    path = ref_gpu.RefGpuPath()
+    path.setup(ref_cpu.programme(rf), turns + warmup)
+    ddt, ddE = torch.tensor(dt, device="cuda"), torch.tensor(dE, device="cuda")
+    prof = torch.zeros(S, dtype=torch.float64, device="cuda")
+    dbc = torch.tensor(bc, device="cuda")
+    dZ = torch.tensor(Z, device="cuda")
+    factor = torch.empty(2 * (S - 1), dtype=torch.float64, device="cuda")
+    path.slice(ddt, prof, cl, cr)
+    args = ((cl, cr), dbc, dZ, S, 1.0, 1e10 / n, factor)
+    for t in range(warmup):
+        path.turn(t, ddt, ddE, prof, *args)
+    s = torch.cuda.current_stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record(s)
+    for t in range(warmup, warmup + turns):
+        path.turn(t, ddt, ddE, prof, *args)
+    b.record(s)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / turns
+    return n / (ms * 1e-3), ms
+
+
 def run_reference(args, world, rank):
     n = int(args.particles)
     W, K = max(3, args.warmup), args.steps
     v, turns, kind, cores, sec = cpu_reference(n, args.slices, K, None, warmup=W)
-    return {
+    g = gpu_reference(n, args.slices, K, W)
+    extra = {} if g is None else {"reference_gpu_kernels": {
+        "value": g[0], "unit": UNIT, "ms_per_step": g[1],
+        "what": "the reference's blond/gpu/kernels.cu rebuilt for sm_100a as blond/compile.py "
+                "builds it (--use_fast_math, -maxrregcount 32), 2 x SMs blocks of 1024 "
+                "threads, cuFFT for the FFT step, device-resident coordinates, FP64"}}
+    return {**extra,
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
         "steps": K, "warmup": W, "ms_per_step": sec / K * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
