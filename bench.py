@@ -170,17 +170,17 @@ def cpu_reference(n: int, S: int, turns: int | None, seconds: float | None,
     return n * turns / sec, turns, path.kind, path.cores, sec
 
 
-def _resonator_host(path, freq):
+def _resonator_host(path, freq, R=(5e6,), Q=(1.0,), fr=(1e9,)):
     """Impedance on the host with the reference's own fast_resonator (or the
     restatement when the reference library is absent)."""
     import ctypes as ct
     f = np.ascontiguousarray(freq, dtype=np.float64)
     re, im = np.zeros(len(f)), np.zeros(len(f))
-    R, Q, fr = np.array([5e6]), np.array([1.0]), np.array([1e9])
+    R, Q, fr = (np.ascontiguousarray(x, dtype=np.float64) for x in (R, Q, fr))
     P = lambda a: a.ctypes.data_as(ct.c_void_p)  # noqa: E731
     fn = getattr(path.lib, "fast_resonator_real_imag", None) or \
         getattr(path.lib, "oracle_fast_resonator_f64")
-    fn(P(re), P(im), P(f), P(R), P(Q), P(fr), ct.c_int(1), ct.c_int(len(f)))
+    fn(P(re), P(im), P(f), P(R), P(Q), P(fr), ct.c_int(len(R)), ct.c_int(len(f)))
     return re + 1j * im
 
 
@@ -441,6 +441,85 @@ def run_reference(args, world, rank):
                    "parallelism": f"{cores} host threads"},
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind,
                          "sample": f"{K} turns of the full workload after {W} warm-up"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def run_reference_c3(args):
+    """The reference on the C3 batch: every beam through its own objects,
+    one after the other -- on the GPU with the reference's kernels rebuilt
+    for sm_100a (the plain FP64 GPU path), and a bounded CPU sample."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_cpu
+    import ref_gpu
+    import torch
+    W, K = 2, max(1, min(args.steps, 5))
+    beams = c3_beams(args.beams, W + K + 4)
+    n_total = sum(b.n_macroparticles for _, b, _, _ in beams)
+    cpu = ref_cpu.CpuPath()
+    S = 512
+    items = []
+    for rf, beam, prof, tiv in beams:
+        iv = tiv.induced_voltage_list[0]
+        res = iv.impedance_source_list[0]
+        bs = float(prof.bin_size)
+        Z = _resonator_host(cpu, np.fft.rfftfreq(iv.n_fft, bs), res.R_S, res.Q,
+                            res.frequency_R) / bs
+        items.append((rf, beam, prof, iv.n_fft, Z))
+    out = {}
+    if ref_gpu.available() and torch.cuda.is_available():
+        path = ref_gpu.RefGpuPath()
+        state = []
+        for rf, beam, prof, n_fft, Z in items:
+            dt = beam.dt.detach().to("cuda", torch.float64).clone()
+            dE = beam.dE.detach().to("cuda", torch.float64).clone()
+            p = torch.zeros(S, dtype=torch.float64, device="cuda")
+            cuts = (float(prof.cut_left), float(prof.cut_right))
+            path.slice(dt, p, *cuts)
+            state.append((dt, dE, p, cuts, torch.tensor(np.asarray(prof.bin_centers),
+                                                        device="cuda"),
+                          torch.tensor(Z, device="cuda"), n_fft,
+                          float(rf.particle.charge), float(beam.ratio),
+                          torch.empty(2 * (S - 1), dtype=torch.float64, device="cuda"),
+                          path.programme(ref_cpu.programme(rf))))
+
+        def one_turn(t):
+            for dt, dE, p, cuts, bc, Z, n_fft, q, ratio, fac, prog in state:
+                path.turn(t, dt, dE, p, cuts, bc, Z, n_fft, q, ratio, fac, prog=prog)
+
+        for t in range(W):
+            one_turn(t)
+        s = torch.cuda.current_stream()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(s)
+        for t in range(W, W + K):
+            one_turn(t)
+        b.record(s)
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / K
+        out["reference_gpu_kernels"] = {
+            "value": n_total / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
+            "what": "every beam through the reference's GPU kernels (blond/gpu/kernels.cu "
+                    "rebuilt for sm_100a) + cuFFT, beam after beam as its objects run, FP64"}
+    # CPU: one turn of every beam
+    sec = 0.0
+    for rf, beam, prof, n_fft, Z in items:
+        dt = beam.dt.detach().cpu().numpy().astype(np.float64).copy()
+        dE = beam.dE.detach().cpu().numpy().astype(np.float64).copy()
+        sec += cpu.run(dt, dE, ref_cpu.programme(rf), 1, 0, impedance=(n_fft, Z),
+                       cuts=(float(prof.cut_left), float(prof.cut_right)),
+                       bin_centers=np.asarray(prof.bin_centers), n_slices=S,
+                       charge=float(rf.particle.charge), ratio=float(beam.ratio))
+    v = n_total / sec
+    return {
+        **out, "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": 1,
+        "steps": 1, "warmup": 0, "ms_per_step": sec * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": C3_WORKLOAD, "beams": args.beams, "particles_total": n_total,
+                   "slices": S, "n_fft": S, "parallelism": f"{cpu.cores} host threads"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cpu.cores, "kind": cpu.kind,
+                         "sample": "one turn of every beam"},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
@@ -763,6 +842,9 @@ def main():
         world = int(os.environ.get("WORLD_SIZE", "1"))
         rank = int(os.environ.get("RANK", "0"))
         if rank != 0:
+            return
+        if args.workload == "c3":
+            print(json.dumps(run_reference_c3(args)), flush=True)
             return
         print(json.dumps(run_reference(args, world, rank)), flush=True)
         return

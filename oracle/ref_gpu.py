@@ -65,18 +65,24 @@ class RefGpuPath:
     def _stream():
         return ct.c_void_p(torch.cuda.current_stream().cuda_stream)
 
-    def setup(self, prog, n_turns_total):
-        """Device copies of the programme: (n_turns+1, n_rf) arrays."""
+    @staticmethod
+    def programme(prog):
+        """Device copies of a programme (oracle/ref_cpu.programme): RF
+        arrays as (n_turns+1, n_rf), acceleration kicks and drift tuples."""
         dev = "cuda"
-        self.V = torch.tensor(prog["V"].T.copy(), device=dev)
-        self.om = torch.tensor(prog["om"].T.copy(), device=dev)
-        self.ph = torch.tensor(prog["ph"].T.copy(), device=dev)
-        self.acc = [float(x) for x in prog["acc"]]
-        self.drift = prog["drift"]
+        return dict(V=torch.tensor(prog["V"].T.copy(), device=dev),
+                    om=torch.tensor(prog["om"].T.copy(), device=dev),
+                    ph=torch.tensor(prog["ph"].T.copy(), device=dev),
+                    acc=[float(x) for x in prog["acc"]], drift=prog["drift"])
 
-    def turn(self, t, dt, dE, profile, cuts, bc, Z, n_fft, charge, ratio, factor):
+    def setup(self, prog, n_turns_total):
+        """Make `prog` the programme turn() uses by default."""
+        self.prog = self.programme(prog)
+
+    def turn(self, t, dt, dE, profile, cuts, bc, Z, n_fft, charge, ratio, factor, prog=None):
         n, S = dt.numel(), profile.numel()
         s = self._stream()
+        p = prog or self.prog
         if Z is not None:
             spec = torch.fft.rfft(profile, n_fft)
             v = -(charge * E_CHARGE * ratio) * torch.fft.irfft(Z * spec, n_fft)
@@ -84,10 +90,10 @@ class RefGpuPath:
             self._check(self.lib.refgpu_lik(self._p(dt), self._p(dE), self._p(v),
                                             self._p(bc), charge, S, n, 0.0,
                                             self._p(factor), s))
-        self._check(self.lib.refgpu_kick(self._p(dt), self._p(dE), self.V.shape[1], charge,
-                                         self._p(self.V[t]), self._p(self.om[t]),
-                                         self._p(self.ph[t]), n, self.acc[t], s))
-        a = self.drift[t + 1]
+        self._check(self.lib.refgpu_kick(self._p(dt), self._p(dE), p["V"].shape[1], charge,
+                                         self._p(p["V"][t]), self._p(p["om"][t]),
+                                         self._p(p["ph"][t]), n, p["acc"][t], s))
+        a = p["drift"][t + 1]
         self._check(self.lib.refgpu_drift(self._p(dt), self._p(dE), 0, *[float(x) for x in a],
                                           n, s))
         self.slice(dt, profile, *cuts)
