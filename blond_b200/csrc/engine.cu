@@ -1930,25 +1930,36 @@ particle_kernel_batch(const BatchArgs a) {
                              (long long)b * S * (PREC == PREC_F64 ? 16 : 8)
                        : nullptr;
         const double cl = a.cut_left[b], iw = a.inv_w[b];
-        for (int i = threadIdx.x; i < count; i += 2 * blockDim.x) {
-            const int i2 = i + blockDim.x;
-            const bool two = i2 < count;
-            double t0 = dt[start + i], t1 = two ? dt[start + i2] : t0;
-            E e0 = dE[start + i], e1 = two ? dE[start + i2] : e0;
+        // four particles per thread and iteration (i + q * blockDim, q < 4),
+        // all loads issued before any arithmetic: with two, each SM had
+        // only ~16 KB of loads in flight, which caps HBM near 2.4 TB/s
+        const int bd = blockDim.x;
+        for (int i = threadIdx.x; i < count; i += 4 * bd) {
+            double t[4];
+            E e[4];
+            bool in[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                in[q] = i + q * bd < count;
+                const long long g = start + i + (in[q] ? q * bd : 0);
+                t[q] = dt[g];
+                e[q] = dE[g];
+            }
             if (KICK) {
-                track_pair<PREC, SOLVER, LIK>(t0, t1, e0, e1, c, pa, a.order);
-                dt[start + i] = t0;
-                dE[start + i] = e0;
-                if (two) {
-                    dt[start + i2] = t1;
-                    dE[start + i2] = e1;
+                track_pair<PREC, SOLVER, LIK>(t[0], t[1], e[0], e[1], c, pa, a.order);
+                track_pair<PREC, SOLVER, LIK>(t[2], t[3], e[2], e[3], c, pa, a.order);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    if (in[q]) {
+                        dt[start + i + q * bd] = t[q];
+                        dE[start + i + q * bd] = e[q];
+                    }
                 }
             }
-            const int b0 = engine_bin(t0, cl, iw, S);
-            if (b0 >= 0) atomicAdd(&sh[b0], 1);
-            if (two) {
-                const int b1 = engine_bin(t1, cl, iw, S);
-                if (b1 >= 0) atomicAdd(&sh[b1], 1);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int bq = in[q] ? engine_bin(t[q], cl, iw, S) : -1;
+                if (bq >= 0) atomicAdd(&sh[bq], 1);
             }
         }
         __syncthreads();
