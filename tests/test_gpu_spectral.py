@@ -1,5 +1,6 @@
-"""Cluster FFT, irfft and one-turn induced voltage vs numpy (pocketfft, the
-library the reference calls).  Bar: 1e-10 normwise (induced voltage), the
+"""Cluster and single-CTA FFTs, irfft and one-turn induced voltage vs numpy
+(pocketfft, the library the reference calls); n_fft = 4096, 8192 and 16384
+take the single-CTA chain, the other lengths the cluster kernel.  Bar: 1e-10 normwise (induced voltage), the
 parity definition for this step; the transforms themselves reach ~1e-15."""
 import numpy as np
 import pytest
@@ -13,7 +14,7 @@ pytestmark = pytest.mark.gpu
 
 # even 5-smooth lengths (cluster path), incl. next_regular values such as
 # 1080, and lengths the direct-DFT path handles (odd / prime factor > 5)
-SMOOTH = [2, 4, 16, 32, 60, 1080, 2048, 3000, 16384, 32768, 65536, 131072]
+SMOOTH = [2, 4, 16, 32, 60, 1080, 2048, 3000, 4096, 8192, 16384, 32768, 65536, 131072]
 DIRECT = [1, 7, 1001, 1014, 4096 - 2]
 
 
@@ -36,7 +37,8 @@ def test_rfft_zero_pads_and_truncates(cuda):
 
 
 @pytest.mark.parametrize("S,n_fft", [(16, 16), (16, 1080), (100, 100), (1024, 1024),
-                                     (512, 2048), (16384, 16384), (65536, 65536)])
+                                     (512, 2048), (4096, 4096), (3000, 8192), (8192, 8192),
+                                     (10000, 16384), (16384, 16384), (65536, 65536)])
 def test_induced_voltage_1turn(cuda, S, n_fft):
     rng = np.random.default_rng(S)
     prof = np.floor(1000 * np.exp(-np.linspace(-3, 3, S) ** 2) + rng.random(S))
