@@ -1,6 +1,5 @@
-"""Cluster and single-CTA FFTs, irfft and one-turn induced voltage vs numpy
-(pocketfft, the library the reference calls); n_fft = 4096, 8192 and 16384
-take the single-CTA chain, the other lengths the cluster kernel.  Bar: 1e-10 normwise (induced voltage), the
+"""Cluster FFT, irfft and one-turn induced voltage vs numpy (pocketfft, the
+library the reference calls).  Bar: 1e-10 normwise (induced voltage), the
 parity definition for this step; the transforms themselves reach ~1e-15."""
 import numpy as np
 import pytest
