@@ -37,7 +37,7 @@ WORKLOAD = ("1e7 protons 26 GeV/c, h=4620 4.5 MV, 2^14 slices, broadband "
             "resonator 5 MOhm/1 GHz/Q=1 via FFT (n_fft 16384), lik + kick + "
             "drift + slice per turn")
 BYTES_PER_PARTICLE = {"f64": 32, "f32p64": 24}  # read + write of dt and dE
-E2E_CHUNKS = 16
+E2E_CHUNKS = 4
 
 
 def parse():

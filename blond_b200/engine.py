@@ -251,7 +251,7 @@ class FusedTracker:
         self.beam.momentum = float(rf.momentum[t])
 
     def track_host(self, host_dt: torch.Tensor, host_dE: torch.Tensor, n_turns: int = 1,
-                   chunks: int = 16):
+                   chunks: int = 4):
         """Advance n_turns on coordinates held in (pinned) host tensors:
         every turn copies them in, tracks and copies them back, pipelined in
         chunks against the particle pass (blond_engine_track_host)."""
