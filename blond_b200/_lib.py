@@ -110,7 +110,16 @@ _EXTRA = {
                                     c_int, c_dbl, c_dbl, c_ptr, c_ptr, c_ptr],
     "blond_adjoint_spectral": [c_int, c_ptr, c_int, c_ptr, c_i64, c_dbl, c_ptr, c_ptr,
                                c_ptr, c_ptr],
+    "blond_resonator_workspace_bytes": [c_int, c_int],
+    "blond_resonator_induced_voltage_f64": [c_ptr, c_ptr, c_int, c_dbl, c_dbl, c_ptr,
+                                            c_i64, c_ptr, c_ptr, c_ptr, c_int, c_dbl,
+                                            c_ptr, c_ptr, c_ptr, c_i64, c_ptr],
+    "blond_interp_f64": [c_ptr, c_i64, c_dbl, c_ptr, c_ptr, c_int, c_dbl, c_dbl,
+                         c_int, c_ptr, c_ptr],
 }
+
+# entry points that return a value instead of a status
+_RESTYPE = {"blond_resonator_workspace_bytes": c_i64}
 
 
 def exported_symbols() -> list[str]:
@@ -146,7 +155,7 @@ def load(path: str | None = None) -> ct.CDLL:
         for k, argt in _EXTRA.items():
             f = getattr(lib, k)
             f.argtypes = argt
-            f.restype = c_int
+            f.restype = _RESTYPE.get(k, c_int)
         _lib = lib
         return lib
 

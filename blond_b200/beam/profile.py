@@ -95,10 +95,10 @@ class Profile:
         fit_options = fit_options or FitOptions()
         filter_options = filter_options or FilterOptions()
         other_slices_options = other_slices_options or OtherSlicesOptions()
-        if fit_options.fit_option is not None or filter_options.filter_method is not None:
+        if filter_options.filter_method is not None:
             raise NotImplementedError(
-                "profile fits and filters are host-side diagnostics outside the "
-                "tracking hot path; use the reference toolbox on a host copy")
+                "profile filters are host-side diagnostics outside the tracking "
+                "hot path; use the reference toolbox on a host copy")
         self.cut_options = cut_options
         cut_options.set_cuts(beam)
         self.beam = beam
@@ -111,6 +111,15 @@ class Profile:
         self.beam_spectrum_freq = np.array([])
         self.smooth = bool(other_slices_options.smooth)
         self.operations = [self._slice_smooth if self.smooth else self._slice]
+        self.fit_option = fit_options.fit_option
+        self.fit_extra_options = None
+        if self.fit_option is not None:
+            self.bunchPosition = 0.0
+            self.bunchLength = 0.0
+            fits = {"gaussian": self.apply_fit, "rms": self.rms, "fwhm": self.fwhm}
+            if self.fit_option not in fits:
+                raise NameError(f"{fit_options=}")
+            self.operations.append(fits[self.fit_option])
         if other_slices_options.direct_slicing and beam is not None:
             self.track()
 
@@ -125,6 +134,41 @@ class Profile:
     def _slice_smooth(self):
         bm.slice_smooth(self.beam.dt, self.n_macroparticles, self.cut_left,
                         self.cut_right)
+
+    # ------------------------------------------------------------ fits
+    # Bunch position and length (4 sigma) after each slicing, as the
+    # reference's Profile.apply_fit / rms / fwhm (profile.py:775-866) with
+    # toolbox/filters_and_fitting.py:129-215.  They are per-turn
+    # diagnostics, not part of the tracking arithmetic: rms reduces on the
+    # device; the Gaussian least-squares fit and the FWHM edge search run on
+    # a host copy of the profile, as the reference's GPU backend does for
+    # the fit (filters_and_fitting.py:138-141).
+    def apply_fit(self):
+        from scipy.optimize import curve_fit
+        y = self.n_macroparticles.double().cpu().numpy()
+        x = np.asarray(self.bin_centers, dtype=np.float64)
+        if self.bunchLength == 0:
+            dt = self.beam.dt.double()
+            p0 = [float(y.max()), float(dt.mean()), float(dt.std(unbiased=False))]
+        else:
+            p0 = [float(y.max()), float(self.bunchPosition), float(self.bunchLength / 4.0)]
+        self.fit_extra_options = curve_fit(_gauss, x, y, p0)[0]
+        self.bunchPosition = self.fit_extra_options[1]
+        self.bunchLength = 4 * self.fit_extra_options[2]
+
+    def rms(self):
+        y = self.n_macroparticles.double()
+        x = torch.as_tensor(np.asarray(self.bin_centers, dtype=np.float64), device=y.device)
+        dx = float(self.bin_centers[1] - self.bin_centers[0])
+        line = y / torch.trapezoid(y, dx=dx)
+        bp = torch.trapezoid(x * line, dx=dx)
+        bl = 4 * torch.sqrt(torch.trapezoid((x - bp) ** 2 * line, dx=dx))
+        self.bunchPosition, self.bunchLength = float(bp), float(bl)
+
+    def fwhm(self, shift: float = 0):
+        y = self.n_macroparticles.double().cpu().numpy()
+        x = np.asarray(self.bin_centers, dtype=np.float64)
+        self.bunchPosition, self.bunchLength = _fwhm(y, x, shift)
 
     def beam_spectrum_freq_generation(self, n_sampling_fft: int):
         self.beam_spectrum_freq = bm.rfftfreq(n_sampling_fft, self.bin_size)
@@ -143,3 +187,27 @@ class Profile:
         d[0] = (p[1] - p[0]) / dist
         d[-1] = (p[-1] - p[-2]) / dist
         return self.bin_centers, d
+
+
+def _gauss(x, *p):
+    """A exp(-(x - x0)^2 / (2 sx^2)) (filters_and_fitting.py:146-155)."""
+    A, x0, sx = p
+    return A * np.exp(-((x - x0) ** 2) / 2.0 / sx ** 2)
+
+
+def _fwhm(y, x, shift=0.0):
+    """Bunch position and 4-sigma length from the full width at half
+    maximum with linear interpolation of both edges
+    (filters_and_fitting.py:179-211); (nan, nan) when the right edge is the
+    last bin (at the first bin the left neighbour wraps to the last, as
+    numpy indexing does in the reference)."""
+    half = shift + 0.5 * (y.max() - shift)
+    above = np.where(y >= half)[0]
+    t1, t2 = above[0], above[-1]
+    w = x[1] - x[0]
+    try:
+        t_left = x[t1] - w * (y[t1] - half) / (y[t1] - y[t1 - 1])
+        t_right = x[t2] + w * (y[t2] - half) / (y[t2] - y[t2 + 1])
+    except IndexError:
+        return np.nan, np.nan
+    return (t_left + t_right) / 2, 4 * (t_right - t_left) / (2 * np.sqrt(2 * np.log(2)))

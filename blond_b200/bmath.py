@@ -14,13 +14,16 @@ import ctypes as ct
 
 import numpy as np
 import torch
+from scipy.constants import e
 
 from . import _lib
 
 __all__ = [
     "kick", "drift", "slice_beam", "slice_smooth", "linear_interp_kick",
     "rf_volt_comp", "fast_resonator", "rfft", "irfft", "rfftfreq",
-    "induced_voltage_1turn", "precision", "use_precision", "B200Backend",
+    "induced_voltage_1turn", "interp", "resonator_induced_voltage",
+    "resonator_induced_voltage_1_turn", "resonator_workspace",
+    "precision", "use_precision", "B200Backend",
 ]
 
 _SOLVERS = {"simple": 0, "legacy": 1, "exact": 2}
@@ -234,6 +237,112 @@ def induced_voltage_1turn(profile, total_impedance, n_fft, scale, n_out):
     return out
 
 
+# ------------------------------------------------------ time-domain wakes
+def interp(x, xp, fp, left=None, right=None, period=None, *, x_shift=0.0):
+    """numpy.interp(x + x_shift, xp, fp, left, right) on the device in
+    float64 (bm.interp, bmath_backends.py:373); a tensor shaped like x.
+    xp must be increasing, as numpy requires; ``period`` is not supported."""
+    if period is not None:
+        raise NotImplementedError("interp: period")
+    X = as_device(x, torch.float64)
+    shape = X.shape
+    X = X.reshape(-1).contiguous()
+    XP = as_device(xp, torch.float64, X.device).reshape(-1).contiguous()
+    FP = as_device(fp, torch.float64, X.device).reshape(-1).contiguous()
+    if XP.numel() == 0:
+        raise ValueError("array of sample points is empty")
+    if XP.numel() != FP.numel():
+        raise ValueError("fp and xp are not of the same length.")
+    out = torch.empty_like(X)
+    flags = (1 if left is not None else 0) | (2 if right is not None else 0)
+    _lib.call("blond_interp_f64", _ptr(X), X.numel(), float(x_shift), _ptr(XP),
+              _ptr(FP), XP.numel(), float(0.0 if left is None else left),
+              float(0.0 if right is None else right), flags, _ptr(out), _stream())
+    return out.reshape(shape)
+
+
+def resonator_workspace(n_slices: int, n_resonators: int, device=None):
+    """Scratch for resonator_induced_voltage (uint8 device tensor)."""
+    n = int(_lib.load().blond_resonator_workspace_bytes(int(n_slices),
+                                                        int(n_resonators)))
+    return torch.empty(n, dtype=torch.uint8, device=device or "cuda")
+
+
+def resonator_induced_voltage(profile, bin_centers, bin_size, beam_n_macroparticles,
+                              time_array, R, omega_r, Q, scale, out=None,
+                              tmp_matrix=None, workspace=None):
+    """Induced voltage of resonators by the analytic convolution of the
+    linearly interpolated line density (butils_wrap_python.py:656-790),
+    float64, one value per time_array point.  ``bin_centers`` must be
+    increasing; R, omega_r, Q are host sequences; ``scale`` is
+    -charge * e * beam_n_macroparticles * ratio.  ``tmp_matrix`` (optional,
+    n_resonators x n_time float64 tensor) receives the per-resonator rows;
+    ``workspace`` (from resonator_workspace) may be reused across calls.
+    Returns (induced_voltage, workspace)."""
+    p = as_device(profile, torch.float64).reshape(-1).contiguous()
+    bc = as_device(bin_centers, torch.float64, p.device).reshape(-1).contiguous()
+    t = as_device(time_array, torch.float64, p.device).reshape(-1).contiguous()
+    Rh = np.ascontiguousarray(np.asarray(R, dtype=np.float64).reshape(-1))
+    wh = np.ascontiguousarray(np.asarray(omega_r, dtype=np.float64).reshape(-1))
+    qh = np.ascontiguousarray(np.asarray(Q, dtype=np.float64).reshape(-1))
+    n_res = Rh.size
+    if not (wh.size == qh.size == n_res):
+        raise ValueError("R, omega_r and Q differ in length")
+    if p.numel() != bc.numel():
+        raise ValueError("profile and bin_centers differ in length")
+    if workspace is None:
+        workspace = resonator_workspace(bc.numel(), n_res, p.device)
+    if out is None:
+        out = torch.empty(t.numel(), dtype=torch.float64, device=p.device)
+    P = lambda a: a.ctypes.data_as(ct.c_void_p)  # noqa: E731
+    _lib.call("blond_resonator_induced_voltage_f64", _ptr(p), _ptr(bc), bc.numel(),
+              float(bin_size), float(beam_n_macroparticles), _ptr(t), t.numel(),
+              P(Rh), P(wh), P(qh), n_res, float(scale), _ptr(out),
+              _ptr(tmp_matrix) if tmp_matrix is not None else None,
+              _ptr(workspace), workspace.numel(), _stream())
+    return out, workspace
+
+
+def resonator_induced_voltage_1_turn(kappa1, n_macroparticles, bin_centers, bin_size,
+                                     n_time, deltaT, tArray, reOmegaP, imOmegaP,
+                                     Qtilde, n_resonators, omega_r, Q, tmp_matrix,
+                                     charge, beam_n_macroparticles, ratio, R,
+                                     induced_voltage, float_precision):
+    """butils_wrap_python.resonator_induced_voltage_1_turn (:656-790) with its
+    signature; returns (induced_voltage, deltaT).  reOmegaP, imOmegaP and
+    Qtilde are re-derived from omega_r and Q by the reference's formulas.
+    kappa1 and tmp_matrix are filled when they are device tensors of the
+    reference's shapes; deltaT, the n_time x n_slices matrix the reference
+    builds, is only filled when it is such a tensor (the kernel never needs
+    it)."""
+    bc = as_device(bin_centers, torch.float64)
+    if bc.numel() > 1 and not bool(torch.all(bc[1:] > bc[:-1])):
+        raise ValueError("bin_centers must be increasing")
+    t = as_device(tArray, torch.float64, bc.device).reshape(-1)[: int(n_time)]
+    tm = None
+    if isinstance(tmp_matrix, torch.Tensor) and tmp_matrix.dtype == torch.float64 \
+            and tmp_matrix.is_contiguous() \
+            and tuple(tmp_matrix.shape) == (int(n_resonators), t.numel()):
+        tm = tmp_matrix
+    scale = -charge * e * beam_n_macroparticles * ratio
+    v, ws = resonator_induced_voltage(n_macroparticles, bc, bin_size,
+                                      beam_n_macroparticles, t, R, omega_r, Q,
+                                      scale, tmp_matrix=tm)
+    if isinstance(kappa1, torch.Tensor) and kappa1.numel() == bc.numel() - 1:
+        n_res = np.asarray(R).size
+        off = n_res * bc.numel() * 16
+        kappa1.copy_(ws[off: off + 8 * (bc.numel() - 1)].view(torch.float64))
+    if isinstance(deltaT, torch.Tensor) and tuple(deltaT.shape) == (t.numel(), bc.numel()):
+        torch.sub(t[:, None], bc[None, :], out=deltaT)
+    dtype = torch.float32 if np.dtype(float_precision) == np.float32 else torch.float64
+    v = v.to(dtype)
+    if isinstance(induced_voltage, torch.Tensor) and induced_voltage.shape == v.shape \
+            and induced_voltage.dtype == dtype:
+        induced_voltage.copy_(v)
+        v = induced_voltage
+    return v, deltaT
+
+
 class B200Backend:
     """The hot-path subset of blond's MasterBackend attribute contract
     (bmath_backends.py:61-201), backed by libblond_b200.  See
@@ -253,6 +362,8 @@ class B200Backend:
         self.rfft = rfft
         self.irfft = irfft
         self.rfftfreq = rfftfreq
+        self.interp = interp
+        self.resonator_induced_voltage_1_turn = resonator_induced_voltage_1_turn
 
     def use_precision(self, p: str = "double"):
         use_precision(p)

@@ -197,6 +197,10 @@ class FusedTracker:
                 continue
             if not isinstance(obj, (InducedVoltageFreq, InducedVoltageTime)):
                 raise NotImplementedError(type(obj).__name__)
+            if getattr(obj, "multi_turn_wake", False):
+                raise NotImplementedError(
+                    "multi-turn wakes: track with TotalInducedVoltage and "
+                    "RingAndRFTracker instead of the fused engine")
             if n_fft is not None and obj.n_fft != n_fft:
                 raise NotImplementedError("contributions with different n_fft")
             n_fft = obj.n_fft

@@ -145,6 +145,50 @@ int blond_induced_voltage_f64(const double* profile, int n_slices,
                               double scale, double* v_out, int64_t n_out,
                               void* stream);
 
+/* ------------------------------------------------------------ time-domain wakes
+ * Analytic resonator convolution of InducedVoltageResonator: replaces
+ * resonator_induced_voltage_1_turn() utils/butils_wrap_python.py:656-790
+ * (called from InducedVoltageResonator.induced_voltage_1turn,
+ * impedances/impedance.py:1286-1315).  For each time_array[j]:
+ *   tmp_matrix[r][j] = R_S[r] / (2 omega_R[r] Q[r])
+ *                      * sum_k kappa_k (F_r(t_j - bc_{k+1}) - F_r(t_j - bc_k)),
+ *   induced_voltage[j] = scale * sum_r tmp_matrix[r][j],
+ * kappa_k = (n_macroparticles[k+1] - n_macroparticles[k])
+ *           / (bc_{k+1} - bc_k) / (beam_n_macroparticles * bin_size),
+ * F_r as the reference defines it, scale = -charge * e * beam_n_macroparticles
+ * * ratio.  The sum is evaluated by a recurrence over the bins in O(n_slices)
+ * per resonator plus O(log n_slices) per time point, which needs the
+ * n_slices bin_centers strictly increasing (a Profile's always are) and
+ * agrees with the reference's O(n_time * n_slices) sum to rounding: about
+ * 1e-13 of max|V| inside the slicing window, and within the reference's own
+ * phase rounding (a * t_j in double) beyond it.
+ *   - n_macroparticles, bin_centers, time_array, induced_voltage (n_time),
+ *     tmp_matrix (n_resonators x n_time, row-major; may be NULL) and
+ *     workspace are device arrays; R_S, omega_R and Q are HOST arrays.
+ *   - workspace holds blond_resonator_workspace_bytes(n_slices,
+ *     n_resonators) bytes, 16-byte aligned; the outputs must not overlap it.
+ *   - 1 <= n_resonators <= BLOND_MAX_RESONATORS, 1 <= n_slices <= 2^24,
+ *     Q >= 0.5 (the reference's constructor raises for Q < 0.5,
+ *     impedance.py:1127-1129) and omega_R > 0, else an error code. */
+#define BLOND_MAX_RESONATORS 64
+int64_t blond_resonator_workspace_bytes(int n_slices, int n_resonators);
+int blond_resonator_induced_voltage_f64(
+    const double* n_macroparticles, const double* bin_centers, int n_slices,
+    double bin_size, double beam_n_macroparticles, const double* time_array,
+    int64_t n_time, const double* R_S, const double* omega_R, const double* Q,
+    int n_resonators, double scale, double* induced_voltage, double* tmp_matrix,
+    void* workspace, int64_t workspace_bytes, void* stream);
+
+/* numpy.interp(x + x_shift, xp, fp, left, right) on the device: bm.interp
+ * (utils/bmath_backends.py:373) as _InducedVoltage.shift_trev_time uses it
+ * for the multi-turn-wake memory (impedances/impedance.py:533-550).  flags
+ * bit 0: use `left` below xp[0] (else fp[0]); bit 1: use `right` above
+ * xp[m-1] (else fp[m-1]).  xp increasing; x, xp, fp, out device arrays; out
+ * must not overlap xp or fp.  Bit-identical to numpy's loop (no FMA). */
+int blond_interp_f64(const double* x, int64_t n, double x_shift,
+                     const double* xp, const double* fp, int m, double left,
+                     double right, int flags, double* out, void* stream);
+
 /* ------------------------------------------------------------ fused turn engine
  * One object per beam.  A turn is, in the order of the reference main loop
  * [TotalInducedVoltage, RingAndRFTracker, Profile]

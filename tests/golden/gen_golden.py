@@ -25,6 +25,15 @@ track_*.npz           multi-turn runs of the reference objects
                       (RingAndRFTracker, Profile, TotalInducedVoltage).
 induced_*.npz         one-turn induced voltages (Freq, Time, Inductive).
 nfft_known.npz        n_fft / n_induced_voltage known answers.
+wakes_resonator.npz   resonator_induced_voltage_1_turn (butils_wrap_python.py:
+                      656-790) on seeded profiles, windows, times and modes.
+mtw_resonator.npz     the reference's own multi-turn-wake resonator test
+                      (unittests/impedances/test_impedance.py:127-187): its
+                      stored expectation mtw_resonator_induced_voltage.npy
+                      and the same run repeated here, with the time array.
+mtw_tracks.npz        multi-turn wakes in mtw_mode 'time' (InducedVoltageFreq,
+                      InducedVoltageTime) tracked over several turns.
+profile_fits.npz      Profile fit options 'gaussian', 'rms', 'fwhm'.
 """
 from __future__ import annotations
 
@@ -48,6 +57,7 @@ from blond.beam.distributions import bigaussian  # noqa: E402
 from blond.beam.profile import (CutOptions, FitOptions, Profile,  # noqa: E402
                                 OtherSlicesOptions)
 from blond.impedances.impedance import (InducedVoltageFreq,  # noqa: E402
+                                        InducedVoltageResonator,
                                         InducedVoltageTime,
                                         InductiveImpedance,
                                         TotalInducedVoltage)
@@ -342,6 +352,160 @@ def gen_nfft():
                                        for t in targets]))
 
 
+# --------------------------------------------------------------------------
+# 6. time-domain wakes: resonator convolution, multi-turn wakes, fits
+# --------------------------------------------------------------------------
+def gen_wakes_resonator():
+    from blond.utils.butils_wrap_python import resonator_induced_voltage_1_turn
+    rng = np.random.default_rng(2024)
+    out = {}
+    cases = [
+        # name, n_slices, bin_size, modes (R, f_r, Q), times
+        ("narrow", 512, 1.5e-12, ([1.19e10], [1.2973e9], [0.696e6]), "mtw3"),
+        ("two", 256, 2.5e-11, ([5e6, 1e6], [1e9, 3e9], [1.0, 30.0]), "window"),
+        ("lowq", 300, 1e-11, ([1e6], [5e9], [0.6]), "outside"),
+        ("many", 128, 5e-11, ([1e5, 3e4, 1e4, 2e3], [200e6, 800e6, 1.4e9, 2.1e9],
+                              [100.0, 3000.0, 30000.0, 2.0]), "window"),
+    ]
+    for name, S, bs, (R, fr, Q), kind in cases:
+        edges = np.linspace(0.0, S * bs, S + 1)
+        bc = (edges[1:] + edges[:-1]) / 2
+        n_mp = 200000
+        x = rng.normal(0.5 * S * bs, 0.12 * S * bs, n_mp)
+        prof = np.histogram(x, S, (0.0, S * bs))[0].astype(np.float64)
+        if kind == "mtw3":
+            t = np.concatenate([2e-5 * k + np.linspace(bc[0], bc[-1], S)
+                                for k in range(3)])
+        elif kind == "outside":
+            t = np.concatenate([bc, bc[0] - 20 * bs + np.arange(3 * S) * 0.37 * bs])
+        else:
+            t = bc.copy()
+        R = np.array(R, float)
+        om = 2 * np.pi * np.array(fr, float)
+        Q = np.array(Q, float)
+        Qt = Q * np.sqrt(1.0 - 1.0 / (4.0 * Q ** 2.0))
+        nt = len(t)
+        v, _ = resonator_induced_voltage_1_turn(
+            np.zeros(S - 1), prof, bc, bs, nt, np.zeros((nt, S)), t,
+            om * Qt / Q, om / (2.0 * Q), Qt, len(R), om, Q,
+            np.ones((len(R), nt)), 1.0, n_mp, 1e11 / n_mp, R, np.zeros(nt),
+            np.float64)
+        for k, a in dict(profile=prof, bin_centers=bc, bin_size=np.array([bs]),
+                         n_macroparticles=np.array([n_mp]), time=t, R=R,
+                         omega_r=om, Q=Q, ratio=np.array([1e11 / n_mp]),
+                         voltage=v).items():
+            out[f"{name}_{k}"] = a
+    out["names"] = np.array([c[0] for c in cases])
+    save("wakes_resonator.npz", **out)
+
+
+def gen_mtw_resonator():
+    import importlib.util
+    path = os.path.join(REF, "unittests/impedances/test_impedance.py")
+    spec = importlib.util.spec_from_file_location("ref_impedance_test", path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    case = mod.TestInducedVoltageResonatorMultiTurnWake()
+    case.setUp()
+    ivr = InducedVoltageResonator(beam=case.beam, profile=case.profile,
+                                  multi_turn_wake=True, resonators=case.resonator,
+                                  rf_station=case.rf_station,
+                                  time_decay_factor=0.00001)
+    tiv = TotalInducedVoltage(beam=case.beam, profile=case.profile,
+                              induced_voltage_list=[ivr])
+    tracker = RingAndRFTracker(rf_station=case.rf_station, beam=case.beam,
+                               profile=case.profile, total_induced_voltage=tiv,
+                               interpolation=True)
+    time_array = ivr.time_array.copy()
+    volts, full, dts, dEs = [], [], [], []
+    for _ in range(case.n_turns):
+        tiv.induced_voltage_sum()
+        full.append(ivr.induced_voltage.copy())
+        tracker.track()
+        volts.append(tiv.induced_voltage.copy())
+        dts.append(case.beam.dt.copy())
+        dEs.append(case.beam.dE.copy())
+    expected = np.load(os.path.join(
+        REF, "unittests/impedances/data/mtw_resonator_induced_voltage.npy"))
+    np.testing.assert_allclose(np.array(volts), expected, rtol=1e-5, atol=1e-1)
+    save("mtw_resonator.npz", expected=expected, rerun=np.array(volts),
+         full=np.array(full), time_array=time_array,
+         n_mtw_memory=np.array([ivr.n_mtw_memory]),
+         profile=case.profile.n_macroparticles.copy(),
+         bin_centers=case.profile.bin_centers.copy(),
+         fit=np.asarray(case.profile.fit_extra_options, float),
+         t_rev=case.ring.t_rev.copy(), phi_s=case.rf_station.phi_s.copy(),
+         omega_rf=case.rf_station.omega_rf[:, :2].copy(),
+         dt=np.array(dts), dE=np.array(dEs))
+
+
+def _small_ring_mtw(kind, n_turns=6, n=5000, S=64, seed=3):
+    """A 30 m ring (t_rev ~ 100 ns) whose wake memory spans three turns."""
+    ring = Ring(30.0, 0.02, 2e9, Proton(), n_turns)
+    rf = RFStation(ring, [4], [20e3], [0.0], n_rf=1)
+    beam = Beam(ring, n, 5e11)
+    bigaussian(ring, rf, beam, 2e-9, seed=seed)
+    dt0, dE0 = beam.dt.copy(), beam.dE.copy()
+    t_rf = rf.t_rf[0, 0]
+    profile = Profile(beam, CutOptions(cut_left=0.0, cut_right=t_rf, n_slices=S))
+    src = Resonators([2e4], [4.2 * 4 / ring.t_rev[0]], [60.0])
+    wake = 3 * ring.t_rev[0]
+    if kind == "freq":
+        iv = InducedVoltageFreq(beam, profile, [src],
+                                frequency_resolution=1 / wake,
+                                multi_turn_wake=True, rf_station=rf,
+                                mtw_mode="time")
+    else:
+        iv = InducedVoltageTime(beam, profile, [src], wake_length=wake,
+                                multi_turn_wake=True, rf_station=rf,
+                                mtw_mode="time")
+    tiv = TotalInducedVoltage(beam, profile, [iv])
+    tracker = RingAndRFTracker(rf, beam)
+    vinds, mems, profiles = [], [], [profile.n_macroparticles.copy()]
+    for _ in range(n_turns):
+        tiv.track()
+        vinds.append(tiv.induced_voltage.copy())
+        mems.append(iv.mtw_memory.copy())
+        tracker.track()
+        profile.track()
+        profiles.append(profile.n_macroparticles.copy())
+    return dict(dt0=dt0, dE0=dE0, dt=beam.dt.copy(), dE=beam.dE.copy(),
+                vind=np.array(vinds), memory=np.array(mems),
+                profiles=np.array(profiles), n_fft=np.array([iv.n_fft]),
+                n_induced_voltage=np.array([iv.n_induced_voltage]),
+                time_mtw=iv.time_mtw, t_rev=ring.t_rev.copy(),
+                cuts=np.array([profile.cut_left, profile.cut_right]))
+
+
+def gen_mtw_tracks():
+    out = {}
+    for kind in ("freq", "time"):
+        for k, a in _small_ring_mtw(kind).items():
+            out[f"{kind}_{k}"] = a
+    save("mtw_tracks.npz", **out)
+
+
+def gen_profile_fits():
+    ring, rf = c1_machine(10)
+    beam = Beam(ring, 20000, 1e10)
+    bigaussian(ring, rf, beam, 0.4e-9, seed=7)
+    cl, cr = _window(rf)
+    out = dict(dt=beam.dt.copy(), cuts=np.array([cl, cr]), n_slices=np.array([200]))
+    out["bin_centers"] = Profile(beam, CutOptions(cut_left=cl, cut_right=cr,
+                                                  n_slices=200)).bin_centers.copy()
+    for opt in ("gaussian", "rms", "fwhm"):
+        p = Profile(beam, CutOptions(cut_left=cl, cut_right=cr, n_slices=200),
+                    FitOptions(fit_option=opt))
+        out[f"{opt}_position"] = np.array([p.bunchPosition])
+        out[f"{opt}_length"] = np.array([p.bunchLength])
+        if opt == "gaussian":
+            out["gaussian_params"] = np.asarray(p.fit_extra_options, float)
+            out["p0"] = np.array([p.n_macroparticles.max(), beam.dt.mean(),
+                                  beam.dt.std()])
+        out["profile"] = p.n_macroparticles.copy()
+    save("profile_fits.npz", **out)
+
+
 def run_reference_profile_test():
     """Run the reference's own profile unit test (its literal expected
     counts) against oracle/_ref before the fixture is trusted."""
@@ -364,3 +528,7 @@ if __name__ == "__main__":
     gen_machine()
     gen_tracks()
     gen_nfft()
+    gen_wakes_resonator()
+    gen_mtw_resonator()
+    gen_mtw_tracks()
+    gen_profile_fits()
