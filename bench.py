@@ -54,11 +54,12 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--kernel", default="auto", choices=["auto", "tma", "plain"])
-    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5"],
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5", "mtw"],
                     help="c2: the single-beam pipeline (default, the headline); "
                          "c3: 256-beam double-RF batch; c4: adjoint gradient; "
                          "c5: 1e8 particles, "
-                         "2^16 slices, 4 resonators + inductive Z/n")
+                         "2^16 slices, 4 resonators + inductive Z/n; "
+                         "mtw: one turn of InducedVoltageResonator's multi-turn wake")
     ap.add_argument("--beams", type=int, default=256)
     ap.add_argument("--tune", default="auto", choices=["auto", "fixed"],
                     help="fixed: no autotuner; --threads/--blocks-per-sm/--prefetch "
@@ -794,6 +795,181 @@ def run_c4(args):
     }
 
 
+MTW_WORKLOAD = ("InducedVoltageResonator multi-turn wake: 1e6 protons 26 GeV/c, "
+                "h=4620 4.5 MV, 1024 slices over 2.5 ns, 4 resonators (R 1e6/5e5/2e5/1e9 "
+                "Ohm, f_r 0.2/0.63/0.915/1.4 GHz, Q 150/500/3e4/5e7), "
+                "time_decay_factor 0.01")
+MTW_METRIC = "induced-voltage points x resonators per second"
+MTW_UNIT = "points*resonators/s"
+
+
+def build_mtw(n=1_000_000, S=1024):
+    from blond_b200.beam.beam import Beam
+    from blond_b200.beam.profile import CutOptions, Profile
+    from blond_b200.impedances.impedance import (InducedVoltageResonator,
+                                                 TotalInducedVoltage)
+    from blond_b200.impedances.impedance_sources import Resonators
+    ring, rf = machine(2000)
+    dt, dE, centre = host_bunch(ring, rf, n)
+    beam = Beam(ring, n, 1e11, dt=dt, dE=dE)
+    cl, cr, _ = window(centre, S)
+    prof = Profile(beam, CutOptions(cut_left=cl, cut_right=cr, n_slices=S))
+    res = Resonators([1e6, 5e5, 2e5, 1e9], [200e6, 630e6, 915e6, 1.4e9],
+                     [150.0, 500.0, 3e4, 5e7])
+    ivr = InducedVoltageResonator(beam, prof, res, multi_turn_wake=True, rf_station=rf,
+                                  time_decay_factor=0.01)
+    return beam, prof, res, ivr, TotalInducedVoltage(beam, prof, [ivr])
+
+
+def _timed_steps(step, K, flush):
+    """Sum of per-step CUDA-event times on the current stream, the L2
+    flushed (untimed) before every step."""
+    import torch
+    s = torch.cuda.current_stream()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(K)]
+    torch.cuda.synchronize()
+    for a, b in ev:
+        flush.zero_()
+        a.record(s)
+        step()
+        b.record(s)
+    torch.cuda.synchronize()
+    return sum(a.elapsed_time(b) for a, b in ev)
+
+
+def mtw_cpu_baseline(prof_host, bc, bin_size, N, t, res, ratio, seconds):
+    """The reference's time x bin evaluation (oracle restatement of
+    butils_wrap_python.py:656-790) on blocks of time points until
+    `seconds` have passed; points x resonators per second, 1 thread."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import wakes_oracle as wo
+    done, t0 = 0, time.perf_counter()
+    block = 512
+    while time.perf_counter() - t0 < seconds and done < len(t):
+        wo.resonator_induced_voltage(prof_host, bc, bin_size, N, t[done:done + block],
+                                     res.R_S, res.omega_R, res.Q, 1.0, ratio)
+        done += block
+    sec = time.perf_counter() - t0
+    return done * len(res.R_S) / sec, done
+
+
+def run_mtw(args):
+    import torch
+    from blond_b200 import bmath as bm
+    W, K = max(3, args.warmup), args.steps
+    beam, prof, res, ivr, tiv = build_mtw()
+    n_time, n_res, S = int(ivr.n_time), int(ivr.n_resonators), int(prof.n_slices)
+    units = n_time * n_res
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    for _ in range(W):
+        tiv.induced_voltage_sum()
+    clocks = ClockSampler(0)
+    ms = _timed_steps(tiv.induced_voltage_sum, K, flush)
+    clk = clocks.stop()
+    # the two kernels alone (scan + evaluation), same arguments as the class
+    from scipy.constants import e as e_charge
+    scale = -beam.particle.charge * e_charge * beam.n_macroparticles * beam.ratio
+
+    def kernels():
+        bm.resonator_induced_voltage(prof.n_macroparticles, ivr._bc_dev, prof.bin_size,
+                                     beam.n_macroparticles, ivr._time_dev, ivr.R,
+                                     ivr.omega_r, ivr.Q, scale,
+                                     tmp_matrix=ivr._tmp_matrix, workspace=ivr._workspace)
+    for _ in range(3):
+        kernels()
+    # replayed from a CUDA graph, so that the events bracket the two
+    # launches and not the host's argument marshalling
+    graph = torch.cuda.CUDAGraph()
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        kernels()
+        torch.cuda.synchronize()
+        with torch.cuda.graph(graph):
+            kernels()
+    torch.cuda.current_stream().wait_stream(side)
+    for _ in range(3):
+        graph.replay()
+    kms = _timed_steps(graph.replay, K, flush) / K
+    # bytes one launch pair must move: time array in, voltage and per-mode
+    # rows out, profile and bin centres in, the recurrence written and read
+    algo = 8 * n_time * (2 + n_res) + 16 * S + 2 * 16 * S * n_res + 8 * S
+    peak = _peaks().get("hbm_gbs") or 6650.0
+    ach = algo / (kms * 1e-3) / 1e9
+    # end to end: the profile from pinned host memory, the summed voltage back
+    hp = torch.empty(S, dtype=torch.float64, pin_memory=True)
+    hp.copy_(prof.n_macroparticles.cpu())
+    hv = torch.empty(S, dtype=torch.float64, pin_memory=True)
+    s = torch.cuda.current_stream()
+
+    def e2e_step():
+        prof.n_macroparticles.copy_(hp, non_blocking=True)
+        tiv.induced_voltage_sum()
+        hv.copy_(tiv.induced_voltage, non_blocking=True)
+    e_ms = _timed_steps(e2e_step, K, flush)
+    cpu_v, sample = (None, 0)
+    if not args.no_cpu_baseline:
+        cpu_v, sample = mtw_cpu_baseline(
+            prof.n_macroparticles.cpu().numpy(), np.asarray(prof.bin_centers), prof.bin_size,
+            beam.n_macroparticles, np.asarray(ivr.time_array), res, beam.ratio,
+            min(args.cpu_seconds, 12.0))
+    return {
+        "metric": MTW_METRIC, "value": units * K / (ms * 1e-3), "unit": MTW_UNIT,
+        "n_gpus": 1, "steps": K, "warmup": W, "ms_per_step": ms / K,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": MTW_WORKLOAD, "slices": S, "n_time": n_time,
+                   "resonators": n_res, "turns_of_memory": n_time // S,
+                   "l2": "flushed (256 MiB write) before every timed step"},
+        "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
+                     "frac": ach / peak, "traffic": None,
+                     "kernel": "resonator_scan_kernel + resonator_eval_kernel",
+                     "kernel_ms": kms, "algorithmic_bytes_per_launch": algo,
+                     "note": "the evaluation issues one FP64 sincos + exp per point and "
+                             "resonator; its bound is FP64 issue, not HBM"},
+        "cpu_baseline": None if cpu_v is None else {
+            "value": cpu_v, "unit": MTW_UNIT, "cores": 1, "kind": "port",
+            "sample": f"{sample} of the {n_time} time points, the reference's time x bin "
+                      "sum (numpy)"},
+        "e2e": {"value": units * K / (e_ms * 1e-3), "unit": MTW_UNIT,
+                "h2d_bytes_per_step": 8 * S, "d2h_bytes_per_step": 8 * S},
+        "gpu_launches": 2 * K,
+        "clocks": clk,
+    }
+
+
+def run_reference_mtw(args):
+    """The reference's InducedVoltageResonator arithmetic on the host (the
+    time x bin sum of butils_wrap_python.py:656-790, restated in numpy),
+    one bounded sample of time points per step."""
+    import torch
+    W, K = 0, max(1, min(args.steps, 3))
+    beam, prof, res, ivr, tiv = build_mtw()
+    n_time, n_res = int(ivr.n_time), int(ivr.n_resonators)
+    args_cpu = (prof.n_macroparticles.cpu().numpy(), np.asarray(prof.bin_centers),
+                prof.bin_size, beam.n_macroparticles, np.asarray(ivr.time_array), res,
+                beam.ratio)
+    del tiv, ivr
+    torch.cuda.empty_cache()
+    vals = [mtw_cpu_baseline(*args_cpu, min(args.cpu_seconds, 12.0) / K) for _ in range(K)]
+    v = float(np.mean([x[0] for x in vals]))
+    sample = vals[0][1]
+    return {
+        "impl": "reference", "metric": MTW_METRIC, "value": v, "unit": MTW_UNIT,
+        "n_gpus": 1, "steps": K, "warmup": W, "ms_per_step": n_time * n_res / v * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": MTW_WORKLOAD, "slices": int(prof.n_slices), "n_time": n_time,
+                   "resonators": n_res, "parallelism": "1 host thread (numpy)"},
+        "cpu_baseline": {"value": v, "unit": MTW_UNIT, "cores": 1, "kind": "port",
+                         "sample": f"{sample} time points per step, scaled to the full "
+                                   f"{n_time}"},
+        "e2e": {"value": v, "unit": MTW_UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+
+
 def main():
     args = parse()
     if args.workload == "c4" and args.impl == "ours":
@@ -801,6 +977,9 @@ def main():
         return
     if args.workload == "c5" and args.impl == "ours":
         print(json.dumps(run_c5(args)), flush=True)
+        return
+    if args.workload == "mtw" and args.impl == "ours":
+        print(json.dumps(run_mtw(args)), flush=True)
         return
     if args.workload == "c3" and args.impl == "ours":
         W, K = max(3, args.warmup), args.steps
@@ -845,6 +1024,9 @@ def main():
             return
         if args.workload == "c3":
             print(json.dumps(run_reference_c3(args)), flush=True)
+            return
+        if args.workload == "mtw":
+            print(json.dumps(run_reference_mtw(args)), flush=True)
             return
         print(json.dumps(run_reference(args, world, rank)), flush=True)
         return

@@ -114,6 +114,9 @@ _EXTRA = {
     "blond_resonator_induced_voltage_f64": [c_ptr, c_ptr, c_int, c_dbl, c_dbl, c_ptr,
                                             c_i64, c_ptr, c_ptr, c_ptr, c_int, c_dbl,
                                             c_ptr, c_ptr, c_ptr, c_i64, c_ptr],
+    "blond_resonator_mtw_f64": [c_ptr, c_ptr, c_int, c_dbl, c_dbl, c_ptr, c_i64,
+                                c_ptr, c_ptr, c_ptr, c_int, c_dbl, c_ptr, c_ptr, c_i64,
+                                c_i64, c_ptr, c_ptr, c_i64, c_ptr],
     "blond_interp_f64": [c_ptr, c_i64, c_dbl, c_ptr, c_ptr, c_int, c_dbl, c_dbl,
                          c_int, c_ptr, c_ptr],
 }

@@ -270,7 +270,7 @@ def resonator_workspace(n_slices: int, n_resonators: int, device=None):
 
 def resonator_induced_voltage(profile, bin_centers, bin_size, beam_n_macroparticles,
                               time_array, R, omega_r, Q, scale, out=None,
-                              tmp_matrix=None, workspace=None):
+                              tmp_matrix=None, workspace=None, memory_in=None, shift=0):
     """Induced voltage of resonators by the analytic convolution of the
     linearly interpolated line density (butils_wrap_python.py:656-790),
     float64, one value per time_array point.  ``bin_centers`` must be
@@ -278,7 +278,11 @@ def resonator_induced_voltage(profile, bin_centers, bin_size, beam_n_macropartic
     -charge * e * beam_n_macroparticles * ratio.  ``tmp_matrix`` (optional,
     n_resonators x n_time float64 tensor) receives the per-resonator rows;
     ``workspace`` (from resonator_workspace) may be reused across calls.
-    Returns (induced_voltage, workspace)."""
+    With ``memory_in`` (float64 device tensor of n_memory >= n_time points)
+    the result is instead the next multi-turn memory, memory_in moved
+    forward by ``shift`` points (zeros behind) plus the voltage on its first
+    n_time points (impedance.py:1317-1335), n_memory values.
+    Returns (induced_voltage or memory, workspace)."""
     p = as_device(profile, torch.float64).reshape(-1).contiguous()
     bc = as_device(bin_centers, torch.float64, p.device).reshape(-1).contiguous()
     t = as_device(time_array, torch.float64, p.device).reshape(-1).contiguous()
@@ -292,13 +296,25 @@ def resonator_induced_voltage(profile, bin_centers, bin_size, beam_n_macropartic
         raise ValueError("profile and bin_centers differ in length")
     if workspace is None:
         workspace = resonator_workspace(bc.numel(), n_res, p.device)
+    P = lambda a: a.ctypes.data_as(ct.c_void_p)  # noqa: E731
+    tm = _ptr(tmp_matrix) if tmp_matrix is not None else None
+    if memory_in is not None:
+        mem = memory_in
+        if mem.dtype != torch.float64 or not mem.is_contiguous():
+            raise ValueError("memory_in must be a contiguous float64 tensor")
+        if out is None:
+            out = torch.empty_like(mem)
+        _lib.call("blond_resonator_mtw_f64", _ptr(p), _ptr(bc), bc.numel(),
+                  float(bin_size), float(beam_n_macroparticles), _ptr(t), t.numel(),
+                  P(Rh), P(wh), P(qh), n_res, float(scale), _ptr(mem), _ptr(out),
+                  mem.numel(), int(shift), tm, _ptr(workspace), workspace.numel(),
+                  _stream())
+        return out, workspace
     if out is None:
         out = torch.empty(t.numel(), dtype=torch.float64, device=p.device)
-    P = lambda a: a.ctypes.data_as(ct.c_void_p)  # noqa: E731
     _lib.call("blond_resonator_induced_voltage_f64", _ptr(p), _ptr(bc), bc.numel(),
               float(bin_size), float(beam_n_macroparticles), _ptr(t), t.numel(),
-              P(Rh), P(wh), P(qh), n_res, float(scale), _ptr(out),
-              _ptr(tmp_matrix) if tmp_matrix is not None else None,
+              P(Rh), P(wh), P(qh), n_res, float(scale), _ptr(out), tm,
               _ptr(workspace), workspace.numel(), _stream())
     return out, workspace
 

@@ -31,7 +31,8 @@
 namespace bb {
 namespace {
 
-constexpr int kScanThreads = 1024;
+constexpr int kScanThreads = 512;
+constexpr int kScanCache = 4;  // elements a scan thread keeps in registers
 constexpr int kEvalThreads = 256;
 
 struct cplx {
@@ -40,29 +41,33 @@ struct cplx {
 
 // Per-resonator constants, passed by value (impedance.py:1218-1220):
 // qt = Q sqrt(1 - 1/(4 Q^2)), a = w qt / Q, b = w / (2 Q), coef = R / (2 w Q).
+// a_pi = a / pi feeds sincospi, whose argument reduction is exact and cheap
+// at any magnitude (a t reaches 1e7 rad over a long multi-turn memory).
 struct ResonatorParams {
     int n;
     double qt[BLOND_MAX_RESONATORS], a[BLOND_MAX_RESONATORS], b[BLOND_MAX_RESONATORS],
-        coef[BLOND_MAX_RESONATORS];
+        coef[BLOND_MAX_RESONATORS], a_pi[BLOND_MAX_RESONATORS];
 };
 __device__ __forceinline__ cplx cmul(cplx a, cplx b) {
     return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
 }
 __device__ __forceinline__ cplx cadd(cplx a, cplx b) { return {a.re + b.re, a.im + b.im}; }
-// e^{x + iy}
-__device__ __forceinline__ cplx cexp(double x, double y) {
+// e^{x + i pi y}
+__device__ __forceinline__ cplx cexp_pi(double x, double y) {
     double s, c;
-    sincos(y, &s, &c);
+    sincospi(y, &s, &c);
     const double m = exp(x);
     return {m * c, m * s};
 }
-// e^{x + iy} - 1 without cancellation for small |x + iy|:
-// Re = expm1(x) cos y - 2 sin^2(y/2), Im = e^x sin y.
+// e^{x + iy} - 1 without cancellation for small |x + iy|, from one sincos
+// of y/2 (s, c) and expm1(x) = m:
+// Re = m cos y - 2 s^2 with cos y = 1 - 2 s^2, Im = (m + 1) 2 s c.
 __device__ __forceinline__ cplx cexpm1(double x, double y) {
     double s, c;
-    sincos(y, &s, &c);
-    const double sh = sin(0.5 * y);
-    return {expm1(x) * c - 2.0 * sh * sh, exp(x) * s};
+    sincos(0.5 * y, &s, &c);
+    const double m = expm1(x);
+    const double s2 = 2.0 * s * s;
+    return {m * (1.0 - s2) - s2, (m + 1.0) * (2.0 * s * c)};
 }
 __device__ __forceinline__ cplx shfl_up(cplx v, int d) {
     return {__shfl_up_sync(0xffffffffu, v.re, d), __shfl_up_sync(0xffffffffu, v.im, d)};
@@ -85,12 +90,31 @@ __device__ __forceinline__ double kappa_at(const double* prof, const double* bc,
     return div_rn(div_rn(sub_rn(prof[k + 1], prof[k]), sub_rn(bc[k + 1], bc[k])), nb);
 }
 
+// Element i of the recurrence, J_i = lam J_{i-1} + add.
+struct Elem {
+    cplx lam, add;
+};
+__device__ __forceinline__ Elem scan_elem(const double* prof, const double* bc, int S, int i,
+                                          double nb, double a, double b) {
+    const double h = bc[i] - bc[i - 1];
+    const cplx em1 = cexpm1(-b * h, a * h);
+    const double kp = kappa_at(prof, bc, S, i - 1, nb);
+    return {{em1.re + 1.0, em1.im}, {-kp * em1.re, -kp * em1.im}};
+}
+__device__ __forceinline__ cplx apply(const Elem& e, cplx J) {
+    return {e.lam.re * J.re - e.lam.im * J.im + e.add.re,
+            e.lam.re * J.im + e.lam.im * J.re + e.add.im};
+}
+
 // One block per resonator: J_i for i in [0, S) into J[r * S + i], and
-// (block 0) kappa_k for k in [0, S) into kappa.
-__global__ void __launch_bounds__(kScanThreads)
+// (block 0) kappa_k for k in [0, S) into kappa.  Each thread takes a
+// contiguous segment of elements; the first kScanCache stay in registers
+// between the two passes, the rest are recomputed.
+__global__ void __launch_bounds__(kScanThreads, 1)
 resonator_scan_kernel(const double* __restrict__ prof, const double* __restrict__ bc,
                       int S, double nb, ResonatorParams rp, double* __restrict__ kappa,
                       double2* __restrict__ J) {
+    constexpr int kWarps = kScanThreads / 32;
     const int r = blockIdx.x;
     const int t = threadIdx.x;
     const int lane = t & 31, warp = t >> 5;
@@ -103,22 +127,26 @@ resonator_scan_kernel(const double* __restrict__ prof, const double* __restrict_
     if (r == 0)
         for (int k = t; k < S; k += kScanThreads) kappa[k] = kappa_at(prof, bc, S, k, nb);
 
-    // pass 1: this thread's segment as one affine map
+    // pass 1: this thread's segment as one affine map J -> A J + B
+    Elem cache[kScanCache];
     cplx A = {1.0, 0.0}, B = {0.0, 0.0};
-    for (int i = lo; i < hi; ++i) {
-        const double h = bc[i] - bc[i - 1];
-        const cplx em1 = cexpm1(-b * h, a * h);
-        const cplx lam = {em1.re + 1.0, em1.im};
-        const double kp = kappa_at(prof, bc, S, i - 1, nb);
-        const cplx nA = cmul(lam, A);
-        const cplx nB = {lam.re * B.re - lam.im * B.im - kp * em1.re,
-                         lam.re * B.im + lam.im * B.re - kp * em1.im};
-        A = nA;
-        B = nB;
+#pragma unroll
+    for (int q = 0; q < kScanCache; ++q) {
+        const int i = lo + q;
+        if (i < hi) {
+            cache[q] = scan_elem(prof, bc, S, i, nb, a, b);
+            A = cmul(cache[q].lam, A);
+            B = apply(cache[q], B);
+        }
+    }
+    for (int i = lo + kScanCache; i < hi; ++i) {
+        const Elem e = scan_elem(prof, bc, S, i, nb, a, b);
+        A = cmul(e.lam, A);
+        B = apply(e, B);
     }
 
     // inclusive warp scan, then over warp totals
-    __shared__ cplx sA[32], sB[32];
+    __shared__ cplx sA[kWarps], sB[kWarps];
     for (int d = 1; d < 32; d <<= 1) {
         const cplx Ae = shfl_up(A, d), Be = shfl_up(B, d);
         if (lane >= d) compose(A, B, Ae, Be);
@@ -129,13 +157,19 @@ resonator_scan_kernel(const double* __restrict__ prof, const double* __restrict_
     }
     __syncthreads();
     if (warp == 0) {
-        cplx wA = sA[lane], wB = sB[lane];  // kScanThreads / 32 == 32 warps
-        for (int d = 1; d < 32; d <<= 1) {
+        cplx wA = {1.0, 0.0}, wB = {0.0, 0.0};
+        if (lane < kWarps) {
+            wA = sA[lane];
+            wB = sB[lane];
+        }
+        for (int d = 1; d < kWarps; d <<= 1) {
             const cplx Ae = shfl_up(wA, d), Be = shfl_up(wB, d);
             if (lane >= d) compose(wA, wB, Ae, Be);
         }
-        sA[lane] = wA;
-        sB[lane] = wB;
+        if (lane < kWarps) {
+            sA[lane] = wA;
+            sB[lane] = wB;
+        }
     }
     __syncthreads();
     // exclusive prefix of this thread = (inclusive of lane-1) o (warps before)
@@ -150,19 +184,23 @@ resonator_scan_kernel(const double* __restrict__ prof, const double* __restrict_
     cplx Jc = eB;
     double2* Jr = J + (size_t)r * S;
     if (t == 0) Jr[0] = make_double2(0.0, 0.0);
-    for (int i = lo; i < hi; ++i) {
-        const double h = bc[i] - bc[i - 1];
-        const cplx em1 = cexpm1(-b * h, a * h);
-        const cplx lam = {em1.re + 1.0, em1.im};
-        const double kp = kappa_at(prof, bc, S, i - 1, nb);
-        Jc = {lam.re * Jc.re - lam.im * Jc.im - kp * em1.re,
-              lam.re * Jc.im + lam.im * Jc.re - kp * em1.im};
+#pragma unroll
+    for (int q = 0; q < kScanCache; ++q) {
+        const int i = lo + q;
+        if (i < hi) {
+            Jc = apply(cache[q], Jc);
+            Jr[i] = make_double2(Jc.re, Jc.im);
+        }
+    }
+    for (int i = lo + kScanCache; i < hi; ++i) {
+        Jc = apply(scan_elem(prof, bc, S, i, nb, a, b), Jc);
         Jr[i] = make_double2(Jc.re, Jc.im);
     }
 }
 
 // #{k : bc_k < x} over increasing bc.
-__device__ __forceinline__ int count_below(const double* __restrict__ bc, int S, double x) {
+__device__ __forceinline__ int count_below_search(const double* __restrict__ bc, int S,
+                                                  double x) {
     int lo = 0, hi = S;
     while (lo < hi) {
         const int mid = (lo + hi) >> 1;
@@ -174,39 +212,90 @@ __device__ __forceinline__ int count_below(const double* __restrict__ bc, int S,
     return lo;
 }
 
+// The same from the evenly spaced estimate (x - bc_0) / mean spacing,
+// corrected by a short walk; the binary search when the walk is long
+// (uneven bins).  Exact for any increasing bc.
+__device__ __forceinline__ int count_below(const double* __restrict__ bc, int S, double x,
+                                           double bc0, double inv_h) {
+    double f = ceil((x - bc0) * inv_h);
+    f = fmin(fmax(f, 0.0), (double)S);
+    int m = (int)f;
+    for (int it = 0; it < 4; ++it) {
+        if (m < S && bc[m] < x) {
+            ++m;
+        } else if (m > 0 && !(bc[m - 1] < x)) {
+            --m;
+        } else {
+            return m;
+        }
+    }
+    return count_below_search(bc, S, x);
+}
+
+// G = 2^log_g lanes per output point (G >= n_resonators up to 32), lane
+// q of a group taking modes q, q + G, ...; the group sums its modes with
+// shuffles.  MTW = false: out[j] = V_j for j < n_time.  MTW = true
+// (InducedVoltageResonator.induced_voltage_mtw, impedance.py:1317-1335):
+// out is the new memory of n_out points,
+//     out[j] = mem_in[j + shift] (0 past its end) + V_j (j < n_time),
+// the reference's append-zeros / drop-one-window / add in one pass.
+template <bool MTW>
 __global__ void __launch_bounds__(kEvalThreads)
 resonator_eval_kernel(const double* __restrict__ time_array, int64_t n_time,
                       const double* __restrict__ bc, int S,
                       const double* __restrict__ kappa, const double2* __restrict__ J,
-                      ResonatorParams rp, double scale, double* __restrict__ out,
+                      ResonatorParams rp, int log_g, double scale, double* __restrict__ out,
+                      int64_t n_out, const double* __restrict__ mem_in, int64_t shift,
                       double* __restrict__ per_resonator) {
-    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n_time;
-         j += (int64_t)gridDim.x * blockDim.x) {
-        const double tj = time_array[j];
-        if (tj != tj) {  // NaN time: the reference's sum is NaN too
-            out[j] = tj;
-            if (per_resonator)
-                for (int r = 0; r < rp.n; ++r) per_resonator[(size_t)r * n_time + j] = tj;
-            continue;
-        }
-        const int m = count_below(bc, S, tj);
-        const int i = m - 1;
-        const double kp = m > 0 ? kappa[i] : 0.0;
-        const double d = m > 0 ? tj - bc[i] : 0.0;
+    const double bc0 = bc[0];
+    const double inv_h = S > 1 ? (double)(S - 1) / (bc[S - 1] - bc0) : 0.0;
+    const int G = 1 << log_g;
+    const int q = threadIdx.x & (G - 1);
+    const int64_t total = n_out << log_g;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    // every lane of a warp runs the same iterations (the shuffles need them)
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < total; base += stride) {
+        const int64_t g = base + threadIdx.x;
+        const int64_t j = g >> log_g;
+        const bool active = g < total;
         double sum = 0.0;
-        for (int r = 0; r < rp.n; ++r) {
-            double v = 0.0;
-            if (m > 0) {
-                const double2 Ji = J[(size_t)r * S + i];
-                const cplx E = cexp(-rp.b[r] * d, rp.a[r] * d);
-                const cplx O = cmul(E, {Ji.x - kp, Ji.y});
-                v = (2.0 * O.re + O.im / rp.qt[r]) + 2.0 * kp;
+        bool nan_t = false;
+        if (active && j < n_time) {
+            const double tj = time_array[j];
+            if (tj != tj) {  // NaN time: the reference's sum is NaN too
+                nan_t = true;
+                sum = tj;
+                if (per_resonator)
+                    for (int r = q; r < rp.n; r += G) per_resonator[(size_t)r * n_time + j] = tj;
+            } else {
+                const int m = count_below(bc, S, tj, bc0, inv_h);
+                const int i = m - 1;
+                const double kp = m > 0 ? kappa[i] : 0.0;
+                const double d = m > 0 ? tj - bc[i] : 0.0;
+                for (int r = q; r < rp.n; r += G) {
+                    double v = 0.0;
+                    if (m > 0) {
+                        const double2 Ji = J[(size_t)r * S + i];
+                        const cplx E = cexp_pi(-rp.b[r] * d, rp.a_pi[r] * d);
+                        const cplx O = cmul(E, {Ji.x - kp, Ji.y});
+                        v = (2.0 * O.re + O.im / rp.qt[r]) + 2.0 * kp;
+                    }
+                    const double tr = rp.coef[r] * v;
+                    if (per_resonator) per_resonator[(size_t)r * n_time + j] = tr;
+                    sum += tr;
+                }
             }
-            const double tr = rp.coef[r] * v;
-            if (per_resonator) per_resonator[(size_t)r * n_time + j] = tr;
-            sum += tr;
         }
-        out[j] = sum * scale;
+        for (int w = 1; w < G; w <<= 1) sum += __shfl_xor_sync(0xffffffffu, sum, w);
+        if (!active || q != 0) continue;
+        const double v_total = j < n_time ? (nan_t ? sum : sum * scale) : 0.0;
+        if (MTW) {
+            const int64_t src = j + shift;
+            const double old = src < n_out ? mem_in[src] : 0.0;
+            out[j] = j < n_time ? old + v_total : old;
+        } else {
+            out[j] = v_total;
+        }
     }
 }
 
@@ -282,15 +371,15 @@ int64_t blond_resonator_workspace_bytes(int n_slices, int n_resonators) {
     return (int64_t)n_resonators * n_slices * 16 + (int64_t)n_slices * 8;
 }
 
-int blond_resonator_induced_voltage_f64(
-    const double* n_macroparticles, const double* bin_centers, int n_slices,
-    double bin_size, double beam_n_macroparticles, const double* time_array,
-    int64_t n_time, const double* R_S, const double* omega_R, const double* Q,
-    int n_resonators, double scale, double* induced_voltage, double* tmp_matrix,
-    void* workspace, int64_t workspace_bytes, void* stream) {
-    clear_error();
-    BB_CHECK_ARG(n_macroparticles && bin_centers && time_array && R_S && omega_R && Q &&
-                     induced_voltage && workspace,
+static int resonator_launch(const double* n_macroparticles, const double* bin_centers,
+                            int n_slices, double bin_size, double beam_n_macroparticles,
+                            const double* time_array, int64_t n_time, const double* R_S,
+                            const double* omega_R, const double* Q, int n_resonators,
+                            double scale, double* out, int64_t n_out, const double* mem_in,
+                            int64_t shift, double* tmp_matrix, void* workspace,
+                            int64_t workspace_bytes, void* stream) {
+    BB_CHECK_ARG(n_macroparticles && bin_centers && time_array && R_S && omega_R && Q && out &&
+                     workspace,
                  "resonator_induced_voltage: null pointer");
     BB_CHECK_SIZE(n_slices >= 1 && n_slices <= (1 << 24),
                   "resonator_induced_voltage: n_slices %d outside [1, 2^24]", n_slices);
@@ -303,16 +392,16 @@ int blond_resonator_induced_voltage_f64(
                  (long long)workspace_bytes,
                  (long long)blond_resonator_workspace_bytes(n_slices, n_resonators));
     BB_CHECK_ARG(aligned(workspace, 16) && aligned(n_macroparticles, 8) &&
-                     aligned(bin_centers, 8) && aligned(time_array, 8) &&
-                     aligned(induced_voltage, 8) && (!tmp_matrix || aligned(tmp_matrix, 8)),
+                     aligned(bin_centers, 8) && aligned(time_array, 8) && aligned(out, 8) &&
+                     (!tmp_matrix || aligned(tmp_matrix, 8)) && (!mem_in || aligned(mem_in, 8)),
                  "resonator_induced_voltage: misaligned array");
-    const size_t nt = (size_t)n_time * 8;
-    BB_CHECK_ARG(!overlaps(induced_voltage, nt, workspace, (size_t)workspace_bytes) &&
-                     (!tmp_matrix ||
-                      (!overlaps(tmp_matrix, nt * n_resonators, workspace,
-                                 (size_t)workspace_bytes) &&
-                       !overlaps(tmp_matrix, nt * n_resonators, induced_voltage, nt))),
-                 "resonator_induced_voltage: output overlaps the workspace");
+    const size_t no = (size_t)n_out * 8, nt = (size_t)n_time * 8;
+    const size_t nw = (size_t)workspace_bytes;
+    BB_CHECK_ARG(!overlaps(out, no, workspace, nw) &&
+                     (!mem_in || !overlaps(out, no, mem_in, no)) &&
+                     (!tmp_matrix || (!overlaps(tmp_matrix, nt * n_resonators, workspace, nw) &&
+                                      !overlaps(tmp_matrix, nt * n_resonators, out, no))),
+                 "resonator_induced_voltage: an output overlaps an input or the workspace");
 
     // Resonator constants in the reference's operation order
     // (impedance.py:1218-1220, butils_wrap_python.py:777-781).
@@ -326,6 +415,7 @@ int blond_resonator_induced_voltage_f64(
         const double qt = Q[r] * sqrt(1.0 - 1.0 / (4.0 * (Q[r] * Q[r])));
         rp.qt[r] = qt;
         rp.a[r] = omega_R[r] * qt / Q[r];
+        rp.a_pi[r] = rp.a[r] / M_PI;
         rp.b[r] = omega_R[r] / (2.0 * Q[r]);
         rp.coef[r] = R_S[r] / (2.0 * omega_R[r] * Q[r]);
     }
@@ -336,13 +426,53 @@ int blond_resonator_induced_voltage_f64(
     resonator_scan_kernel<<<n_resonators, kScanThreads, 0, s>>>(
         n_macroparticles, bin_centers, n_slices, nb, rp, kappa, J);
     BB_LAUNCH_CHECK();
-    if (n_time > 0) {
-        resonator_eval_kernel<<<eval_grid(n_time), kEvalThreads, 0, s>>>(
-            time_array, n_time, bin_centers, n_slices, kappa, J, rp, scale, induced_voltage,
-            tmp_matrix);
+    if (n_out > 0) {
+        int log_g = 0;
+        while ((1 << log_g) < n_resonators && log_g < 5) ++log_g;
+        const int grid = eval_grid(n_out << log_g);
+        if (mem_in)
+            resonator_eval_kernel<true><<<grid, kEvalThreads, 0, s>>>(
+                time_array, n_time, bin_centers, n_slices, kappa, J, rp, log_g, scale, out,
+                n_out, mem_in, shift, tmp_matrix);
+        else
+            resonator_eval_kernel<false><<<grid, kEvalThreads, 0, s>>>(
+                time_array, n_time, bin_centers, n_slices, kappa, J, rp, log_g, scale, out,
+                n_out, nullptr, 0, tmp_matrix);
         BB_LAUNCH_CHECK();
     }
     return BLOND_OK;
+}
+
+int blond_resonator_induced_voltage_f64(
+    const double* n_macroparticles, const double* bin_centers, int n_slices,
+    double bin_size, double beam_n_macroparticles, const double* time_array,
+    int64_t n_time, const double* R_S, const double* omega_R, const double* Q,
+    int n_resonators, double scale, double* induced_voltage, double* tmp_matrix,
+    void* workspace, int64_t workspace_bytes, void* stream) {
+    clear_error();
+    return resonator_launch(n_macroparticles, bin_centers, n_slices, bin_size,
+                            beam_n_macroparticles, time_array, n_time, R_S, omega_R, Q,
+                            n_resonators, scale, induced_voltage, n_time, nullptr, 0,
+                            tmp_matrix, workspace, workspace_bytes, stream);
+}
+
+int blond_resonator_mtw_f64(
+    const double* n_macroparticles, const double* bin_centers, int n_slices,
+    double bin_size, double beam_n_macroparticles, const double* time_array,
+    int64_t n_time, const double* R_S, const double* omega_R, const double* Q,
+    int n_resonators, double scale, const double* memory_in, double* memory_out,
+    int64_t n_memory, int64_t shift, double* tmp_matrix, void* workspace,
+    int64_t workspace_bytes, void* stream) {
+    clear_error();
+    BB_CHECK_ARG(memory_in, "resonator_mtw: null memory_in");
+    BB_CHECK_SIZE(n_memory >= n_time && shift >= 0,
+                  "resonator_mtw: memory of %lld points, n_time %lld, shift %lld "
+                  "(n_memory >= n_time and shift >= 0 required)",
+                  (long long)n_memory, (long long)n_time, (long long)shift);
+    return resonator_launch(n_macroparticles, bin_centers, n_slices, bin_size,
+                            beam_n_macroparticles, time_array, n_time, R_S, omega_R, Q,
+                            n_resonators, scale, memory_out, n_memory, memory_in, shift,
+                            tmp_matrix, workspace, workspace_bytes, stream);
 }
 
 int blond_interp_f64(const double* x, int64_t n, double x_shift, const double* xp,

@@ -430,11 +430,22 @@ class InducedVoltageResonator(_InducedVoltage):
 
     def induced_voltage_mtw(self, beam_spectrum_dict=None):
         """impedance.py:1317-1335: drop one window of memory, add this
-        turn's voltage at the first n_time points, read those back."""
+        turn's voltage at the first n_time points, read those back.  In
+        double precision with at most 64 modes this is one fused launch
+        pair writing a new memory tensor (blond_resonator_mtw_f64)."""
         S = int(self.array_length)
-        mem = self.mtw_memory
-        self.mtw_memory = torch.cat((mem, mem.new_zeros(S)))[S:].contiguous()
-        self.induced_voltage_1turn(beam_spectrum_dict)
         n_t = int(self.n_time)
-        self.mtw_memory[:n_t] += self.induced_voltage.to(self.mtw_memory.dtype)
+        mem = self.mtw_memory
+        if mem.dtype == torch.float64 and len(self._groups) == 1:
+            scale = -self.beam.particle.charge * e * self.beam.n_macroparticles \
+                * self.beam.ratio
+            self.mtw_memory, _ = bm.resonator_induced_voltage(
+                self.profile.n_macroparticles, self._bc_dev, self.profile.bin_size,
+                self.beam.n_macroparticles, self._time_dev, self.R, self.omega_r,
+                self.Q, scale, tmp_matrix=self._tmp_matrix, workspace=self._workspace,
+                memory_in=mem, shift=S)
+        else:
+            self.mtw_memory = torch.cat((mem, mem.new_zeros(S)))[S:].contiguous()
+            self.induced_voltage_1turn(beam_spectrum_dict)
+            self.mtw_memory[:n_t] += self.induced_voltage.to(self.mtw_memory.dtype)
         self.induced_voltage = self.mtw_memory[:n_t]

@@ -179,6 +179,23 @@ int blond_resonator_induced_voltage_f64(
     int n_resonators, double scale, double* induced_voltage, double* tmp_matrix,
     void* workspace, int64_t workspace_bytes, void* stream);
 
+/* One turn of InducedVoltageResonator's multi-turn memory
+ * (impedances/impedance.py:1317-1335) fused with the convolution above:
+ *   memory_out[j] = memory_in[j + shift] (0 past n_memory)
+ *                   + induced_voltage[j] (j < n_time),   j < n_memory,
+ * where induced_voltage is what blond_resonator_induced_voltage_f64 gives
+ * (the reference appends `shift` = n_slices zeros, drops the first
+ * n_slices points and adds the new voltage to the first n_time).
+ * memory_in and memory_out are distinct device arrays of n_memory >= n_time
+ * doubles; the other arguments as above. */
+int blond_resonator_mtw_f64(
+    const double* n_macroparticles, const double* bin_centers, int n_slices,
+    double bin_size, double beam_n_macroparticles, const double* time_array,
+    int64_t n_time, const double* R_S, const double* omega_R, const double* Q,
+    int n_resonators, double scale, const double* memory_in, double* memory_out,
+    int64_t n_memory, int64_t shift, double* tmp_matrix, void* workspace,
+    int64_t workspace_bytes, void* stream);
+
 /* numpy.interp(x + x_shift, xp, fp, left, right) on the device: bm.interp
  * (utils/bmath_backends.py:373) as _InducedVoltage.shift_trev_time uses it
  * for the multi-turn-wake memory (impedances/impedance.py:533-550).  flags

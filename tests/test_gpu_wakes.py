@@ -146,6 +146,27 @@ def test_resonator_reference_signature(cuda):
     assert normwise(rows.sum(axis=0) * (-E * N * c["ratio"][0]), c["voltage"]) < 1e-12
 
 
+def test_resonator_mtw_fused_matches_separate_steps(cuda):
+    """memory_out = memory_in moved by one window + V, bit for bit the
+    reference's append / slice / add on the same V."""
+    c = dict(_cases())["narrow"]
+    N, S = int(c["n_macroparticles"][0]), len(c["bin_centers"])
+    scale = -1.0 * E * N * c["ratio"][0]
+    args = (dev(c["profile"]), dev(c["bin_centers"]), c["bin_size"][0], N, dev(c["time"]),
+            c["R"], c["omega_r"], c["Q"], scale)
+    v, _ = bm.resonator_induced_voltage(*args)
+    n_t = len(c["time"])
+    for n_mem in (n_t, n_t + 1, n_t + 3 * S):
+        mem = dev(np.random.default_rng(n_mem).normal(size=n_mem) * 1e5)
+        new, _ = bm.resonator_induced_voltage(*args, memory_in=mem, shift=S)
+        want = torch.cat((mem, mem.new_zeros(S)))[S:].clone()
+        want[:n_t] += v
+        assert torch.equal(new, want)
+    with pytest.raises(_lib.BlondB200Error):
+        bm.resonator_induced_voltage(*args, memory_in=dev(np.zeros(n_t - 1)), shift=S)
+    torch.cuda.synchronize()
+
+
 def test_resonator_argument_checks(cuda):
     bc, p, t = dev(np.arange(1.0, 9.0)), dev(np.ones(8)), dev(np.arange(4.0))
     with pytest.raises(_lib.BlondB200Error):
