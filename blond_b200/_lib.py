@@ -47,6 +47,8 @@ def _sig(real):
         "histogram": [P, P, real, real, c_int, c_i64, P],
         "smooth_histogram": [P, P, real, real, c_int, c_i64, P],
         "linear_interp_kick": [P, P, P, P, real, c_int, c_i64, real, P],
+        "beam_phase": [P, P, real, real, real, real, c_int, P, P],
+        "beam_phase_fast": [P, P, real, real, real, c_int, P, P],
     }
 
 

@@ -21,7 +21,8 @@ from . import _lib
 __all__ = [
     "kick", "drift", "slice_beam", "slice_smooth", "linear_interp_kick",
     "rf_volt_comp", "fast_resonator", "rfft", "irfft", "rfftfreq",
-    "induced_voltage_1turn", "interp", "resonator_induced_voltage",
+    "induced_voltage_1turn", "interp", "resonator_induced_voltage", "beam_phase",
+    "beam_phase_fast",
     "resonator_induced_voltage_1_turn", "resonator_workspace",
     "precision", "use_precision", "B200Backend",
 ]
@@ -237,6 +238,47 @@ def induced_voltage_1turn(profile, total_impedance, n_fft, scale, n_out):
     return out
 
 
+# ------------------------------------------------------------ beam phase
+def _beam_phase_call(name, bin_centers, profile, args, start=0, stop=None):
+    p = profile
+    if not isinstance(p, torch.Tensor):
+        p = as_device(p, precision.torch_t)
+    bc = as_device(bin_centers, p.dtype, p.device)
+    stop = bc.numel() if stop is None else int(stop)
+    start = int(start)
+    if stop <= start:
+        return float("nan")
+    bcs, ps = bc[start:stop].contiguous(), p[start:stop].contiguous()
+    out = torch.empty(1, dtype=p.dtype, device=p.device)
+    r = _real(p)
+    _lib.call(f"{name}_{_suffix(p)}", _ptr(bcs), _ptr(ps), *[r(float(a)) for a in args],
+              stop - start, _ptr(out), _stream())
+    return out
+
+
+def beam_phase(bin_centers, profile, alpha, omega_rf, phi_rf, bin_size, *,
+               start=0, stop=None, device_result=False):
+    """butils_wrap_cpp.beam_phase (:785-808): the beam phase coefficient
+    (cpp_routines/beam_phase.cpp:6-40) of profile[start:stop], a float
+    (NaN for an empty range).  device_result=True returns the one-element
+    device tensor instead (no synchronisation)."""
+    out = _beam_phase_call("blond_beam_phase", bin_centers, profile,
+                           (alpha, omega_rf, phi_rf, bin_size), start, stop)
+    if device_result or not isinstance(out, torch.Tensor):
+        return out
+    return float(out.item())
+
+
+def beam_phase_fast(bin_centers, profile, omega_rf, phi_rf, bin_size, *,
+                    start=0, stop=None, device_result=False):
+    """butils_wrap_cpp.beam_phase_fast (:811-832), without the exp weight."""
+    out = _beam_phase_call("blond_beam_phase_fast", bin_centers, profile,
+                           (omega_rf, phi_rf, bin_size), start, stop)
+    if device_result or not isinstance(out, torch.Tensor):
+        return out
+    return float(out.item())
+
+
 # ------------------------------------------------------ time-domain wakes
 def interp(x, xp, fp, left=None, right=None, period=None, *, x_shift=0.0):
     """numpy.interp(x + x_shift, xp, fp, left, right) on the device in
@@ -379,6 +421,8 @@ class B200Backend:
         self.irfft = irfft
         self.rfftfreq = rfftfreq
         self.interp = interp
+        self.beam_phase = beam_phase
+        self.beam_phase_fast = beam_phase_fast
         self.resonator_induced_voltage_1_turn = resonator_induced_voltage_1_turn
 
     def use_precision(self, p: str = "double"):

@@ -7,7 +7,10 @@ the bin centres plus the induced voltage applied by linear interpolation,
 then the drift with the turn+1 parameters, on the device coordinates.  The
 RF programme is uploaded to the device once (turn-major, one contiguous
 column per turn); only a phase column that dphi_rf changed is re-sent.
-Beam/cavity feedback, periodicity and xsuite coupling are not supported.
+The beam-phase loop (``beam_feedback``, blond_b200.llrf.BeamFeedback) runs
+at the start of every turn >= its delay and corrects next turn's omega_rf
+column, which is re-sent.  Noise and cavity feedback, periodicity and
+xsuite coupling are not supported.
 """
 from __future__ import annotations
 
@@ -23,9 +26,8 @@ class RingAndRFTracker:
                  periodicity: bool = False, interpolation: bool = False,
                  with_xsuite: bool = False, profile=None,
                  total_induced_voltage=None):
-        if beam_feedback is not None or noise_feedback is not None or \
-                cavity_feedback is not None:
-            raise NotImplementedError("RF feedback loops are not supported")
+        if noise_feedback is not None or cavity_feedback is not None:
+            raise NotImplementedError("noise and cavity feedback are not supported")
         if periodicity or with_xsuite:
             raise NotImplementedError("periodicity / xsuite are not supported")
         self.rf_params = rf_station
@@ -38,7 +40,8 @@ class RingAndRFTracker:
                                "solver not recognised!")
         if self.rf_params.alpha_order > 1:
             self.solver = "exact"
-        self.beamFB = self.noiseFB = self.cavityFB = None
+        self.beamFB = beam_feedback
+        self.noiseFB = self.cavityFB = None
         self.periodicity = False
         self.with_xsuite = False
         self.interpolation = bool(interpolation)
@@ -90,6 +93,9 @@ class RingAndRFTracker:
         if rf.phi_noise is not None:
             rf.phi_rf[:, turn] += rf.phi_noise[:, turn]
             self._sync_phase(turn)
+        if self.beamFB is not None and turn >= self.beamFB.delay:
+            self.beamFB.track()
+            self._sync_column(1, turn + 1)
         rf.dphi_rf += (2.0 * np.pi * rf.harmonic[:, turn + 1]
                        * (rf.omega_rf[:, turn + 1] - rf.omega_rf_d[:, turn + 1])
                        / rf.omega_rf_d[:, turn + 1])
@@ -118,6 +124,27 @@ class RingAndRFTracker:
         self.counter[0] += 1
 
     def _sync_phase(self, t: int):
+        self._sync_column(2, t)
+
+    def _sync_column(self, which: int, t: int):
+        """Re-send turn t of omega_rf (which=1) or phi_rf (which=2)."""
         if self._dev_prog is not None:
-            col = torch.as_tensor(np.asarray(self.rf_params.phi_rf[:, t], float))
-            self._dev_prog[2][t].copy_(col.to(self._dev_prog[2].dtype))
+            src = (self.rf_params.omega_rf, self.rf_params.phi_rf)[which - 1]
+            col = torch.as_tensor(np.asarray(src[:, t], float))
+            self._dev_prog[which][t].copy_(col.to(self._dev_prog[which].dtype))
+
+
+class FullRingAndRF:
+    """RingAndRFTracker sections tracked in order (trackers/tracker.py:
+    60-213); the potential-well helpers are not provided."""
+
+    def __init__(self, ring_and_rf_section):
+        self.ring_and_rf_section = list(ring_and_rf_section)
+        self.ring_circumference = 0.0
+        for section in self.ring_and_rf_section:
+            self.ring_circumference += section.rf_params.section_length
+        self.ring_radius = self.ring_circumference / (2 * np.pi)
+
+    def track(self):
+        for section in self.ring_and_rf_section:
+            section.track()

@@ -115,6 +115,29 @@ int blond_linear_interp_kick_f32(const float* dt, float* dE,
                                  int n_slices, int64_t n, float acc_kick,
                                  void* stream);
 
+/* ------------------------------------------------------------ beam phase
+ * replaces beam_phase() and beam_phase_fast() cpp_routines/beam_phase.cpp:6-65
+ * (bound at butils_wrap_cpp.py:785-832, called by BeamFeedback.beam_phase,
+ * llrf/beam_feedback.py:276-309):
+ *   coeff = T[w p sin(omega_rf bc + phi_rf)] / T[w p cos(omega_rf bc + phi_rf)]
+ * with w = exp(alpha bc) (beam_phase) or 1 (beam_phase_fast) and T the
+ * constant-step trapezoid of blondmath.cpp:496-512.  The reference returns
+ * the value; here it is written to coeff, ONE device value, on the stream. */
+int blond_beam_phase_f64(const double* bin_centers, const double* profile,
+                         double alpha, double omega_rf, double phi_rf,
+                         double bin_size, int n_bins, double* coeff,
+                         void* stream);
+int blond_beam_phase_f32(const float* bin_centers, const float* profile,
+                         float alpha, float omega_rf, float phi_rf,
+                         float bin_size, int n_bins, float* coeff,
+                         void* stream);
+int blond_beam_phase_fast_f64(const double* bin_centers, const double* profile,
+                              double omega_rf, double phi_rf, double bin_size,
+                              int n_bins, double* coeff, void* stream);
+int blond_beam_phase_fast_f32(const float* bin_centers, const float* profile,
+                              float omega_rf, float phi_rf, float bin_size,
+                              int n_bins, float* coeff, void* stream);
+
 /* ------------------------------------------------------------ impedance setup
  * replaces fast_resonator_real_imag() cpp_routines/fast_resonator.cpp:19-74
  * re/im accumulate (+= / -=); index 0 (DC) is untouched. */

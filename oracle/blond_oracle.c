@@ -173,5 +173,28 @@ void oracle_fast_resonator_##SUF(real *re, real *im, const real *freq,       \
     }                                                                         \
 }
 
+/* beam_phase.cpp:6-65 with trapz_const_delta (blondmath.cpp:496-512):     \
+ * ratio of the constant-step trapezoids of w p sin(omega bc + phi) and     \
+ * w p cos(...), w = exp(alpha bc) (weighted) or 1.                       */
+#define DEFINE_BEAM_PHASE(real, SUF, SIN, COS, EXP)                           \
+real oracle_beam_phase_##SUF(const real *bc, const real *p, real alpha,      \
+                             real omega, real phi, real bin_size, int n,      \
+                             int weighted)                                    \
+{                                                                             \
+    real s = 0, c = 0, s0 = 0, c0 = 0, s1 = 0, c1 = 0;                        \
+    for (int i = 0; i < n; ++i) {                                             \
+        const real base = weighted ? EXP(alpha * bc[i]) * p[i] : p[i];        \
+        const real a = omega * bc[i] + phi;                                   \
+        const real fs = base * SIN(a), fc = base * COS(a);                    \
+        if (i == 0) { s0 = fs; c0 = fc; }                                     \
+        if (i == n - 1) { s1 = fs; c1 = fc; }                                 \
+        if (i > 0 && i < n - 1) { s += fs; c += fc; }                         \
+    }                                                                         \
+    const real ps = (s0 + s1) / 2. + s, pc = (c0 + c1) / 2. + c;              \
+    return (bin_size * ps) / (bin_size * pc);                                 \
+}
+
 DEFINE_ORACLE(double, f64, sin, floor, sqrt)
 DEFINE_ORACLE(float, f32, sinf, floorf, sqrtf)
+DEFINE_BEAM_PHASE(double, f64, sin, cos, exp)
+DEFINE_BEAM_PHASE(float, f32, sinf, cosf, expf)

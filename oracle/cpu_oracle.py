@@ -115,6 +115,18 @@ def fast_resonator(R, Q, freq, fr):
     return re + 1j * im
 
 
+def beam_phase(bin_centers, profile, alpha, omega_rf, phi_rf, bin_size, weighted=True):
+    """beam_phase.cpp:6-65 (weighted) / beam_phase_fast (weighted=False)."""
+    lib = load()
+    bc = np.ascontiguousarray(bin_centers)
+    p = np.ascontiguousarray(profile, dtype=bc.dtype)
+    r = _r(bc.dtype)
+    f = getattr(lib, f"oracle_beam_phase_{_suf(bc.dtype)}")
+    f.restype = r
+    return float(f(_P(bc), _P(p), r(alpha), r(omega_rf), r(phi_rf), r(bin_size),
+                   ct.c_int(len(bc)), ct.c_int(1 if weighted else 0)))
+
+
 def induced_voltage(profile, total_impedance, n_fft, charge, ratio, n_out):
     """impedance.py:475-489 with numpy.fft."""
     spec = np.fft.rfft(profile, n_fft)
