@@ -55,6 +55,8 @@ class BatchTracker:
         for t, p, rf in zip(trackers, profiles, rfs):
             if t.interpolation:
                 raise NotImplementedError("the batched engine tracks the non-interpolated kick")
+            if getattr(t, "beamFB", None) is not None:
+                raise NotImplementedError("a beam-phase loop: track with RingAndRFTracker")
             if rf.n_rf != n_rf or int(p.n_slices) != S or int(rf.n_turns) != nt \
                     or t.solver != solver:
                 raise ValueError("beams of a batch must share n_rf, n_slices, n_turns "

@@ -111,6 +111,8 @@ class FusedTracker:
                                       "non-interpolated kick")
         if getattr(profile, "smooth", False):
             raise NotImplementedError("the fused engine deposits with slice_beam")
+        if getattr(tracker, "beamFB", None) is not None:
+            raise NotImplementedError("a beam-phase loop: track with RingAndRFTracker")
         rf = tracker.rf_params
         beam = tracker.beam
         self.tracker, self.profile, self.tiv = tracker, profile, total_induced_voltage

@@ -34,6 +34,12 @@ mtw_resonator.npz     the reference's own multi-turn-wake resonator test
 mtw_tracks.npz        multi-turn wakes in mtw_mode 'time' (InducedVoltageFreq,
                       InducedVoltageTime) tracked over several turns.
 profile_fits.npz      Profile fit options 'gaussian', 'rms', 'fwhm'.
+beam_phase.npz        the reference's compiled beam_phase / beam_phase_fast.
+beam_feedback.npz     BeamFeedback (every machine type) tracked for 200 turns:
+                      per-turn beam phase, phase error, frequency correction,
+                      mean dt, the final RF frequency/phase rows and a sample
+                      of the final coordinates (the SPS set-up of the
+                      reference's unittests/llrf/test_beam_feedback.py:22-59).
 """
 from __future__ import annotations
 
@@ -506,6 +512,108 @@ def gen_profile_fits():
     save("profile_fits.npz", **out)
 
 
+# --------------------------------------------------------------------------
+# 7. beam-phase loop
+# --------------------------------------------------------------------------
+BF_CASES = {
+    # name: (machine set-up, configuration, delay)
+    "LHC": ("sps", {"machine": "LHC", "PL_gain": 1000.0}, 0),
+    "LHC_window": ("sps", {"machine": "LHC", "PL_gain": 1000.0,
+                           "window_coefficient": 2e8, "time_offset": 2.55e-9}, 0),
+    "LHC_SL": ("lhc", {"machine": "LHC", "PL_gain": 500.0, "SL_gain": 50.0}, 0),
+    "LHC_F": ("sps", {"machine": "LHC_F", "PL_gain": 1000.0, "FL_gain": 0.05}, 5),
+    "SPS_F": ("sps", {"machine": "SPS_F", "PL_gain": 1000.0, "FL_gain": 0.05}, 0),
+    "SPS_F_window": ("sps", {"machine": "SPS_F", "PL_gain": 1000.0, "FL_gain": 0.05,
+                             "window_coefficient": -1 / 5.1e-9,
+                             "time_offset": 2.5e-9}, 0),
+    "SPS_RL": ("sps", {"machine": "SPS_RL", "PL_gain": 1000.0, "RL_gain": 1e6,
+                       "sample_dE": 3}, 0),
+    "PSB": ("sps", {"machine": "PSB", "PL_gain": 1000.0, "RL_gain": [1e4, 1e2],
+                    "period": 1e-4}, 0),
+}
+BF_TURNS = 200
+BF_PARTICLES = 200000
+
+
+def bf_machine(kind, n_turns=BF_TURNS):
+    """The SPS set-up of test_beam_feedback.py:22-59 (bunch 0.05 ns, moved
+    by 0.1 ns) or an LHC-like ring (450 GeV/c, h=35640, 6 MV) whose
+    synchrotron frequency suits the LHC synchro loop."""
+    if kind == "sps":
+        ring = Ring(6911.5038, 1.0 / 17.95142852 ** 2, 25.92e9, Proton(), n_turns)
+        rf = RFStation(ring, 4620, 4.5e6, 0)
+        sigma, shift = 0.05e-9, 0.1e-9
+    else:
+        ring = Ring(26658.883, 3.225e-4, 450e9, Proton(), n_turns)
+        rf = RFStation(ring, 35640, 6e6, 0)
+        sigma, shift = 0.25e-9, 0.2e-9
+    return ring, rf, sigma, shift
+
+
+def gen_beam_phase():
+    """The reference's compiled beam_phase / beam_phase_fast
+    (cpp_routines/beam_phase.cpp:6-65) on seeded profiles, both precisions."""
+    out = {}
+    for tag, real, c_real in (("f64", np.float64, ct.c_double), ("f32", np.float32, ct.c_float)):
+        lib = ct.CDLL(os.path.join(ROOT, "oracle", "_ref",
+                                   f"libblond_ref_{'double' if tag == 'f64' else 'single'}.so"))
+        lib.beam_phase.restype = c_real
+        lib.beam_phase_fast.restype = c_real
+        rng = np.random.default_rng(777)
+        P = lambda a: a.ctypes.data_as(ct.c_void_p)  # noqa: E731
+        vals = []
+        for k, n in enumerate((1024, 333, 4096, 2)):
+            bc = np.linspace(0.0, 5e-9, n + 1)[:-1].astype(real) + real(2.5e-9 / n)
+            prof = np.maximum(0, 1e4 * np.exp(-((bc - 2.6e-9) / 0.3e-9) ** 2)
+                              + rng.normal(0, 20, n)).astype(real)
+            prm = (2e8 * (k - 1), 1.2583e9 + 10 * k, 0.01 * k, 5e-9 / n)
+            a = lib.beam_phase(P(bc), P(prof), c_real(prm[0]), c_real(prm[1]),
+                               c_real(prm[2]), c_real(prm[3]), ct.c_int(n))
+            f = lib.beam_phase_fast(P(bc), P(prof), c_real(prm[1]), c_real(prm[2]),
+                                    c_real(prm[3]), ct.c_int(n))
+            out[f"{tag}_{k}_bc"], out[f"{tag}_{k}_profile"] = bc, prof
+            out[f"{tag}_{k}_params"] = np.array(prm)
+            vals.append((a, f))
+        out[f"{tag}_coeff"] = np.array(vals)
+    save("beam_phase.npz", **out)
+
+
+def gen_beam_feedback():
+    from blond.llrf.beam_feedback import BeamFeedback
+    from blond.trackers.tracker import FullRingAndRF
+    # BeamFeedback.beam_phase_sharpWindow (SPS_F) calls bm.trapz and
+    # bm.logical_and, which no backend of the reference defines
+    # (utils/bmath_backends.py); numpy's functions of those names are
+    # provided here.
+    for name, fn in (("trapz", np.trapezoid), ("logical_and", np.logical_and)):
+        if not hasattr(bm, name):
+            setattr(bm, name, fn)
+    out = {"names": np.array(list(BF_CASES))}
+    for name, (kind, cfg, delay) in BF_CASES.items():
+        ring, rf, sigma, shift = bf_machine(kind)
+        beam = Beam(ring, BF_PARTICLES, 1.2e6)
+        bigaussian(ring, rf, beam, sigma, seed=1234)
+        beam.dt += shift
+        profile = Profile(beam, CutOptions(cut_left=0, cut_right=rf.t_rf[0, 0],
+                                           n_slices=1024))
+        cfg = {k: (list(v) if isinstance(v, list) else v) for k, v in cfg.items()}
+        loop = BeamFeedback(ring, rf, profile, cfg, delay=delay)
+        section = RingAndRFTracker(rf, beam, profile=profile, beam_feedback=loop)
+        tracker = FullRingAndRF([section])
+        trace = np.zeros((BF_TURNS, 4))
+        for turn in range(BF_TURNS):
+            trace[turn, 0] = np.mean(beam.dt)
+            profile.track()
+            tracker.track()
+            trace[turn, 1:] = (loop.phi_beam, loop.dphi, loop.domega_rf)
+        out[f"{name}_trace"] = trace
+        out[f"{name}_omega_rf"] = rf.omega_rf[0].copy()
+        out[f"{name}_phi_rf"] = rf.phi_rf[0].copy()
+        out[f"{name}_dt"] = beam.dt[::997].copy()
+        out[f"{name}_dE"] = beam.dE[::997].copy()
+    save("beam_feedback.npz", **out)
+
+
 def run_reference_profile_test():
     """Run the reference's own profile unit test (its literal expected
     counts) against oracle/_ref before the fixture is trusted."""
@@ -532,3 +640,5 @@ if __name__ == "__main__":
     gen_mtw_resonator()
     gen_mtw_tracks()
     gen_profile_fits()
+    gen_beam_phase()
+    gen_beam_feedback()
