@@ -16,6 +16,7 @@
 // The turn index lives in device memory, so a CUDA graph of K turns is
 // captured once and replayed.
 #include "spectral.cuh"
+#include "feedback.cuh"
 
 #include <algorithm>
 #include <cstddef>
@@ -635,6 +636,14 @@ struct blond_engine {
     double iv_scale = 0.0;
     bool has_ind = false;
     double* d_ind = nullptr;
+    // beam-phase loop (blond_engine_set_feedback)
+    bool has_fb = false;
+    bb::FeedbackArgs fb = {};
+    double* d_fb_table = nullptr;
+    double* d_fb_on_time = nullptr;
+    double* d_fb_state = nullptr;
+    double* d_fb_trace = nullptr;
+    double* d_fb_partials = nullptr;
     // state
     long long* d_turn = nullptr;
     int* d_err = nullptr;  // set by a kernel whose bounded wait gave up
@@ -962,7 +971,38 @@ static int launch_profile(blond_engine* e, bool clear, cudaStream_t s) {
     return BLOND_OK;
 }
 
+// The beam-phase loop of this turn, after its head has written the profile.
+static int launch_loop(blond_engine* e, cudaStream_t s) {
+    if (!e->has_fb) return BLOND_OK;
+    FeedbackArgs a = e->fb;
+    a.turn = e->d_turn;
+    a.profile = e->d_profile;
+    a.bc = e->d_bc;
+    a.S = e->S;
+    a.dE = e->dE;
+    a.dE_f32 = e->precision == BLOND_PREC_F32P64;
+    a.n = e->n;
+    a.om = e->d_om;
+    a.ph = e->d_ph;
+    a.table = e->d_fb_table;
+    a.on_time = e->d_fb_on_time;
+    a.state = e->d_fb_state;
+    a.trace = e->d_fb_trace;
+    a.partials = e->d_fb_partials;
+    a.n_rf = e->n_rf;
+    a.n_turns = e->n_turns;
+    return launch_feedback(a, s);
+}
+
+static int launch_spectral_head(blond_engine* e, cudaStream_t s);
+
 static int launch_head(blond_engine* e, cudaStream_t s) {
+    int rc = launch_spectral_head(e, s);
+    if (rc) return rc;
+    return launch_loop(e, s);
+}
+
+static int launch_spectral_head(blond_engine* e, cudaStream_t s) {
     if (!(e->has_fft || e->has_ind)) return launch_profile(e, true, s);
     if (!e->has_fft) {
         set_error("engine: an inductive impedance needs an FFT impedance in this build");
@@ -1082,7 +1122,8 @@ int blond_engine_destroy(blond_engine* e) {
     if (e->io_out) cudaStreamDestroy(e->io_out);
     for (void* p : {(void*)e->d_V, (void*)e->d_om, (void*)e->d_ph, (void*)e->d_acc,
                     (void*)e->d_drift, (void*)e->d_bc, (void*)e->d_H, (void*)e->d_tw,
-                    (void*)e->d_ind,
+                    (void*)e->d_ind, (void*)e->d_fb_table, (void*)e->d_fb_on_time,
+                    (void*)e->d_fb_state, (void*)e->d_fb_trace, (void*)e->d_fb_partials,
                     (void*)e->d_turn, (void*)e->d_err, (void*)e->own_hist, (void*)e->d_profile,
                     (void*)e->d_vind, e->d_table})
         free_ptr(p);
@@ -1645,6 +1686,78 @@ int blond_engine_time_kernels(blond_engine* e, int64_t n_turns, double* head_ms,
     *head_ms = h;
     *particles_ms = p;
     return launch_profile(e, false, s);
+}
+
+int blond_engine_set_feedback(blond_engine* e, int machine, int delay, double gain,
+                              double gain2, double alpha, int has_time_offset,
+                              double time_offset, double bin_size, double ring_radius,
+                              int sample_dE, const double* turn_table, const double* on_time,
+                              int n_on_time, const double* state) {
+    BB_CHECK_ARG(e, "engine_set_feedback: null engine");
+    if (machine == 0) {
+        e->has_fb = false;
+        e->graph_dirty = true;
+        return BLOND_OK;
+    }
+    BB_CHECK_ARG(machine >= BLOND_FB_LHC && machine <= BLOND_FB_PSB,
+                 "engine_set_feedback: unknown machine %d", machine);
+    BB_CHECK_ARG(turn_table && state, "engine_set_feedback: null table or state");
+    BB_CHECK_ARG(e->rf_set, "engine_set_feedback: call set_rf first");
+    BB_CHECK_ARG(sample_dE >= 1, "engine_set_feedback: sample_dE must be >= 1");
+    BB_CHECK_ARG(machine != BLOND_FB_PSB || (on_time && n_on_time >= 1),
+                 "engine_set_feedback: the PSB loop needs its on-time turns");
+    const size_t cols = (size_t)FB_COLS + 2 * (size_t)e->n_rf;
+    int rc;
+    if ((rc = upload((void**)&e->d_fb_table, turn_table,
+                     sizeof(double) * cols * (size_t)(e->n_turns + 1))))
+        return rc;
+    if ((rc = upload((void**)&e->d_fb_state, state,
+                     sizeof(double) * ((size_t)FBS_DPHI_RF + e->n_rf))))
+        return rc;
+    if (machine == BLOND_FB_PSB &&
+        (rc = upload((void**)&e->d_fb_on_time, on_time, sizeof(double) * n_on_time)))
+        return rc;
+    std::vector<double> zeros((size_t)(e->n_turns + 1) * 3, 0.0);
+    if ((rc = upload((void**)&e->d_fb_trace, zeros.data(), sizeof(double) * zeros.size())))
+        return rc;
+    if (!e->d_fb_partials) BB_CUDA(cudaMalloc((void**)&e->d_fb_partials, sizeof(double) * kFbPartials));
+    FeedbackArgs& a = e->fb;
+    a = {};
+    a.machine = machine;
+    a.delay = delay;
+    a.gain = gain;
+    a.gain2 = gain2;
+    a.alpha = alpha;
+    a.has_time_offset = has_time_offset;
+    a.time_offset = time_offset;
+    a.bin_size = bin_size;
+    a.ring_radius = ring_radius;
+    a.sample_dE = sample_dE;
+    a.n_on_time = machine == BLOND_FB_PSB ? n_on_time : 0;
+    e->has_fb = true;
+    e->graph_dirty = true;
+    return BLOND_OK;
+}
+
+int blond_engine_get_feedback(blond_engine* e, double* state, double* omega_rf,
+                              double* phi_rf, double* trace, void* stream) {
+    BB_CHECK_ARG(e, "engine_get_feedback: null engine");
+    BB_CHECK_ARG(e->has_fb, "engine_get_feedback: no beam-phase loop set");
+    cudaStream_t s = as_stream(stream);
+    const size_t cols = (size_t)(e->n_turns + 1) * e->n_rf;
+    if (state)
+        BB_CUDA(cudaMemcpyAsync(state, e->d_fb_state, sizeof(double) * (FBS_DPHI_RF + e->n_rf),
+                                cudaMemcpyDeviceToDevice, s));
+    if (omega_rf)
+        BB_CUDA(cudaMemcpyAsync(omega_rf, e->d_om, sizeof(double) * cols,
+                                cudaMemcpyDeviceToDevice, s));
+    if (phi_rf)
+        BB_CUDA(cudaMemcpyAsync(phi_rf, e->d_ph, sizeof(double) * cols,
+                                cudaMemcpyDeviceToDevice, s));
+    if (trace)
+        BB_CUDA(cudaMemcpyAsync(trace, e->d_fb_trace, sizeof(double) * 3 * (e->n_turns + 1),
+                                cudaMemcpyDeviceToDevice, s));
+    return BLOND_OK;
 }
 
 int blond_engine_get_profile(blond_engine* e, double* out, void* stream) {

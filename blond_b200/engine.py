@@ -70,6 +70,10 @@ class TurnEngine:
         _lib.call(f"blond_engine_{name}", self.h, *args)
 
 
+# BeamFeedback.machine -> blond_engine_set_feedback code (include/blond_b200.h)
+FB_MACHINES = {"LHC": 1, "LHC_F": 2, "SPS_F": 3, "SPS_RL": 4, "PSB": 5}
+
+
 def _stream():
     return ct.c_void_p(torch.cuda.current_stream().cuda_stream)
 
@@ -111,8 +115,6 @@ class FusedTracker:
                                       "non-interpolated kick")
         if getattr(profile, "smooth", False):
             raise NotImplementedError("the fused engine deposits with slice_beam")
-        if getattr(tracker, "beamFB", None) is not None:
-            raise NotImplementedError("a beam-phase loop: track with RingAndRFTracker")
         rf = tracker.rf_params
         beam = tracker.beam
         self.tracker, self.profile, self.tiv = tracker, profile, total_induced_voltage
@@ -138,6 +140,7 @@ class FusedTracker:
                       float(profile.cut_right), _p(bc))
         if total_induced_voltage is not None:
             self._set_impedance(total_induced_voltage, beam, rf)
+        self.loop = getattr(tracker, "beamFB", None)
         # coordinates
         if beam.dt.dtype != torch.float64:
             raise TypeError("the fused engine needs float64 dt")
@@ -171,6 +174,8 @@ class FusedTracker:
         self.tune_mode = tune
         self.tuned = None
         self.eng.call("set_turn", int(rf.counter[0]), _stream())
+        if self.loop is not None:
+            self._set_loop(self.loop, process_group)
         # sharded: this rank holds a part of the beam; the int32 histogram is
         # summed over `process_group` after every particle pass.  The beam's
         # ratio (intensity / macro-particles) must be the whole beam's.
@@ -182,6 +187,88 @@ class FusedTracker:
             self.eng.call("bind_histogram", ct.c_void_p(self.hist.data_ptr()))
             start_sharded(lambda: self.eng.call("slice", _stream()), self._reduce,
                           lambda: self.eng.call("step", 3, _stream()))
+
+    def _set_loop(self, loop, process_group):
+        """The beam-phase loop on the device (blond_engine_set_feedback):
+        its per-turn table, parameters and current state from the
+        BeamFeedback object (blond_b200.llrf.beam_feedback)."""
+        if loop.RFnoise is not None or loop.noiseFB is not None:
+            raise NotImplementedError("phase noise in the fused beam-phase loop")
+        if loop.machine == "SPS_RL" and process_group is not None:
+            raise NotImplementedError("the SPS_RL loop averages dE over the whole beam; "
+                                      "not on a sharded beam")
+        if loop.machine == "SPS_RL" and loop.reference != 0:
+            raise NotImplementedError("radial steering (reference != 0)")
+        code = FB_MACHINES[loop.machine]
+        rf, ring = self.rf, loop.ring
+        nt1 = int(rf.n_turns) + 1
+        n_rf = rf.n_rf
+
+        def col(x):
+            return np.broadcast_to(np.asarray(x, dtype=float), (nt1,))
+        zeros = np.zeros(nt1)
+        gain = col(loop.gain)
+        g2 = loop.gain2
+        g2a, g2b = (col(g2[0]), col(g2[1])) if loop.machine == "PSB" else (zeros, zeros)
+        lhc_a = col(loop.lhc_a) if loop.machine == "LHC" else zeros
+        lhc_t = col(loop.lhc_t) if loop.machine == "LHC" else zeros
+        table = np.column_stack(
+            [col(rf.phi_s), col(rf.eta_0), col(np.asarray(ring.alpha_0)[0]), col(rf.gamma),
+             col(np.asarray(ring.beta)[0]), col(np.asarray(ring.energy)[0]), lhc_a, lhc_t,
+             gain, g2a, g2b]
+            + [np.asarray(rf.omega_rf_d, float)[j, :nt1] for j in range(n_rf)]
+            + [np.asarray(rf.harmonic, float)[j, :nt1] for j in range(n_rf)])
+        table = np.ascontiguousarray(table, dtype=np.float64)
+        state = np.zeros(16 + n_rf)
+        if loop.machine == "LHC":
+            state[0] = loop.lhc_y
+        if loop.machine == "PSB":
+            state[1:8] = (loop.dphi_sum, loop.dphi_av, loop.dphi_av_prev, loop.domega_PL,
+                          loop.domega_RL, loop.dR_over_R_prev, loop.PL_counter)
+            state[12] = loop.dR_over_R
+        state[8:12] = (loop.phi_beam, loop.dphi, loop.domega_rf, loop.drho)
+        state[16:] = np.asarray(rf.dphi_rf, float)
+        on_time = np.ascontiguousarray(getattr(loop, "on_time", np.zeros(1)), dtype=np.float64)
+        if on_time.size == 0:
+            on_time = np.zeros(1)
+        gain2 = 0.0 if loop.machine == "PSB" else float(loop.gain2)
+        gain1 = 0.0 if loop.machine == "PSB" else float(loop.gain)
+        self.eng.call("set_feedback", code, int(loop.delay), gain1, gain2,
+                      float(loop.alpha), 1 if loop.time_offset is not None else 0,
+                      float(loop.time_offset or 0.0), float(self.profile.bin_size),
+                      float(ring.ring_radius), int(getattr(loop, "sample_dE", 1)),
+                      _p(table), _p(on_time), int(on_time.size), _p(state))
+        self._fb_n_state = state.size
+
+    def _pull_loop(self):
+        """The device loop's state and the corrected RF programmes back into
+        the BeamFeedback and RFStation objects (what the host loop leaves)."""
+        if self.loop is None:
+            return
+        rf, loop = self.rf, self.loop
+        nt1, n_rf = int(rf.n_turns) + 1, rf.n_rf
+        st = torch.empty(self._fb_n_state, dtype=torch.float64, device="cuda")
+        om = torch.empty((nt1, n_rf), dtype=torch.float64, device="cuda")
+        ph = torch.empty_like(om)
+        tr = torch.empty((nt1, 3), dtype=torch.float64, device="cuda")
+        self.eng.call("get_feedback", ct.c_void_p(st.data_ptr()), ct.c_void_p(om.data_ptr()),
+                      ct.c_void_p(ph.data_ptr()), ct.c_void_p(tr.data_ptr()), _stream())
+        st, om, ph, tr = (x.cpu().numpy() for x in (st, om, ph, tr))
+        rf.omega_rf[:, :] = om.T
+        rf.phi_rf[:, :] = ph.T
+        rf.dphi_rf[:] = st[16:16 + n_rf]
+        loop.phi_beam, loop.dphi, loop.domega_rf = float(st[8]), float(st[9]), float(st[10])
+        if loop.machine == "LHC":
+            loop.lhc_y = float(st[0])
+        elif loop.machine == "SPS_RL":
+            loop.average_dE, loop.drho = float(st[13]), float(st[11])
+        elif loop.machine == "PSB":
+            (loop.dphi_sum, loop.dphi_av, loop.dphi_av_prev, loop.domega_PL, loop.domega_RL,
+             loop.dR_over_R_prev) = (float(x) for x in st[1:7])
+            loop.PL_counter = int(st[7])
+            loop.dR_over_R = float(st[12])
+        self.loop_trace = tr
+        self.tracker._dev_prog = None  # the drop-in tracker re-sends the programmes
 
     def _reduce(self):
         import torch.distributed as dist
@@ -255,6 +342,7 @@ class FusedTracker:
         self.beam.gamma = float(rf.gamma[t])
         self.beam.energy = float(rf.energy[t])
         self.beam.momentum = float(rf.momentum[t])
+        self._pull_loop()
 
     def track_host(self, host_dt: torch.Tensor, host_dE: torch.Tensor, n_turns: int = 1,
                    chunks: int = 4):
@@ -280,6 +368,7 @@ class FusedTracker:
         self.beam.gamma = float(rf.gamma[t])
         self.beam.energy = float(rf.energy[t])
         self.beam.momentum = float(rf.momentum[t])
+        self._pull_loop()
 
     def prepare(self):
         """Build and upload the CUDA graph now (otherwise the first track()
@@ -298,6 +387,7 @@ class FusedTracker:
         h, p = ct.c_double(), ct.c_double()
         self.eng.call("time_kernels", int(n_turns), ct.byref(h), ct.byref(p), _stream())
         self.rf.counter[0] += int(n_turns)
+        self._pull_loop()
         return h.value, p.value
 
     def sync(self):

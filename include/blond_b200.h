@@ -288,6 +288,46 @@ int blond_engine_run(blond_engine* engine, int64_t n_turns, void* stream);
  * BLOND_ERR_TIMEOUT if a bounded wait in a kernel gave up (the coordinates
  * are then not valid), else BLOND_OK.  Clears the flag. */
 int blond_engine_check(blond_engine* engine, void* stream);
+
+/* The beam-phase loop inside the turn: replaces BeamFeedback.track()
+ * (llrf/beam_feedback.py:237-622) called by RingAndRFTracker.track()
+ * (trackers/tracker.py:551-552) and the tracker's accumulation of the RF
+ * phase offset (tracker.py:553-565).  After the head of turn t (turn >=
+ * delay) one block measures the beam phase of the profile (beam_phase,
+ * exp(alpha t)-weighted from time_offset on; SPS_F: the sharp window),
+ * runs the machine's loop on device state and adds the frequency correction
+ * to omega_rf of turn t + 1 of every RF system (times h_j / h_0); then, every
+ * turn, dphi_rf += 2 pi h (omega_rf - omega_rf_d) / omega_rf_d at t + 1 and
+ * phi_rf[t + 1] += dphi_rf.  SPS_RL also averages dE[::sample_dE] of the
+ * bound beam (one extra pass over those particles).
+ *   turn_table: HOST, (n_turns + 1) rows of 11 + 2 n_rf values: phi_s, eta_0,
+ *     alpha_0, gamma, beta, energy, lhc_a, lhc_t, PL gain, second gain,
+ *     third gain (PSB radial integral), omega_rf_d[n_rf], harmonic[n_rf].
+ *   state: HOST, BLOND_FB_STATE(n_rf) values: lhc_y, dphi_sum, dphi_av,
+ *     dphi_av_prev, domega_PL, domega_RL, dR_over_R_prev, PL_counter,
+ *     phi_beam, dphi, domega_rf, drho, dR_over_R, average_dE, (2 unused),
+ *     dphi_rf[n_rf].
+ *   on_time: HOST, the PSB loop's action turns (precalculate_time).
+ * machine 0 removes the loop.  Phase noise is not modelled. */
+#define BLOND_FB_LHC 1
+#define BLOND_FB_LHC_F 2
+#define BLOND_FB_SPS_F 3
+#define BLOND_FB_SPS_RL 4
+#define BLOND_FB_PSB 5
+#define BLOND_FB_STATE(n_rf) (16 + (n_rf))
+int blond_engine_set_feedback(blond_engine* engine, int machine, int delay,
+                              double gain, double gain2, double alpha,
+                              int has_time_offset, double time_offset,
+                              double bin_size, double ring_radius,
+                              int sample_dE, const double* turn_table,
+                              const double* on_time, int n_on_time,
+                              const double* state);
+/* Device copies of the loop state, the omega_rf / phi_rf programmes
+ * (turn-major, (n_turns + 1) x n_rf) and the per-turn trace ((n_turns + 1)
+ * x 3: phi_beam, dphi, domega_rf); NULL skips an output. */
+int blond_engine_get_feedback(blond_engine* engine, double* state,
+                              double* omega_rf, double* phi_rf, double* trace,
+                              void* stream);
 /* Particle-pass implementation: 0 = bulk-copy (TMA) pipelined (default;
  * falls back to 1 when the profile is too long for its shared memory),
  * 1 = plain loads. */
