@@ -61,6 +61,9 @@ def parse():
                          "2^16 slices, 4 resonators + inductive Z/n; "
                          "mtw: one turn of InducedVoltageResonator's multi-turn wake")
     ap.add_argument("--beams", type=int, default=256)
+    ap.add_argument("--feedback", default="none",
+                    choices=["none", "LHC", "LHC_F", "SPS_F", "SPS_RL", "PSB"],
+                    help="c2 with a beam-phase loop of this machine type in every turn")
     ap.add_argument("--tune", default="auto", choices=["auto", "fixed"],
                     help="fixed: no autotuner; --threads/--blocks-per-sm/--prefetch "
                          "give the particle pass's launch shape (profiling runs)")
@@ -218,7 +221,17 @@ def barrier(world):
 
 
 # ----------------------------------------------------------------- our arm
-def build_fused(n, S, n_turns, precision, kernel="auto", seed=0, group=None, shape=None):
+FEEDBACK_CONFIGS = {
+    "LHC": {"machine": "LHC", "PL_gain": 1000.0},
+    "LHC_F": {"machine": "LHC_F", "PL_gain": 1000.0, "FL_gain": 0.05},
+    "SPS_F": {"machine": "SPS_F", "PL_gain": 1000.0, "FL_gain": 0.05},
+    "SPS_RL": {"machine": "SPS_RL", "PL_gain": 1000.0, "RL_gain": 1e6, "sample_dE": 1},
+    "PSB": {"machine": "PSB", "PL_gain": 1000.0, "RL_gain": [1e4, 1e2], "period": 1e-4},
+}
+
+
+def build_fused(n, S, n_turns, precision, kernel="auto", seed=0, group=None, shape=None,
+                feedback="none"):
     """One beam of n macro-particles per GPU.  With a process group the GPUs
     hold shards of ONE beam (seed = rank: independent samples of the same
     bunch) whose histogram is summed every turn; the charge per
@@ -237,7 +250,13 @@ def build_fused(n, S, n_turns, precision, kernel="auto", seed=0, group=None, sha
     prof = Profile(beam, CutOptions(cut_left=cl, cut_right=cr, n_slices=S))
     iv = InducedVoltageFreq(beam, prof, [Resonators(5e6, 1e9, 1.0)])
     tiv = TotalInducedVoltage(beam, prof, [iv])
-    tracker = RingAndRFTracker(rf, beam)
+    loop = None
+    if feedback != "none":
+        from blond_b200.llrf.beam_feedback import BeamFeedback
+        cfg = {k: (list(v) if isinstance(v, list) else v)
+               for k, v in FEEDBACK_CONFIGS[feedback].items()}
+        loop = BeamFeedback(ring, rf, prof, cfg)
+    tracker = RingAndRFTracker(rf, beam, beam_feedback=loop)
     if shape is None:
         fused = FusedTracker(tracker, prof, tiv, precision=precision, turns_per_graph=50,
                              kernel=kernel, process_group=group)
@@ -277,7 +296,7 @@ def run_ours(args, world, rank, local):
     shape = ((args.threads, args.blocks_per_sm, args.prefetch) if args.tune == "fixed"
              else None)
     fused, beam, n_fft = build_fused(n, S, total, args.precision, args.kernel, seed=rank,
-                                     group=group, shape=shape)
+                                     group=group, shape=shape, feedback=args.feedback)
     fused.track(W)
     if group is None:
         fused.prepare()  # graph capture/upload outside the timed region
@@ -321,6 +340,8 @@ def run_ours(args, world, rank, local):
         "config": {"workload": WORKLOAD, "particles": n, "slices": S, "n_fft": n_fft,
                    "intensity": 1e10, "turns_per_graph": 50,
                    "autotuned": fused.tuned,
+                   **({"beam_phase_loop": FEEDBACK_CONFIGS[args.feedback]}
+                      if args.feedback != "none" else {}),
                    "l2": f"inputs larger than L2: {alg_bytes // 2 / 1e6:.0f} MB of dt/dE read per turn",
                    "parallelism": (f"dp{world}: one beam of {world} x {n:.0e} particles, "
                                    "int32 histogram all-reduce (NCCL) per turn")

@@ -643,7 +643,8 @@ struct blond_engine {
     double* d_fb_on_time = nullptr;
     double* d_fb_state = nullptr;
     double* d_fb_trace = nullptr;
-    double* d_fb_partials = nullptr;
+    double* d_fb_partials = nullptr;  // dE partials, then the beam-phase partials
+    int* d_fb_ticket = nullptr;  // last-block ticket of the loop pass (0 between passes)
     // state
     long long* d_turn = nullptr;
     int* d_err = nullptr;  // set by a kernel whose bounded wait gave up
@@ -971,14 +972,14 @@ static int launch_profile(blond_engine* e, bool clear, cudaStream_t s) {
     return BLOND_OK;
 }
 
-// The beam-phase loop of this turn, after its head has written the profile.
-static int launch_loop(blond_engine* e, cudaStream_t s) {
-    if (!e->has_fb) return BLOND_OK;
+// The beam-phase loop's arguments for this engine's buffers.
+static FeedbackArgs fb_args(const blond_engine* e) {
     FeedbackArgs a = e->fb;
     a.turn = e->d_turn;
     a.profile = e->d_profile;
     a.bc = e->d_bc;
     a.S = e->S;
+    a.dt = static_cast<const double*>(e->dt);
     a.dE = e->dE;
     a.dE_f32 = e->precision == BLOND_PREC_F32P64;
     a.n = e->n;
@@ -989,20 +990,37 @@ static int launch_loop(blond_engine* e, cudaStream_t s) {
     a.state = e->d_fb_state;
     a.trace = e->d_fb_trace;
     a.partials = e->d_fb_partials;
+    a.phase_partials = e->d_fb_partials + kFbPartials;
     a.n_rf = e->n_rf;
     a.n_turns = e->n_turns;
-    return launch_feedback(a, s);
+    return a;
 }
 
-static int launch_spectral_head(blond_engine* e, cudaStream_t s);
+static int launch_spectral_head(blond_engine* e, cudaStream_t s, bool loop);
 
+// The head of a turn: profile (and induced voltage, table).  With a
+// beam-phase loop the spectral head also forms the beam-phase sums while it
+// converts the histogram, and its last CTA runs the loop (it corrects the
+// next turn's RF programme); without a spectral head one all-SM pass does
+// the conversion and the loop.  SPS_RL first sums dE over the beam.
 static int launch_head(blond_engine* e, cudaStream_t s) {
-    int rc = launch_spectral_head(e, s);
-    if (rc) return rc;
-    return launch_loop(e, s);
+    int rc;
+    if (!e->has_fb) return launch_spectral_head(e, s, false);
+    const FeedbackArgs a = fb_args(e);
+    if (!e->has_fft) {
+        if ((rc = launch_feedback_dE(a, s))) return rc;
+        return launch_feedback_turn(a, e->d_hist, e->d_fb_ticket, 1, s);
+    }
+    if (a.machine != BLOND_FB_SPS_RL) return launch_spectral_head(e, s, true);
+    // SPS_RL averages dE after the induced-voltage kick (the reference's
+    // TotalInducedVoltage.track precedes RingAndRFTracker.track): head
+    // first, then that average, then the loop on the head's profile
+    if ((rc = launch_spectral_head(e, s, false))) return rc;
+    if ((rc = launch_feedback_dE_lik(a, e->d_table, e->bc0, e->lik_inv_w, e->bw, s))) return rc;
+    return launch_feedback_turn(a, nullptr, e->d_fb_ticket, 0, s);
 }
 
-static int launch_spectral_head(blond_engine* e, cudaStream_t s) {
+static int launch_spectral_head(blond_engine* e, cudaStream_t s, bool loop) {
     if (!(e->has_fft || e->has_ind)) return launch_profile(e, true, s);
     if (!e->has_fft) {
         set_error("engine: an inductive impedance needs an FFT impedance in this build");
@@ -1028,6 +1046,12 @@ static int launch_spectral_head(blond_engine* e, cudaStream_t s) {
     P.turn = e->d_turn;
     P.bump_turn = 1;
     P.twg = e->d_tw;
+    if (loop) {
+        SpecLoop L;
+        L.ticket = e->d_fb_ticket;
+        L.fb = fb_args(e);
+        return launch_spectral_loop(P, L, s);
+    }
     return launch_spectral(P, s);
 }
 
@@ -1115,6 +1139,7 @@ int blond_engine_create(blond_engine** out, int precision, int n_rf, int solver,
 
 int blond_engine_destroy(blond_engine* e) {
     if (!e) return BLOND_OK;
+
     if (e->graph) cudaGraphExecDestroy(e->graph);
     if (e->cap_stream) cudaStreamDestroy(e->cap_stream);
     for (cudaEvent_t ev : e->io_ev) cudaEventDestroy(ev);
@@ -1123,7 +1148,7 @@ int blond_engine_destroy(blond_engine* e) {
     for (void* p : {(void*)e->d_V, (void*)e->d_om, (void*)e->d_ph, (void*)e->d_acc,
                     (void*)e->d_drift, (void*)e->d_bc, (void*)e->d_H, (void*)e->d_tw,
                     (void*)e->d_ind, (void*)e->d_fb_table, (void*)e->d_fb_on_time,
-                    (void*)e->d_fb_state, (void*)e->d_fb_trace, (void*)e->d_fb_partials,
+                    (void*)e->d_fb_state, (void*)e->d_fb_trace, (void*)e->d_fb_partials, (void*)e->d_fb_ticket,
                     (void*)e->d_turn, (void*)e->d_err, (void*)e->own_hist, (void*)e->d_profile,
                     (void*)e->d_vind, e->d_table})
         free_ptr(p);
@@ -1720,7 +1745,10 @@ int blond_engine_set_feedback(blond_engine* e, int machine, int delay, double ga
     std::vector<double> zeros((size_t)(e->n_turns + 1) * 3, 0.0);
     if ((rc = upload((void**)&e->d_fb_trace, zeros.data(), sizeof(double) * zeros.size())))
         return rc;
-    if (!e->d_fb_partials) BB_CUDA(cudaMalloc((void**)&e->d_fb_partials, sizeof(double) * kFbPartials));
+    if (!e->d_fb_partials)
+        BB_CUDA(cudaMalloc((void**)&e->d_fb_partials,
+                           sizeof(double) * (kFbPartials + 2 * kFbMaxParts)));
+
     FeedbackArgs& a = e->fb;
     a = {};
     a.machine = machine;
@@ -1734,6 +1762,10 @@ int blond_engine_set_feedback(blond_engine* e, int machine, int delay, double ga
     a.ring_radius = ring_radius;
     a.sample_dE = sample_dE;
     a.n_on_time = machine == BLOND_FB_PSB ? n_on_time : 0;
+    if (!e->d_fb_ticket) {
+        BB_CUDA(cudaMalloc((void**)&e->d_fb_ticket, sizeof(int)));
+        BB_CUDA(cudaMemset(e->d_fb_ticket, 0, sizeof(int)));
+    }
     e->has_fb = true;
     e->graph_dirty = true;
     return BLOND_OK;

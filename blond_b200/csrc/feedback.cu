@@ -12,6 +12,8 @@
 #include "common.cuh"
 #include "feedback.cuh"
 
+#include <algorithm>
+
 namespace bb {
 namespace {
 
@@ -102,177 +104,139 @@ fb_dE_kernel(const void* dE, int f32, int64_t n, int sample, double* partials) {
     }
 }
 
-// first index with bc >= x (count of bc < x), bc increasing
-__device__ int fb_lower(const double* bc, int S, double x) {
-    int lo = 0, hi = S;
-    while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (bc[mid] < x) lo = mid + 1; else hi = mid;
+// Sum of dE[k * sample_dE] after this turn's interpolated kick, computed
+// as the particle pass computes it (same table, same expression).
+__global__ void __launch_bounds__(256)
+fb_dE_lik_kernel(const double* dt, const void* dE, int f32, int64_t n, int sample,
+                 const void* table, double bc0, double lik_inv_w, double bw, int S,
+                 double* partials) {
+    const int64_t m = (n + sample - 1) / sample;
+    double acc = 0.0;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < m;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = k * sample;
+        const double t = dt[i];
+        const double f = floor((t - bc0) * lik_inv_w);
+        const bool in = f >= 0.0 && f < (double)(S - 1);
+        const int q = in ? (int)f : 0;
+        if (!f32) {
+            double e = static_cast<const double*>(dE)[i];
+            if (in) {
+                const double2 tb = __ldg(reinterpret_cast<const double2*>(table) + q);
+                e += t * tb.x + tb.y;
+            }
+            acc += e;
+        } else {
+            float e = static_cast<const float*>(dE)[i];
+            if (in) {
+                const float2 tb = __ldg(reinterpret_cast<const float2*>(table) + q);
+                const float x = (float)(t - (bc0 + (double)q * bw));
+                e += __fmaf_rn(tb.y, x, tb.x);
+            }
+            acc += (double)e;
+        }
     }
-    return lo;
-}
-// first index with bc > x
-__device__ int fb_upper(const double* bc, int S, double x) {
-    int lo = 0, hi = S;
-    while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (bc[mid] <= x) lo = mid + 1; else hi = mid;
+    __shared__ double sh[8];
+    for (int d = 16; d > 0; d >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, d);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tsum = 0.0;
+        for (int w = 0; w < 8; ++w) tsum += sh[w];
+        partials[blockIdx.x] = tsum;
     }
-    return lo;
 }
 
-__global__ void __launch_bounds__(kPhaseThreads) feedback_kernel(FeedbackArgs a) {
-    __shared__ int range[2];
-    __shared__ double ss[32], sc[32], sd[32];
-    const long long t = *a.turn - 1;
-    const int nr = a.n_rf;
-    const int cols = FB_COLS + 2 * nr;
-    const double* row = a.table + (size_t)t * cols;
-    const double* next = a.table + (size_t)(t + 1) * cols;
+// One pass per turn: histogram -> profile (histogram cleared) with every
+// warp's share of the two projections in phase_partials; the block that
+// takes the last ticket (no waiting) sums the shares in index order (and
+// SPS_RL's dE partials) and runs the loop; with bump it then advances the
+// turn counter (heads without a spectral kernel).  The arguments come by
+// value: no pointer chasing on the loop's critical path.
+__global__ void __launch_bounds__(kFbThreads)
+fb_convert_kernel(const FeedbackArgs a, int* __restrict__ hist, int* __restrict__ ticket,
+                  int bump) {
+    const long long t = hist ? *a.turn : *a.turn - 1;
+    const int S = a.S;
+    double* __restrict__ profile = const_cast<double*>(a.profile);
+    double s_sum = 0, c_sum = 0;
     const bool active = t >= a.delay;
-    const double omega = a.om[(size_t)t * nr], phi = a.ph[(size_t)t * nr];
-    if (threadIdx.x == 0) {
-        int start = 0, stop = a.S;
-        if (a.machine == BLOND_FB_SPS_F) {
-            // beam_feedback.py:326-334: window from time_offset and alpha
-            if (a.alpha != 0.0) {
-                const double lo = a.time_offset - M_PI / omega;
-                const double hi = -1 / a.alpha + a.time_offset - 2 * M_PI / omega;
-                start = fb_lower(a.bc, a.S, lo);
-                stop = max(start, fb_upper(a.bc, a.S, hi));
-            }
-        } else if (a.has_time_offset) {
-            start = fb_lower(a.bc, a.S, a.time_offset);
+    FbBins b = {};
+    if (active) b = fb_bins(a, t);
+    for (int i = blockIdx.x * kFbThreads + threadIdx.x; i < S; i += gridDim.x * kFbThreads) {
+        double x;
+        if (hist) {
+            x = (double)hist[i];
+            hist[i] = 0;
+            profile[i] = x;
+        } else {
+            x = profile[i];
         }
-        range[0] = start;
-        range[1] = stop;
-    }
-    __syncthreads();
-    const int start = range[0], stop = range[1], n = stop - start;
-    const bool weighted = a.machine != BLOND_FB_SPS_F;
-    double s_sum = 0, c_sum = 0, d_sum = 0;
-    if (active) {
-        for (int k = threadIdx.x; k < n; k += kPhaseThreads) {
-            const int i = start + k;
-            const double base = weighted ? exp(a.alpha * a.bc[i]) * a.profile[i] : a.profile[i];
-            double sn, cs;
-            sincos(omega * a.bc[i] + phi, &sn, &cs);
-            const double w = (k == 0 || k == n - 1) ? 0.5 : 1.0;
-            s_sum += w * (base * sn);
-            c_sum += w * (base * cs);
-        }
-        if (a.machine == BLOND_FB_SPS_RL)
-            for (int k = threadIdx.x; k < kFbPartials; k += kPhaseThreads) d_sum += a.partials[k];
+        if (active) fb_add(b, i, x, s_sum, c_sum);
     }
     for (int d = 16; d > 0; d >>= 1) {
         s_sum += __shfl_down_sync(0xffffffffu, s_sum, d);
         c_sum += __shfl_down_sync(0xffffffffu, c_sum, d);
-        d_sum += __shfl_down_sync(0xffffffffu, d_sum, d);
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int wpb = kFbThreads / 32;
     if (lane == 0) {
-        ss[warp] = s_sum;
-        sc[warp] = c_sum;
-        sd[warp] = d_sum;
+        a.phase_partials[2 * (blockIdx.x * wpb + warp)] = s_sum;
+        a.phase_partials[2 * (blockIdx.x * wpb + warp) + 1] = c_sum;
+        __threadfence();
     }
     __syncthreads();
-    if (threadIdx.x != 0) return;
-    s_sum = c_sum = d_sum = 0;
-    for (int w = 0; w < kPhaseThreads / 32; ++w) {
-        s_sum += ss[w];
-        c_sum += sc[w];
-        d_sum += sd[w];
+    int last = 0;
+    if (threadIdx.x == 0) last = atomicAdd(ticket, 1) == (int)gridDim.x - 1;
+    last = __syncthreads_or(last);
+    if (!last || warp != 0) return;
+    __threadfence();
+    const int parts = gridDim.x * wpb;
+    double s = 0, c = 0, dsum = 0;
+    for (int q = lane; q < parts; q += 32) {
+        s += a.phase_partials[2 * q];
+        c += a.phase_partials[2 * q + 1];
     }
-    double* st = a.state;
-    double domega = st[FBS_DOMEGA_RF];
-    if (active) {
-        if (n == 1) {
-            s_sum *= 2;
-            c_sum *= 2;
-        }
-        const double coeff = n > 0 ? (a.bin_size * s_sum) / (a.bin_size * c_sum) : nan("");
-        const double phi_beam = atan(coeff) + M_PI;
-        const double dphi = phi_beam - row[FBT_PHI_S];
-        const double om_off = omega - row[FB_COLS];  // omega_rf - omega_rf_d, main system
-        switch (a.machine) {
-        case BLOND_FB_LHC: {  // beam_feedback.py:516-565
-            const double dphi_rf = st[FBS_DPHI_RF];
-            const double la = row[FBT_LHC_A], lt = row[FBT_LHC_T];
-            domega = -a.gain * dphi - a.gain2 * (st[FBS_LHC_Y] + la * (dphi_rf + 0.0));
-            st[FBS_LHC_Y] = (1 - lt) * st[FBS_LHC_Y] + (1 - la) * lt * (dphi_rf + 0.0);
-            break;
-        }
-        case BLOND_FB_LHC_F:  // beam_feedback.py:432-458
-            domega = -a.gain * dphi - a.gain2 * (om_off + 0.0);
-            break;
-        case BLOND_FB_SPS_F:  // beam_feedback.py:460-479
-            domega = -a.gain * dphi + -a.gain2 * om_off;
-            break;
-        case BLOND_FB_SPS_RL: {  // beam_feedback.py:370-391, 481-514
-            const int64_t m = (a.n + a.sample_dE - 1) / a.sample_dE;
-            const double avg = d_sum / (double)m;
-            const double drho = row[FBT_ALPHA0] * a.ring_radius * avg /
-                                (row[FBT_BETA] * row[FBT_BETA] * row[FBT_ENERGY]);
-            const double sgn = row[FBT_ETA0] > 0 ? 1.0 : (row[FBT_ETA0] < 0 ? -1.0 : 0.0);
-            st[FBS_AVG_DE] = avg;
-            st[FBS_DRHO] = drho;
-            domega = -a.gain * dphi + -sgn * a.gain2 * (0.0 - drho) / a.ring_radius;
-            break;
-        }
-        case BLOND_FB_PSB: {  // beam_feedback.py:567-622
-            st[FBS_DPHI_SUM] += dphi;
-            const int pc = (int)st[FBS_PL_COUNTER];
-            if (pc < a.n_on_time && (double)t == a.on_time[pc] && t >= a.delay) {
-                const double prev = a.on_time[pc > 0 ? pc - 1 : a.n_on_time - 1];
-                const double av = st[FBS_DPHI_SUM] / (a.on_time[pc] - prev);
-                st[FBS_DPHI_AV] = av;
-                st[FBS_DOMEGA_PL] = 0.99803799 * st[FBS_DOMEGA_PL] +
-                                    row[FBT_GAIN] * (0.99901903 * av - 0.99901003 * st[FBS_DPHI_AV_PREV]);
-                st[FBS_DPHI_AV_PREV] = av;
-                st[FBS_DPHI_SUM] = 0.0;
-                const double g = row[FBT_GAMMA];
-                const double dr = om_off / (row[FB_COLS] * (1.0 / (row[FBT_ALPHA0] * (g * g)) - 1.0));
-                st[FBS_DR] = dr;
-                st[FBS_DOMEGA_RL] = st[FBS_DOMEGA_RL] + row[FBT_GAIN2A] * (dr - st[FBS_DR_PREV]) +
-                                    row[FBT_GAIN2B] * dr;
-                st[FBS_DR_PREV] = dr;
-                st[FBS_PL_COUNTER] = pc + 1;
-            }
-            domega = -st[FBS_DOMEGA_PL] - st[FBS_DOMEGA_RL];
-            break;
-        }
-        }
-        st[FBS_PHI_BEAM] = phi_beam;
-        st[FBS_DPHI] = dphi;
-        st[FBS_DOMEGA_RF] = domega;
-        // BeamFeedback.track: next turn's frequency of every system
-        const double* h1 = next + FB_COLS + nr;
-        for (int j = 0; j < nr; ++j) a.om[(size_t)(t + 1) * nr + j] += domega * h1[j] / h1[0];
+    if (a.machine == BLOND_FB_SPS_RL && active)
+        for (int q = lane; q < kFbPartials; q += 32) dsum += a.partials[q];
+    for (int d = 16; d > 0; d >>= 1) {
+        s += __shfl_down_sync(0xffffffffu, s, d);
+        c += __shfl_down_sync(0xffffffffu, c, d);
+        dsum += __shfl_down_sync(0xffffffffu, dsum, d);
     }
-    // RingAndRFTracker.track (tracker.py:553-565): accumulated phase offset
-    bool any = false;
-    for (int j = 0; j < nr; ++j) {
-        const double od = next[FB_COLS + j], h = next[FB_COLS + nr + j];
-        st[FBS_DPHI_RF + j] += 2.0 * M_PI * h * (a.om[(size_t)(t + 1) * nr + j] - od) / od;
-        any = any || st[FBS_DPHI_RF + j] != 0.0;
+    if (lane == 0) {
+        *ticket = 0;  // every block has taken its ticket: ready for the next turn
+        fb_turn_end(a, t, s, c, dsum);
+        if (bump) *a.turn = t + 1;
     }
-    if (any)
-        for (int j = 0; j < nr; ++j) a.ph[(size_t)(t + 1) * nr + j] += st[FBS_DPHI_RF + j];
-    if (a.trace) {
-        a.trace[t * 3 + 0] = st[FBS_PHI_BEAM];
-        a.trace[t * 3 + 1] = st[FBS_DPHI];
-        a.trace[t * 3 + 2] = st[FBS_DOMEGA_RF];
-    }
+}
+
+int convert_grid(int S) {
+    const int64_t need = ((int64_t)S + kFbThreads - 1) / kFbThreads;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(need, kFbMaxBlocks));
 }
 
 }  // namespace
 
-int launch_feedback(const FeedbackArgs& a, cudaStream_t s) {
+int launch_feedback_dE(const FeedbackArgs& a, cudaStream_t s) {
     if (a.machine == BLOND_FB_SPS_RL) {
         fb_dE_kernel<<<kFbPartials, 256, 0, s>>>(a.dE, a.dE_f32, a.n, a.sample_dE, a.partials);
         BB_LAUNCH_CHECK();
     }
-    feedback_kernel<<<1, kPhaseThreads, 0, s>>>(a);
+    return BLOND_OK;
+}
+
+int launch_feedback_dE_lik(const FeedbackArgs& a, const void* table, double bc0,
+                           double lik_inv_w, double bw, cudaStream_t s) {
+    fb_dE_lik_kernel<<<kFbPartials, 256, 0, s>>>(a.dt, a.dE, a.dE_f32, a.n, a.sample_dE, table,
+                                                 bc0, lik_inv_w, bw, a.S, a.partials);
+    BB_LAUNCH_CHECK();
+    return BLOND_OK;
+}
+
+int launch_feedback_turn(const FeedbackArgs& a, int* hist, int* ticket, int bump,
+                         cudaStream_t s) {
+    fb_convert_kernel<<<convert_grid(a.S), kFbThreads, 0, s>>>(a, hist, ticket, bump);
     BB_LAUNCH_CHECK();
     return BLOND_OK;
 }

@@ -74,9 +74,14 @@ int prepare_spectral() {
     static bool attr_done[64] = {false};
     const DeviceInfo& d = device_info();
     if (!attr_done[d.device & 63]) {
-        BB_CUDA(cudaFuncSetAttribute(spectral_kernel,
+        BB_CUDA(cudaFuncSetAttribute(spectral_kernel<false>,
                                      cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-        BB_CUDA(cudaFuncSetAttribute(spectral_kernel,
+        BB_CUDA(cudaFuncSetAttribute(spectral_kernel<false>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     d.max_smem_optin));
+        BB_CUDA(cudaFuncSetAttribute(spectral_kernel<true>,
+                                     cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        BB_CUDA(cudaFuncSetAttribute(spectral_kernel<true>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      d.max_smem_optin));
         attr_done[d.device & 63] = true;
@@ -84,7 +89,9 @@ int prepare_spectral() {
     return BLOND_OK;
 }
 
-int launch_spectral(const SpecParams& P, cudaStream_t stream) {
+template <bool FB>
+static int launch_spectral_t(const SpecParams& P, const typename SpecLoopArg<FB>::type& L,
+                             cudaStream_t stream) {
     const DeviceInfo& d = device_info();
     if (P.p.smem > d.max_smem_optin) {
         set_error("spectral: %d B of shared memory per CTA exceeds %d", P.p.smem,
@@ -105,8 +112,20 @@ int launch_spectral(const SpecParams& P, cudaStream_t stream) {
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    BB_CUDA(cudaLaunchKernelEx(&cfg, spectral_kernel, P));
+    BB_CUDA(cudaLaunchKernelEx(&cfg, spectral_kernel<FB>, P, L));
     return BLOND_OK;
+}
+
+int launch_spectral(const SpecParams& P, cudaStream_t stream) {
+    return launch_spectral_t<false>(P, SpecNoLoop{}, stream);
+}
+
+int launch_spectral_loop(const SpecParams& P, const SpecLoop& L, cudaStream_t stream) {
+    if (P.batch > 0) {
+        set_error("spectral: the beam-phase loop runs with a single profile");
+        return BLOND_ERR_UNSUPPORTED;
+    }
+    return launch_spectral_t<true>(P, L, stream);
 }
 
 __global__ void twiddle_table_kernel(const SpecPlan p, double2* out) {

@@ -31,6 +31,7 @@
 #include <cooperative_groups.h>
 
 #include "common.cuh"
+#include "feedback.cuh"
 
 namespace bb {
 
@@ -109,6 +110,19 @@ struct SpecParams {
     const double2* acc_a;
     double2* acc_g;
 };
+
+// The engine's beam-phase loop run inside the head (single profile only):
+// the load phase adds each bin's projections, the CTA that takes the last
+// ticket sums the CTAs' warp shares in order and runs the loop.  A separate
+// kernel argument, present only in spectral_kernel<true>, so that the
+// kernel without the loop is compiled exactly as before.
+struct SpecLoop {
+    int* ticket;
+    FeedbackArgs fb;
+};
+struct SpecNoLoop {};
+template <bool FB> struct SpecLoopArg { using type = SpecNoLoop; };
+template <> struct SpecLoopArg<true> { using type = SpecLoop; };
 
 // Device code below is compiled only in spectral.cu (which defines
 // BB_SPECTRAL_KERNELS); other files see the types and host entry points.
@@ -308,8 +322,9 @@ __host__ __device__ inline SpecLayout spec_layout(const SpecPlan& p) {
 // One cluster of p.C CTAs.  Column phase: CTA c owns n2 in [c Bc, (c+1) Bc),
 // element (n1, n2) at n1 * Bc + n2 - c Bc.  Row phase: CTA c owns k1 in
 // [c Br, (c+1) Br), element (k1, k2) at k2 * Br + k1 - c Br.
+template <bool FB>
 __global__ void __launch_bounds__(kSpecThreads, 1)
-spectral_kernel(const SpecParams P) {
+spectral_kernel(const SpecParams P, const typename SpecLoopArg<FB>::type LP) {
     cg::cluster_group cluster = cg::this_cluster();
     const SpecPlan& p = P.p;
     const int c = (int)cluster.block_rank();
@@ -378,6 +393,13 @@ spectral_kernel(const SpecParams P) {
     const long long turn = P.turn ? *P.turn : 0;
     double ind = 0.0;
     if (P.ind_coeff) ind = P.ind_coeff[turn];
+    bool fb_on = false;
+    double fb_s = 0, fb_c = 0;
+    FbBins fbb = {};
+    if constexpr (FB) {
+        fb_on = turn >= LP.fb.delay;
+        if (fb_on) fbb = fb_bins(LP.fb, turn);
+    }
 
     BB_PHASE(1);
     // ---- twiddle tables (computed here unless they were copied)
@@ -414,6 +436,10 @@ spectral_kernel(const SpecParams P) {
                     if (i0 < P.n_in) g_profile[i0] = x0;
                     if (i1 < P.n_in) g_profile[i1] = x1;
                 }
+                if (fb_on) {
+                    if (i0 < nlim) fb_add(fbb, (int)i0, x0, fb_s, fb_c);
+                    if (i1 < nlim) fb_add(fbb, (int)i1, x1, fb_s, fb_c);
+                }
             } else {
                 if (i0 < nlim) x0 = g_in_f64[i0];
                 if (i1 < nlim) x1 = g_in_f64[i1];
@@ -427,6 +453,7 @@ spectral_kernel(const SpecParams P) {
                 const double x = (double)g_in_i32[i];
                 g_in_i32[i] = 0;
                 if (g_profile) g_profile[i] = x;
+                if (fb_on) fb_add(fbb, (int)i, x, fb_s, fb_c);
             }
         }
         wait_twiddles();
@@ -642,6 +669,42 @@ spectral_kernel(const SpecParams P) {
             }
         }
     }
+    if constexpr (FB) {
+        // the CTAs' warp shares, then the last CTA runs this turn's loop
+        for (int d = 16; d > 0; d >>= 1) {
+            fb_s += __shfl_down_sync(0xffffffffu, fb_s, d);
+            fb_c += __shfl_down_sync(0xffffffffu, fb_c, d);
+        }
+        const int lane = tid & 31, wpb = nth >> 5;
+        if (lane == 0) {
+            LP.fb.phase_partials[2 * (c * wpb + (tid >> 5))] = fb_s;
+            LP.fb.phase_partials[2 * (c * wpb + (tid >> 5)) + 1] = fb_c;
+            __threadfence();
+        }
+        __syncthreads();
+        int last = 0;
+        if (tid == 0) last = atomicAdd(LP.ticket, 1) == p.C - 1;
+        last = __syncthreads_or(last);
+        if (last && tid < 32) {
+            __threadfence();
+            double s = 0, cc = 0, dsum = 0;
+            for (int q = lane; q < p.C * wpb; q += 32) {
+                s += LP.fb.phase_partials[2 * q];
+                cc += LP.fb.phase_partials[2 * q + 1];
+            }
+            if (LP.fb.machine == BLOND_FB_SPS_RL && fb_on)
+                for (int q = lane; q < kFbPartials; q += 32) dsum += LP.fb.partials[q];
+            for (int d = 16; d > 0; d >>= 1) {
+                s += __shfl_down_sync(0xffffffffu, s, d);
+                cc += __shfl_down_sync(0xffffffffu, cc, d);
+                dsum += __shfl_down_sync(0xffffffffu, dsum, d);
+            }
+            if (lane == 0) {
+                *LP.ticket = 0;
+                fb_turn_end(LP.fb, turn, s, cc, dsum);
+            }
+        }
+    }
     if (P.bump_turn && beam == 0 && c == 0 && tid == 0) *P.turn = turn + 1;
     BB_PHASE(10);
 }
@@ -653,6 +716,8 @@ spectral_kernel(const SpecParams P) {
 bool make_spec_plan(int64_t N, SpecPlan& plan);
 // Launch one cluster of spectral_kernel with the plan in P.
 int launch_spectral(const SpecParams& P, cudaStream_t stream);
+// The same with the engine's beam-phase loop inside (single profile).
+int launch_spectral_loop(const SpecParams& P, const SpecLoop& L, cudaStream_t stream);
 // Set spectral_kernel's launch attributes on the current device (idempotent;
 // call before a stream capture that will contain the kernel).
 int prepare_spectral();

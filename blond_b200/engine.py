@@ -242,7 +242,8 @@ class FusedTracker:
 
     def _pull_loop(self):
         """The device loop's state and the corrected RF programmes back into
-        the BeamFeedback and RFStation objects (what the host loop leaves)."""
+        the BeamFeedback and RFStation objects (what the host loop leaves);
+        part of sync()."""
         if self.loop is None:
             return
         rf, loop = self.rf, self.loop
@@ -342,7 +343,6 @@ class FusedTracker:
         self.beam.gamma = float(rf.gamma[t])
         self.beam.energy = float(rf.energy[t])
         self.beam.momentum = float(rf.momentum[t])
-        self._pull_loop()
 
     def track_host(self, host_dt: torch.Tensor, host_dE: torch.Tensor, n_turns: int = 1,
                    chunks: int = 4):
@@ -368,7 +368,6 @@ class FusedTracker:
         self.beam.gamma = float(rf.gamma[t])
         self.beam.energy = float(rf.energy[t])
         self.beam.momentum = float(rf.momentum[t])
-        self._pull_loop()
 
     def prepare(self):
         """Build and upload the CUDA graph now (otherwise the first track()
@@ -387,12 +386,13 @@ class FusedTracker:
         h, p = ct.c_double(), ct.c_double()
         self.eng.call("time_kernels", int(n_turns), ct.byref(h), ct.byref(p), _stream())
         self.rf.counter[0] += int(n_turns)
-        self._pull_loop()
         return h.value, p.value
 
     def sync(self):
         """Copy the engine's profile (and induced voltage) into the drop-in
-        objects, and the float32 energies back into beam.dE ('f32p64')."""
+        objects, the float32 energies back into beam.dE ('f32p64'), and a
+        beam-phase loop's state and corrected RF programmes into the
+        BeamFeedback and RFStation objects."""
         self.check()
         prof = torch.empty(self.profile.n_slices, dtype=torch.float64, device="cuda")
         self.eng.call("get_profile", ct.c_void_p(prof.data_ptr()), _stream())
@@ -403,6 +403,7 @@ class FusedTracker:
             self.tiv.induced_voltage = v.to(self.profile.n_macroparticles.dtype)
         if self.precision == "f32p64":
             self.beam.dE.copy_(self.dE)
+        self._pull_loop()
 
     def profile_tensor(self) -> torch.Tensor:
         prof = torch.empty(self.profile.n_slices, dtype=torch.float64, device="cuda")

@@ -292,14 +292,17 @@ int blond_engine_check(blond_engine* engine, void* stream);
 /* The beam-phase loop inside the turn: replaces BeamFeedback.track()
  * (llrf/beam_feedback.py:237-622) called by RingAndRFTracker.track()
  * (trackers/tracker.py:551-552) and the tracker's accumulation of the RF
- * phase offset (tracker.py:553-565).  After the head of turn t (turn >=
- * delay) one block measures the beam phase of the profile (beam_phase,
- * exp(alpha t)-weighted from time_offset on; SPS_F: the sharp window),
- * runs the machine's loop on device state and adds the frequency correction
+ * phase offset (tracker.py:553-565), with no host work per turn.  In turn t
+ * (turn >= delay) the beam phase of the profile is measured (beam_phase,
+ * exp(alpha t)-weighted from time_offset on; SPS_F: the sharp window), the
+ * machine's loop runs on device state and the frequency correction is added
  * to omega_rf of turn t + 1 of every RF system (times h_j / h_0); then, every
  * turn, dphi_rf += 2 pi h (omega_rf - omega_rf_d) / omega_rf_d at t + 1 and
- * phi_rf[t + 1] += dphi_rf.  SPS_RL also averages dE[::sample_dE] of the
- * bound beam (one extra pass over those particles).
+ * phi_rf[t + 1] += dphi_rf.  With an FFT impedance the measurement is part
+ * of the head kernel (its last CTA runs the loop), else one all-SM pass
+ * converts the histogram and runs it.  SPS_RL also averages dE[::sample_dE]
+ * of the bound beam (after the induced-voltage kick when there is an
+ * impedance, as the reference's main loop orders it): one extra pass.
  *   turn_table: HOST, (n_turns + 1) rows of 11 + 2 n_rf values: phi_s, eta_0,
  *     alpha_0, gamma, beta, energy, lhc_a, lhc_t, PL gain, second gain,
  *     third gain (PSB radial integral), omega_rf_d[n_rf], harmonic[n_rf].

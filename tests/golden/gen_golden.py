@@ -530,7 +530,12 @@ BF_CASES = {
                        "sample_dE": 3}, 0),
     "PSB": ("sps", {"machine": "PSB", "PL_gain": 1000.0, "RL_gain": [1e4, 1e2],
                     "period": 1e-4}, 0),
+    # with a broadband resonator (1e11 protons): induced voltage + loop per turn
+    "LHC_F_Z": ("sps", {"machine": "LHC_F", "PL_gain": 1000.0, "FL_gain": 0.05}, 0),
+    "SPS_RL_Z": ("sps", {"machine": "SPS_RL", "PL_gain": 1000.0, "RL_gain": 1e6,
+                         "sample_dE": 2}, 0),
 }
+BF_IMPEDANCE = {"LHC_F_Z", "SPS_RL_Z"}
 BF_TURNS = 200
 BF_PARTICLES = 200000
 
@@ -591,7 +596,8 @@ def gen_beam_feedback():
     out = {"names": np.array(list(BF_CASES))}
     for name, (kind, cfg, delay) in BF_CASES.items():
         ring, rf, sigma, shift = bf_machine(kind)
-        beam = Beam(ring, BF_PARTICLES, 1.2e6)
+        z = name in BF_IMPEDANCE
+        beam = Beam(ring, BF_PARTICLES, 1e11 if z else 1.2e6)
         bigaussian(ring, rf, beam, sigma, seed=1234)
         beam.dt += shift
         profile = Profile(beam, CutOptions(cut_left=0, cut_right=rf.t_rf[0, 0],
@@ -600,11 +606,21 @@ def gen_beam_feedback():
         loop = BeamFeedback(ring, rf, profile, cfg, delay=delay)
         section = RingAndRFTracker(rf, beam, profile=profile, beam_feedback=loop)
         tracker = FullRingAndRF([section])
+        tiv = None
+        if z:
+            tiv = TotalInducedVoltage(beam, profile, [InducedVoltageFreq(
+                beam, profile, [Resonators(5e6, 1e9, 1.0)])])
         trace = np.zeros((BF_TURNS, 4))
         for turn in range(BF_TURNS):
             trace[turn, 0] = np.mean(beam.dt)
-            profile.track()
-            tracker.track()
+            if z:
+                # the fused engine's order: induced kick, RF turn, slicing
+                tiv.track()
+                tracker.track()
+                profile.track()
+            else:
+                profile.track()
+                tracker.track()
             trace[turn, 1:] = (loop.phi_beam, loop.dphi, loop.domega_rf)
         out[f"{name}_trace"] = trace
         out[f"{name}_omega_rf"] = rf.omega_rf[0].copy()

@@ -11,8 +11,10 @@
   beam phase, phase error and frequency correction within 1e-9 normwise,
   the RF frequency and phase programmes within 1e-12, coordinates 1e-9.
 * The same loops inside the fused engine's turn (FusedTracker; the beam
-  phase, loop filter and RF programme correction run on the device), at the
-  same bars, tracked both turn by turn and 200 turns in one call.
+  phase, loop filter and RF programme correction run on the device, inside
+  the head kernel when there is an FFT impedance and in an all-SM pass
+  otherwise), at the same bars, tracked both turn by turn and 200 turns in
+  one call; fused.sync() brings the loop state back to the host objects.
 """
 import numpy as np
 import pytest
@@ -24,6 +26,8 @@ from blond_b200.beam.beam import Beam, Proton
 from blond_b200.beam.distributions import bigaussian
 from blond_b200.beam.profile import CutOptions, Profile
 from blond_b200.engine import FusedTracker
+from blond_b200.impedances.impedance import InducedVoltageFreq, TotalInducedVoltage
+from blond_b200.impedances.impedance_sources import Resonators
 from blond_b200.input_parameters.rf_parameters import RFStation
 from blond_b200.input_parameters.ring import Ring
 from blond_b200.llrf.beam_feedback import BeamFeedback
@@ -45,7 +49,30 @@ CASES = {
                        "sample_dE": 3}, 0),
     "PSB": ("sps", {"machine": "PSB", "PL_gain": 1000.0, "RL_gain": [1e4, 1e2],
                     "period": 1e-4}, 0),
+    # with a broadband resonator: the fused engine runs the loop inside its
+    # spectral head kernel
+    "LHC_F_Z": ("sps", {"machine": "LHC_F", "PL_gain": 1000.0, "FL_gain": 0.05}, 0),
+    "SPS_RL_Z": ("sps", {"machine": "SPS_RL", "PL_gain": 1000.0, "RL_gain": 1e6,
+                         "sample_dE": 2}, 0),
 }
+IMPEDANCE = {"LHC_F_Z", "SPS_RL_Z"}
+
+
+def setup_case(name):
+    kind, cfg, delay = CASES[name]
+    cfg = {k: (list(v) if isinstance(v, list) else v) for k, v in cfg.items()}
+    ring, rf, sigma, shift = machine(kind)
+    beam = Beam(ring, 200000, 1e11 if name in IMPEDANCE else 1.2e6)
+    bigaussian(ring, rf, beam, sigma, seed=1234)
+    beam.dt += shift
+    profile = Profile(beam, CutOptions(cut_left=0, cut_right=rf.t_rf[0, 0], n_slices=1024))
+    loop = BeamFeedback(ring, rf, profile, cfg, delay=delay)
+    tracker = RingAndRFTracker(rf, beam, profile=profile, beam_feedback=loop)
+    tiv = None
+    if name in IMPEDANCE:
+        tiv = TotalInducedVoltage(beam, profile, [InducedVoltageFreq(
+            beam, profile, [Resonators(5e6, 1e9, 1.0)])])
+    return rf, beam, profile, loop, tracker, tiv
 
 
 @pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
@@ -84,20 +111,18 @@ def machine(kind, n_turns=200):
 @pytest.mark.parametrize("name", list(CASES))
 def test_beam_feedback_tracks_reference(cuda, name):
     g = golden("beam_feedback.npz")
-    kind, cfg, delay = CASES[name]
-    cfg = {k: (list(v) if isinstance(v, list) else v) for k, v in cfg.items()}
-    ring, rf, sigma, shift = machine(kind)
-    beam = Beam(ring, 200000, 1.2e6)
-    bigaussian(ring, rf, beam, sigma, seed=1234)
-    beam.dt += shift
-    profile = Profile(beam, CutOptions(cut_left=0, cut_right=rf.t_rf[0, 0], n_slices=1024))
-    loop = BeamFeedback(ring, rf, profile, cfg, delay=delay)
-    tracker = FullRingAndRF([RingAndRFTracker(rf, beam, profile=profile, beam_feedback=loop)])
+    rf, beam, profile, loop, section, tiv = setup_case(name)
+    tracker = FullRingAndRF([section])
     trace = np.zeros((200, 4))
     for turn in range(200):
         trace[turn, 0] = float(beam.dt.mean())
-        profile.track()
-        tracker.track()
+        if tiv is not None:
+            tiv.track()
+            tracker.track()
+            profile.track()
+        else:
+            profile.track()
+            tracker.track()
         trace[turn, 1:] = (loop.phi_beam, loop.dphi, loop.domega_rf)
     want = g[f"{name}_trace"]
     for col in range(4):
@@ -108,36 +133,27 @@ def test_beam_feedback_tracks_reference(cuda, name):
     assert normwise(beam.dE.cpu().numpy()[::997], g[f"{name}_dE"]) < 1e-9
 
 
-def setup_case(name):
-    kind, cfg, delay = CASES[name]
-    cfg = {k: (list(v) if isinstance(v, list) else v) for k, v in cfg.items()}
-    ring, rf, sigma, shift = machine(kind)
-    beam = Beam(ring, 200000, 1.2e6)
-    bigaussian(ring, rf, beam, sigma, seed=1234)
-    beam.dt += shift
-    profile = Profile(beam, CutOptions(cut_left=0, cut_right=rf.t_rf[0, 0], n_slices=1024))
-    loop = BeamFeedback(ring, rf, profile, cfg, delay=delay)
-    tracker = RingAndRFTracker(rf, beam, profile=profile, beam_feedback=loop)
-    return rf, beam, profile, loop, tracker
 
 
 @pytest.mark.parametrize("name", list(CASES))
 def test_fused_beam_feedback_matches_reference(cuda, name):
     g = golden("beam_feedback.npz")
-    rf, beam, profile, loop, tracker = setup_case(name)
-    fused = FusedTracker(tracker, profile, None, precision="f64")
+    rf, beam, profile, loop, tracker, tiv = setup_case(name)
+    fused = FusedTracker(tracker, profile, tiv, precision="f64")
     want = g[f"{name}_trace"]
-    if name in ("LHC", "PSB"):
+    if name in ("LHC", "PSB", "SPS_RL_Z"):
         # turn by turn: the loop state round-trips through the host objects
         mean_dt = np.zeros(200)
         trace = np.zeros((200, 3))
         for turn in range(200):
             mean_dt[turn] = float(beam.dt.mean())
             fused.track(1)
+            fused.sync()
             trace[turn] = (loop.phi_beam, loop.dphi, loop.domega_rf)
         assert normwise(mean_dt, want[:, 0]) < 1e-9
     else:
         fused.track(200)
+        fused.sync()
         trace = fused.loop_trace[:200]
         assert (loop.phi_beam, loop.dphi, loop.domega_rf) == tuple(trace[-1])
     for col in range(3):
@@ -155,8 +171,10 @@ def test_fused_beam_feedback_f32p64_follows_f64(cuda):
     200 turns."""
     out = {}
     for prec in ("f64", "f32p64"):
-        rf, beam, profile, loop, tracker = setup_case("LHC_F")
-        FusedTracker(tracker, profile, None, precision=prec).track(200)
+        rf, beam, profile, loop, tracker, _ = setup_case("LHC_F")
+        fused = FusedTracker(tracker, profile, None, precision=prec)
+        fused.track(200)
+        fused.sync()
         out[prec] = rf.omega_rf[0].copy() - rf.omega_rf_d[0]
     assert np.all(np.isfinite(out["f32p64"]))
     assert normwise(out["f32p64"], out["f64"]) < 1e-3
