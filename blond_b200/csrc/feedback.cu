@@ -105,36 +105,49 @@ fb_dE_kernel(const void* dE, int f32, int64_t n, int sample, double* partials) {
 }
 
 // Sum of dE[k * sample_dE] after this turn's interpolated kick, computed
-// as the particle pass computes it (same table, same expression).
+// as the particle pass computes it (same table, same expression).  Four
+// sampled particles per iteration with their loads issued first: the table
+// gather depends on dt, and a chain per particle would leave the pass
+// latency-bound.
+template <typename E>
+__device__ __forceinline__ void lik_apply(double t, E& e, const void* table, double bc0,
+                                          double lik_inv_w, double bw, int S) {
+    const double f = floor((t - bc0) * lik_inv_w);
+    if (!(f >= 0.0 && f < (double)(S - 1))) return;
+    const int q = (int)f;
+    if constexpr (sizeof(E) == 8) {
+        const double2 tb = __ldg(reinterpret_cast<const double2*>(table) + q);
+        e += t * tb.x + tb.y;
+    } else {
+        const float2 tb = __ldg(reinterpret_cast<const float2*>(table) + q);
+        const float x = (float)(t - (bc0 + (double)q * bw));
+        e += __fmaf_rn(tb.y, x, tb.x);
+    }
+}
+
+template <typename E>
 __global__ void __launch_bounds__(256)
-fb_dE_lik_kernel(const double* dt, const void* dE, int f32, int64_t n, int sample,
+fb_dE_lik_kernel(const double* __restrict__ dt, const E* __restrict__ dE, int64_t n, int sample,
                  const void* table, double bc0, double lik_inv_w, double bw, int S,
                  double* partials) {
     const int64_t m = (n + sample - 1) / sample;
+    const int64_t G = (int64_t)gridDim.x * blockDim.x;
     double acc = 0.0;
-    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < m;
-         k += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t i = k * sample;
-        const double t = dt[i];
-        const double f = floor((t - bc0) * lik_inv_w);
-        const bool in = f >= 0.0 && f < (double)(S - 1);
-        const int q = in ? (int)f : 0;
-        if (!f32) {
-            double e = static_cast<const double*>(dE)[i];
-            if (in) {
-                const double2 tb = __ldg(reinterpret_cast<const double2*>(table) + q);
-                e += t * tb.x + tb.y;
-            }
-            acc += e;
-        } else {
-            float e = static_cast<const float*>(dE)[i];
-            if (in) {
-                const float2 tb = __ldg(reinterpret_cast<const float2*>(table) + q);
-                const float x = (float)(t - (bc0 + (double)q * bw));
-                e += __fmaf_rn(tb.y, x, tb.x);
-            }
-            acc += (double)e;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < m; k += 4 * G) {
+        double t[4];
+        E e[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int64_t idx = k + u * G;
+            t[u] = idx < m ? dt[idx * sample] : 0.0;
+            e[u] = idx < m ? dE[idx * sample] : E(0);
         }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (k + u * G < m) lik_apply(t[u], e[u], table, bc0, lik_inv_w, bw, S);
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (k + u * G < m) acc += (double)e[u];
     }
     __shared__ double sh[8];
     for (int d = 16; d > 0; d >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, d);
@@ -228,8 +241,14 @@ int launch_feedback_dE(const FeedbackArgs& a, cudaStream_t s) {
 
 int launch_feedback_dE_lik(const FeedbackArgs& a, const void* table, double bc0,
                            double lik_inv_w, double bw, cudaStream_t s) {
-    fb_dE_lik_kernel<<<kFbPartials, 256, 0, s>>>(a.dt, a.dE, a.dE_f32, a.n, a.sample_dE, table,
-                                                 bc0, lik_inv_w, bw, a.S, a.partials);
+    if (a.dE_f32)
+        fb_dE_lik_kernel<float><<<kFbPartials, 256, 0, s>>>(
+            a.dt, static_cast<const float*>(a.dE), a.n, a.sample_dE, table, bc0, lik_inv_w,
+            bw, a.S, a.partials);
+    else
+        fb_dE_lik_kernel<double><<<kFbPartials, 256, 0, s>>>(
+            a.dt, static_cast<const double*>(a.dE), a.n, a.sample_dE, table, bc0, lik_inv_w,
+            bw, a.S, a.partials);
     BB_LAUNCH_CHECK();
     return BLOND_OK;
 }

@@ -51,7 +51,7 @@ struct FeedbackArgs {
     int64_t n_turns;
 };
 
-constexpr int kFbPartials = 296;   // blocks of the dE reduction (2 per SM on B200)
+constexpr int kFbPartials = 1184;  // blocks of the dE reductions (8 per SM on B200)
 constexpr int kFbThreads = 256;    // threads per block of the convert kernel
 constexpr int kFbMaxBlocks = 148;  // at most one block per SM
 constexpr int kFbMaxParts = 1024;  // warp partials of the beam phase (phase_partials / 2)
