@@ -49,6 +49,7 @@ def _sig(real):
         "linear_interp_kick": [P, P, P, P, real, c_int, c_i64, real, P],
         "beam_phase": [P, P, real, real, real, real, c_int, P, P],
         "beam_phase_fast": [P, P, real, real, real, c_int, P, P],
+        "beam_statistics": [P, P, P, c_i64, P, P, P, P],
     }
 
 

@@ -70,9 +70,10 @@ class Beam:
         else:
             assert n == len(dE)
             self.dE = _to_device(dE, dtype)
-        self.mean_dt = self.mean_dE = 0.0
-        self.sigma_dt = self.sigma_dE = 0.0
-        self.epsn_rms_l = 0.0
+        self._stats_host = dict.fromkeys(_STAT_NAMES, 0.0)
+        self._stats_dev = None      # device results of the last statistics()
+        self._stats_pending = False
+        self._stats_work = None     # scratch and ticket of the reduction
         self.n_macroparticles_eliminated = 0
         self._id = None
 
@@ -95,14 +96,45 @@ class Beam:
         return int(torch.count_nonzero(self._id))
 
     def statistics(self):
-        """Mean and rms of the alive particles (beam.py:430-458)."""
-        if self._id is None:
-            dt, dE = self.dt.double(), self.dE.double()
-        else:
-            alive = self._id != 0
-            dt, dE = self.dt[alive].double(), self.dE[alive].double()
-        self.mean_dt = float(dt.mean())
-        self.sigma_dt = float(dt.std(unbiased=False))
-        self.mean_dE = float(dE.mean())
-        self.sigma_dE = float(dE.std(unbiased=False))
-        self.epsn_rms_l = float(np.pi * self.sigma_dE * self.sigma_dt)
+        """Mean and rms of the alive particles (beam.py:430-458) by one
+        device reduction (blond_beam_statistics); nothing waits for it:
+        mean_dt, sigma_dt, mean_dE, sigma_dE, epsn_rms_l are read back when
+        first used.  stats_tensor() gives the device results."""
+        if self._stats_work is None:
+            self._stats_dev = torch.full((8,), float("nan"), dtype=torch.float64,
+                                         device=self.dt.device)
+            self._stats_work = (torch.empty(bm.STATS_SCRATCH, dtype=torch.float64,
+                                            device=self.dt.device),
+                                torch.zeros(1, dtype=torch.int32, device=self.dt.device))
+        dt, dE = self.dt, self.dE
+        if dE.dtype != dt.dtype:
+            dE = dE.to(dt.dtype)
+        bm.beam_statistics(dt, dE, self._id, out=self._stats_dev,
+                           scratch=self._stats_work[0], ticket=self._stats_work[1])
+        self._stats_pending = True
+
+    def stats_tensor(self):
+        """The device results of the last statistics(): [n_alive, mean_dt,
+        sigma_dt, mean_dE, sigma_dE, epsn_rms_l, sum dt^2, sum dE^2]."""
+        return self._stats_dev
+
+    def _stat(self, name):
+        if self._stats_pending:
+            v = self._stats_dev.cpu().numpy()
+            for k, x in zip(_STAT_NAMES, v[1:]):
+                self._stats_host[k] = float(x)
+            self._stats_pending = False
+        return self._stats_host[name]
+
+    def _set_stat(self, name, value):
+        self._stat(name)  # settle pending device results first
+        self._stats_host[name] = value
+
+
+# attribute names Beam.statistics sets (beam.py:444-458), in the order of
+# the device results after n_alive
+_STAT_NAMES = ("mean_dt", "sigma_dt", "mean_dE", "sigma_dE", "epsn_rms_l",
+               "_mpi_sumsq_dt", "_mpi_sumsq_dE")
+for _name in _STAT_NAMES:
+    setattr(Beam, _name, property(lambda self, n=_name: self._stat(n),
+                                  lambda self, v, n=_name: self._set_stat(n, v)))

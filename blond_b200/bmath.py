@@ -22,7 +22,7 @@ __all__ = [
     "kick", "drift", "slice_beam", "slice_smooth", "linear_interp_kick",
     "rf_volt_comp", "fast_resonator", "rfft", "irfft", "rfftfreq",
     "induced_voltage_1turn", "interp", "resonator_induced_voltage", "beam_phase",
-    "beam_phase_fast",
+    "beam_phase_fast", "beam_statistics",
     "resonator_induced_voltage_1_turn", "resonator_workspace",
     "precision", "use_precision", "B200Backend",
 ]
@@ -277,6 +277,34 @@ def beam_phase_fast(bin_centers, profile, omega_rf, phi_rf, bin_size, *,
     if device_result or not isinstance(out, torch.Tensor):
         return out
     return float(out.item())
+
+
+# ------------------------------------------------------------ statistics
+STATS_SCRATCH = 7 * 1024  # BLOND_STATS_SCRATCH
+
+
+def beam_statistics(dt, dE, id=None, out=None, scratch=None, ticket=None):
+    """Beam.statistics (beam.py:430-458) on the device: an 8-element float64
+    tensor [n_alive, mean_dt, sigma_dt, mean_dE, sigma_dE, epsn_rms_l,
+    sum dt^2, sum dE^2] over the particles with id != 0.  No
+    synchronisation; pass the same out / scratch / ticket every call to
+    reuse them (out carries the previous means as the sums' shift)."""
+    if dt.dtype != dE.dtype:
+        raise TypeError("dt and dE must have the same dtype")
+    dev = dt.device
+    if out is None:
+        out = torch.full((8,), float("nan"), dtype=torch.float64, device=dev)
+    if scratch is None:
+        scratch = torch.empty(STATS_SCRATCH, dtype=torch.float64, device=dev)
+    if ticket is None:
+        ticket = torch.zeros(1, dtype=torch.int32, device=dev)
+    idp = None
+    if id is not None:
+        id = id.to(torch.int64).contiguous()
+        idp = _ptr(id)
+    _lib.call(f"blond_beam_statistics_{_suffix(dt)}", _ptr(dt), _ptr(dE), idp, dt.numel(),
+              _ptr(out), _ptr(scratch), _ptr(ticket), _stream())
+    return out
 
 
 # ------------------------------------------------------ time-domain wakes

@@ -138,6 +138,24 @@ int blond_beam_phase_fast_f32(const float* bin_centers, const float* profile,
                               float omega_rf, float phi_rf, float bin_size,
                               int n_bins, float* coeff, void* stream);
 
+/* ------------------------------------------------------------ beam statistics
+ * replaces Beam.statistics() beam/beam.py:430-458 (numpy mean / std over the
+ * particles with id != 0; id may be NULL: all alive).  Writes 8 doubles to
+ * the device array stats: n_alive, mean_dt, sigma_dt, mean_dE, sigma_dE,
+ * epsn_rms_l = pi sigma_dE sigma_dt, sum dt^2, sum dE^2.  stats also holds the
+ * previous call's means, used as the shift of the one-pass sums (NaN or
+ * zeros are fine on the first call).  scratch: BLOND_STATS_SCRATCH doubles,
+ * ticket: one int that must be 0 before the first call (it is 0 again after
+ * every call); calls sharing them must not overlap on the device. */
+#define BLOND_STATS_MAX_BLOCKS 1024
+#define BLOND_STATS_SCRATCH (7 * BLOND_STATS_MAX_BLOCKS)
+int blond_beam_statistics_f64(const double* dt, const double* dE,
+                              const int64_t* id, int64_t n, double* stats,
+                              double* scratch, int* ticket, void* stream);
+int blond_beam_statistics_f32(const float* dt, const float* dE,
+                              const int64_t* id, int64_t n, double* stats,
+                              double* scratch, int* ticket, void* stream);
+
 /* ------------------------------------------------------------ impedance setup
  * replaces fast_resonator_real_imag() cpp_routines/fast_resonator.cpp:19-74
  * re/im accumulate (+= / -=); index 0 (DC) is untouched. */
