@@ -26,18 +26,32 @@ stats_kernel(const T* __restrict__ dt, const T* __restrict__ dE,
     if (!isfinite(sdt)) sdt = 0.0;
     if (!isfinite(sdE)) sdE = 0.0;
     double v[kStatVals] = {0, 0, 0, 0, 0, 0, 0};
-    for (int64_t i = blockIdx.x * (int64_t)kStatThreads + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * kStatThreads) {
-        if (id && id[i] == 0) continue;
-        const double x = (double)dt[i], y = (double)dE[i];
-        const double a = x - sdt, b = y - sdE;
-        v[0] += 1.0;
-        v[1] += a;
-        v[2] += a * a;
-        v[3] += b;
-        v[4] += b * b;
-        v[5] += x * x;
-        v[6] += y * y;
+    // four elements per iteration, all loads issued before the arithmetic
+    const int64_t G = (int64_t)gridDim.x * kStatThreads;
+    for (int64_t i0 = blockIdx.x * (int64_t)kStatThreads + threadIdx.x; i0 < n; i0 += 4 * G) {
+        T x[4], y[4];
+        bool keep[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int64_t i = i0 + u * G;
+            keep[u] = i < n;
+            x[u] = keep[u] ? dt[i] : T(0);
+            y[u] = keep[u] ? dE[i] : T(0);
+            if (id && keep[u]) keep[u] = id[i] != 0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (!keep[u]) continue;
+            const double xd = (double)x[u], yd = (double)y[u];
+            const double a = xd - sdt, b = yd - sdE;
+            v[0] += 1.0;
+            v[1] += a;
+            v[2] += a * a;
+            v[3] += b;
+            v[4] += b * b;
+            v[5] += xd * xd;
+            v[6] += yd * yd;
+        }
     }
     __shared__ double sh[kStatThreads / 32][kStatVals];
     __shared__ bool last;
@@ -58,11 +72,28 @@ stats_kernel(const T* __restrict__ dt, const T* __restrict__ dE,
     __syncthreads();
     if (threadIdx.x == 0) last = atomicAdd(ticket, 1) == (int)gridDim.x - 1;
     __syncthreads();
-    if (!last || threadIdx.x != 0) return;
+    if (!last) return;
     __threadfence();
+    // the last block combines the partials: thread k sums blocks k, k + 256,
+    // ..., then a fixed tree over the threads (the same order every call)
     double t[kStatVals] = {0, 0, 0, 0, 0, 0, 0};
-    for (int b = 0; b < (int)gridDim.x; ++b)
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += kStatThreads)
+#pragma unroll
         for (int q = 0; q < kStatVals; ++q) t[q] += part[(size_t)b * kStatVals + q];
+#pragma unroll
+    for (int q = 0; q < kStatVals; ++q) {
+        double x = t[q];
+        for (int d = 16; d > 0; d >>= 1) x += __shfl_down_sync(0xffffffffu, x, d);
+        if (lane == 0) sh[warp][q] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+#pragma unroll
+    for (int q = 0; q < kStatVals; ++q) {
+        double x = 0.0;
+        for (int w = 0; w < kStatThreads / 32; ++w) x += sh[w][q];
+        t[q] = x;
+    }
     *ticket = 0;
     const double cnt = t[0];
     const double m1 = t[1] / cnt, m3 = t[3] / cnt;
@@ -90,7 +121,7 @@ int stats_impl(const T* dt, const T* dE, const int64_t* id, int64_t n, double* s
                  "beam_statistics: misaligned array");
     const DeviceInfo& d = device_info();
     int64_t grid = (n + kStatThreads - 1) / kStatThreads;
-    grid = grid < (int64_t)d.sm_count * 4 ? grid : (int64_t)d.sm_count * 4;
+    grid = grid < (int64_t)d.sm_count * 8 ? grid : (int64_t)d.sm_count * 8;
     if (grid > BLOND_STATS_MAX_BLOCKS) grid = BLOND_STATS_MAX_BLOCKS;
     stats_kernel<T><<<(int)grid, kStatThreads, 0, as_stream(stream)>>>(dt, dE, id, n, stats,
                                                                       scratch, ticket);
