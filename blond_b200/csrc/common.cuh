@@ -81,6 +81,15 @@ inline int particle_grid(int64_t n, int threads, int blocks_per_sm,
 
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
+// Programmatic dependent launch (sm_90+): let the grid launched after this
+// one on the stream start (it still waits in pdl_wait), and wait for the
+// grid before this one to complete and flush its memory.  Both are no-ops
+// for a launch without programmatic stream serialization.
+__device__ __forceinline__ void pdl_launch_dependents() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // ------------------------------------------------------ device utilities
 template <typename T> struct Vec2;
 template <> struct Vec2<double> { using type = double2; };

@@ -318,6 +318,17 @@ particle_kernel(const ParticleArgs a) {
     using E2 = typename Vec2<E>::type;
     extern __shared__ __align__(16) int sh[];
     __shared__ TurnConsts c;
+    // launched with programmatic serialization (the engine's turn): the
+    // next turn's head may launch now and set itself up; this block clears
+    // its histogram, then waits for the head (turn counter, RF programme,
+    // table, cleared global histogram) before reading anything it wrote
+    pdl_launch_dependents();
+    // profiles too long for a shared-memory copy deposit straight into
+    // the global histogram
+    int* const hd = a.global_hist ? a.hist : sh;
+    if (!a.global_hist)
+        for (int k = threadIdx.x; k < a.S; k += blockDim.x) sh[k] = 0;
+    pdl_wait();
     long long t_idx = a.turn ? (*a.turn - 1) : 0;
     if (t_idx < 0) t_idx = 0;
     if (t_idx >= a.n_turns) t_idx = a.n_turns - 1;
@@ -333,11 +344,6 @@ particle_kernel(const ParticleArgs a) {
             c.d = a.drift[t_idx + 1];
         }
     }
-    // profiles too long for a shared-memory copy deposit straight into
-    // the global histogram
-    int* const hd = a.global_hist ? a.hist : sh;
-    if (!a.global_hist)
-        for (int k = threadIdx.x; k < a.S; k += blockDim.x) sh[k] = 0;
     __syncthreads();
 
     double* dt = reinterpret_cast<double*>(a.dt);
@@ -666,6 +672,9 @@ struct blond_engine {
     int hist_mode = -1;  // -1 automatic, else HIST_AGG/I32/PACKED/GLOBAL
     int ring = 0;        // plain pass: prefetch ring stages (0 = direct loads)
     int cluster = 1;     // plain pass: blocks whose histograms merge on chip
+    // programmatic dependent launch between the turn's head and particle
+    // pass: each kernel lets the next one launch and set up early
+    bool pdl = true;
     // host-buffer pipeline (blond_engine_track_host): copy streams and one
     // (in, done, out) event triple per chunk
     cudaStream_t io_in = nullptr, io_out = nullptr;
@@ -883,13 +892,22 @@ static int launch_particles_t(blond_engine* e, const ParticleArgs& a, cudaStream
         cfg.blockDim = dim3(e->threads, 1, 1);
         cfg.dynamicSmemBytes = smem_ring;
         cfg.stream = s;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeClusterDimension;
-        attr[0].val.clusterDim.x = cl;
-        attr[0].val.clusterDim.y = 1;
-        attr[0].val.clusterDim.z = 1;
+        cudaLaunchAttribute attr[2];
+        int na = 0;
+        if (cl > 1) {
+            attr[na].id = cudaLaunchAttributeClusterDimension;
+            attr[na].val.clusterDim.x = cl;
+            attr[na].val.clusterDim.y = 1;
+            attr[na].val.clusterDim.z = 1;
+            ++na;
+        }
+        if (e->pdl) {
+            attr[na].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+            attr[na].val.programmaticStreamSerializationAllowed = 1;
+            ++na;
+        }
         cfg.attrs = attr;
-        cfg.numAttrs = cl > 1 ? 1 : 0;
+        cfg.numAttrs = na;
         BB_CUDA(cudaLaunchKernelEx(&cfg, k, a));
     }
     BB_LAUNCH_CHECK();
@@ -1029,6 +1047,7 @@ static int launch_spectral_head(blond_engine* e, cudaStream_t s, bool loop) {
     SpecParams P = {};
     P.p = e->plan;
     P.mode = SPEC_FORWARD | SPEC_MULTIPLY | SPEC_INVERSE;
+    P.pdl = e->pdl ? 1 : 0;
     P.in_i32 = e->d_hist;
     P.n_in = e->S;
     P.profile_out = e->d_profile;

@@ -105,13 +105,15 @@ static int launch_spectral_t(const SpecParams& P, const typename SpecLoopArg<FB>
     cfg.blockDim = dim3(kSpecThreads, 1, 1);
     cfg.dynamicSmemBytes = P.p.smem;
     cfg.stream = stream;
-    cudaLaunchAttribute attr[1];
+    cudaLaunchAttribute attr[2];
     attr[0].id = cudaLaunchAttributeClusterDimension;
     attr[0].val.clusterDim.x = P.p.C;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
+    attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[1].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
-    cfg.numAttrs = 1;
+    cfg.numAttrs = P.pdl ? 2 : 1;
     BB_CUDA(cudaLaunchKernelEx(&cfg, spectral_kernel<FB>, P, L));
     return BLOND_OK;
 }

@@ -109,6 +109,10 @@ struct SpecParams {
     // P_t the profile spectrum and L_t the spectrum of this input
     const double2* acc_a;
     double2* acc_g;
+    // launch with programmatic stream serialization (the engine's turn):
+    // the kernel triggers its dependents at entry and waits for the grid
+    // before it before reading the histogram or the turn counter
+    int pdl;
 };
 
 // The engine's beam-phase loop run inside the head (single profile only):
@@ -326,6 +330,7 @@ template <bool FB>
 __global__ void __launch_bounds__(kSpecThreads, 1)
 spectral_kernel(const SpecParams P, const typename SpecLoopArg<FB>::type LP) {
     cg::cluster_group cluster = cg::this_cluster();
+    pdl_launch_dependents();  // the particle pass may launch and set up now
     const SpecPlan& p = P.p;
     const int c = (int)cluster.block_rank();
     const int tid = threadIdx.x, nth = blockDim.x;
@@ -390,6 +395,7 @@ spectral_kernel(const SpecParams P, const typename SpecLoopArg<FB>::type LP) {
         }
         asm volatile("cp.async.commit_group;" ::: "memory");
     }
+    pdl_wait();  // the previous grid's histogram, counter and programme
     const long long turn = P.turn ? *P.turn : 0;
     double ind = 0.0;
     if (P.ind_coeff) ind = P.ind_coeff[turn];
