@@ -281,15 +281,65 @@ __device__ __forceinline__ void cluster_flush(int* sh, int* hist, int S) {
 // 512, so 256-, 512- and 1024-thread launches all use the same code.
 constexpr int kEngineThreads = 1024;
 
+// The particle arrays stream through L2 once per turn (hundreds of MB
+// against a 126 MB L2).  Their loads and stores carry an L2 evict-first
+// policy, so they are the lines replaced first and the head kernel's code,
+// twiddles, impedance and the interpolation table stay in L2 from one turn
+// to the next (C2, FP64: 99.8 -> 94.2 us per turn, the head 30.5 -> 27 us).
+__device__ __forceinline__ uint64_t evict_first_policy() {
+    uint64_t pol;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
 // Per-thread asynchronous copies into shared memory (cp.async, 16 or 8
 // bytes): the prefetch ring of the plain pass.
-__device__ __forceinline__ void ring_copy16(void* smem, const void* gmem) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
-                     (uint32_t)__cvta_generic_to_shared(smem)), "l"(gmem) : "memory");
+__device__ __forceinline__ void ring_copy16(void* smem, const void* gmem, uint64_t pol) {
+    asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;" ::"r"(
+                     (uint32_t)__cvta_generic_to_shared(smem)), "l"(gmem), "l"(pol) : "memory");
 }
-__device__ __forceinline__ void ring_copy8(void* smem, const void* gmem) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(
-                     (uint32_t)__cvta_generic_to_shared(smem)), "l"(gmem) : "memory");
+__device__ __forceinline__ void ring_copy8(void* smem, const void* gmem, uint64_t pol) {
+    asm volatile("cp.async.ca.shared.global.L2::cache_hint [%0], [%1], 8, %2;" ::"r"(
+                     (uint32_t)__cvta_generic_to_shared(smem)), "l"(gmem), "l"(pol) : "memory");
+}
+__device__ __forceinline__ void stream_store(double2* p, double2 v, uint64_t pol) {
+    asm volatile("st.global.L2::cache_hint.v2.f64 [%0], {%1, %2}, %3;" ::"l"(p), "d"(v.x),
+                 "d"(v.y), "l"(pol) : "memory");
+}
+__device__ __forceinline__ void stream_store(float2* p, float2 v, uint64_t pol) {
+    asm volatile("st.global.L2::cache_hint.v2.f32 [%0], {%1, %2}, %3;" ::"l"(p), "f"(v.x),
+                 "f"(v.y), "l"(pol) : "memory");
+}
+__device__ __forceinline__ void stream_store(double* p, double v, uint64_t pol) {
+    asm volatile("st.global.L2::cache_hint.f64 [%0], %1, %2;" ::"l"(p), "d"(v), "l"(pol)
+                 : "memory");
+}
+__device__ __forceinline__ void stream_store(float* p, float v, uint64_t pol) {
+    asm volatile("st.global.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(p), "f"(v), "l"(pol)
+                 : "memory");
+}
+__device__ __forceinline__ double2 stream_load(const double2* p, uint64_t pol) {
+    double2 v;
+    asm volatile("ld.global.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;"
+                 : "=d"(v.x), "=d"(v.y) : "l"(p), "l"(pol) : "memory");
+    return v;
+}
+__device__ __forceinline__ float2 stream_load(const float2* p, uint64_t pol) {
+    float2 v;
+    asm volatile("ld.global.L2::cache_hint.v2.f32 {%0, %1}, [%2], %3;"
+                 : "=f"(v.x), "=f"(v.y) : "l"(p), "l"(pol) : "memory");
+    return v;
+}
+__device__ __forceinline__ double stream_load(const double* p, uint64_t pol) {
+    double v;
+    asm volatile("ld.global.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol)
+                 : "memory");
+    return v;
+}
+__device__ __forceinline__ float stream_load(const float* p, uint64_t pol) {
+    float v;
+    asm volatile("ld.global.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol)
+                 : "memory");
+    return v;
 }
 __device__ __forceinline__ void ring_commit() {
     asm volatile("cp.async.commit_group;" ::: "memory");
@@ -354,17 +404,18 @@ particle_kernel(const ParticleArgs a) {
     // whole warps iterate together (needed by __match_any_sync)
     const int lane = threadIdx.x & 31;
     int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31);
+    const uint64_t pol = evict_first_policy();
     if (NST == 0) {
         for (; base < npairs; base += stride) {
             const int64_t p = base + lane;
             int b0 = -1, b1 = -1;
             if (p < npairs) {
-                double2 tt = reinterpret_cast<const double2*>(dt)[p];
-                E2 ee = reinterpret_cast<const E2*>(dE)[p];
+                double2 tt = stream_load(reinterpret_cast<const double2*>(dt) + p, pol);
+                E2 ee = stream_load(reinterpret_cast<const E2*>(dE) + p, pol);
                 if (KICK) track_pair<PREC, SOLVER, LIK>(tt.x, tt.y, ee.x, ee.y, c, a, order);
                 if (KICK) {
-                    reinterpret_cast<double2*>(dt)[p] = tt;
-                    reinterpret_cast<E2*>(dE)[p] = ee;
+                    stream_store(reinterpret_cast<double2*>(dt) + p, tt, pol);
+                    stream_store(reinterpret_cast<E2*>(dE) + p, ee, pol);
                 }
                 b0 = engine_bin(tt.x, a.cut_left, a.inv_w, a.S);
                 b1 = engine_bin(tt.y, a.cut_left, a.inv_w, a.S);
@@ -381,9 +432,9 @@ particle_kernel(const ParticleArgs a) {
         const E2* gdE = reinterpret_cast<const E2*>(dE);
         auto fill = [&](int slot, int64_t p) {
             if (p < npairs) {
-                ring_copy16(&rdt[slot * blockDim.x + threadIdx.x], &gdt[p]);
-                if (sizeof(E2) == 16) ring_copy16(&rdE[slot * blockDim.x + threadIdx.x], &gdE[p]);
-                else ring_copy8(&rdE[slot * blockDim.x + threadIdx.x], &gdE[p]);
+                ring_copy16(&rdt[slot * blockDim.x + threadIdx.x], &gdt[p], pol);
+                if (sizeof(E2) == 16) ring_copy16(&rdE[slot * blockDim.x + threadIdx.x], &gdE[p], pol);
+                else ring_copy8(&rdE[slot * blockDim.x + threadIdx.x], &gdE[p], pol);
             }
             ring_commit();  // one group per stage, empty past the end
         };
@@ -401,8 +452,8 @@ particle_kernel(const ParticleArgs a) {
                 double2 tt = rdt[slot * blockDim.x + threadIdx.x];
                 E2 ee = rdE[slot * blockDim.x + threadIdx.x];
                 track_pair<PREC, SOLVER, LIK>(tt.x, tt.y, ee.x, ee.y, c, a, order);
-                reinterpret_cast<double2*>(dt)[p] = tt;
-                reinterpret_cast<E2*>(dE)[p] = ee;
+                stream_store(reinterpret_cast<double2*>(dt) + p, tt, pol);
+                stream_store(reinterpret_cast<E2*>(dE) + p, ee, pol);
                 b0 = engine_bin(tt.x, a.cut_left, a.inv_w, a.S);
                 b1 = engine_bin(tt.y, a.cut_left, a.inv_w, a.S);
             }
@@ -452,11 +503,11 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
                  : "memory");
 }
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes,
-                                         uint64_t* bar) {
+                                         uint64_t* bar, uint64_t pol) {
     asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-            smem_u32(dst)),
-        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint "
+        "[%0], [%1], %2, [%3], %4;" ::"r"(smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(pol)
         : "memory");
 }
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
@@ -522,12 +573,13 @@ particle_kernel_tma(const ParticleArgs a, int* err) {
     const long long mine = nchunks > blockIdx.x
                                ? (nchunks - 1 - blockIdx.x) / gridDim.x + 1 : 0;
     const uint32_t bytes_dt = sizeof(double) * kTile, bytes_dE = sizeof(E) * kTile;
+    const uint64_t pol = evict_first_policy();
     auto issue = [&](long long i) {
         const int s = (int)(i % nst);
         const long long chunk = blockIdx.x + i * gridDim.x;
         mbar_expect_tx(&full[s], bytes_dt + bytes_dE);
-        bulk_g2s(st_dt + (size_t)s * kTile, dt + chunk * kTile, bytes_dt, &full[s]);
-        bulk_g2s(st_dE + (size_t)s * kTile, dE + chunk * kTile, bytes_dE, &full[s]);
+        bulk_g2s(st_dt + (size_t)s * kTile, dt + chunk * kTile, bytes_dt, &full[s], pol);
+        bulk_g2s(st_dE + (size_t)s * kTile, dE + chunk * kTile, bytes_dE, &full[s], pol);
     };
     if (threadIdx.x == 0)
         for (long long i = 0; i < mine && i < nst; ++i) issue(i);
@@ -546,8 +598,8 @@ particle_kernel_tma(const ParticleArgs a, int* err) {
                 double2 tt = sdt[p];
                 E2 ee = sdE[p];
                 track_pair<PREC, SOLVER, LIK>(tt.x, tt.y, ee.x, ee.y, c, a, order);
-                reinterpret_cast<double2*>(dt + base)[p] = tt;
-                reinterpret_cast<E2*>(dE + base)[p] = ee;
+                stream_store(reinterpret_cast<double2*>(dt + base) + p, tt, pol);
+                stream_store(reinterpret_cast<E2*>(dE + base) + p, ee, pol);
                 block_deposit<HIST>(sh, half, a.hist, engine_bin(tt.x, a.cut_left, a.inv_w, a.S));
                 block_deposit<HIST>(sh, half, a.hist, engine_bin(tt.y, a.cut_left, a.inv_w, a.S));
             }
@@ -2064,6 +2116,7 @@ particle_kernel_batch(const BatchArgs a) {
     double* dt = reinterpret_cast<double*>(a.dt);
     E* dE = reinterpret_cast<E*>(a.dE);
     const int S = a.S;
+    const uint64_t pol = evict_first_policy();
     for (int ch = blockIdx.x; ch < a.n_chunks; ch += gridDim.x) {
         const int b = a.chunk_beam[ch];
         const long long start = a.chunk_start[ch];
@@ -2106,8 +2159,8 @@ particle_kernel_batch(const BatchArgs a) {
             for (int q = 0; q < 4; ++q) {
                 in[q] = i + q * bd < count;
                 const long long g = start + i + (in[q] ? q * bd : 0);
-                t[q] = dt[g];
-                e[q] = dE[g];
+                t[q] = stream_load(dt + g, pol);
+                e[q] = stream_load(dE + g, pol);
             }
             if (KICK) {
                 track_pair<PREC, SOLVER, LIK>(t[0], t[1], e[0], e[1], c, pa, a.order);
@@ -2115,8 +2168,8 @@ particle_kernel_batch(const BatchArgs a) {
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
                     if (in[q]) {
-                        dt[start + i + q * bd] = t[q];
-                        dE[start + i + q * bd] = e[q];
+                        stream_store(dt + start + i + q * bd, t[q], pol);
+                        stream_store(dE + start + i + q * bd, e[q], pol);
                     }
                 }
             }
