@@ -99,15 +99,26 @@ def window(centre, S):
 
 # ----------------------------------------------------------------- clocks
 class ClockSampler:
-    """nvidia-smi samples (200 ms) during the timed region."""
+    """SM clock and clock-event reasons during the timed region.  NVML is
+    polled about every millisecond from a host thread (the timed region of
+    the default run lasts ~20 ms); without NVML, nvidia-smi samples every
+    200 ms instead."""
 
     Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, device_index: int):
         self.rows = []
         self.proc = None
+        self.nvml = None
+        self.halt = threading.Event()
+        try:
+            self._start_nvml(device_index)
+            return
+        except Exception:  # no NVML: fall back to nvidia-smi
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
@@ -118,11 +129,56 @@ class ClockSampler:
         except (OSError, FileNotFoundError):
             self.proc = None
 
+    def _start_nvml(self, device_index):
+        import pynvml as nv
+        import torch
+        nv.nvmlInit()
+        try:  # the CUDA device's own GPU, whatever CUDA_VISIBLE_DEVICES says
+            h = nv.nvmlDeviceGetHandleByUUID(
+                "GPU-" + str(torch.cuda.get_device_properties(device_index).uuid))
+        except Exception:
+            h = nv.nvmlDeviceGetHandleByIndex(device_index)
+        self.nvml, self.h = nv, h
+        self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+        self.bits = [nv.nvmlClocksEventReasonHwSlowdown,
+                     nv.nvmlClocksEventReasonHwThermalSlowdown,
+                     nv.nvmlClocksEventReasonSwThermalSlowdown,
+                     nv.nvmlClocksEventReasonSwPowerCap]
+        self._sample()  # fails here, not in the thread, if NVML cannot read
+        self.t = threading.Thread(target=self._poll, daemon=True)
+        self.t.start()
+
+    def _sample(self):
+        nv, h = self.nvml, self.h
+        mhz = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+        r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+        self.rows.append((mhz, [bool(r & b) for b in self.bits]))
+
+    def _poll(self):
+        while not self.halt.is_set():
+            try:
+                self._sample()
+            except Exception:
+                return
+            time.sleep(0.001)
+
     def _read(self):
         for line in self.proc.stdout:
             self.rows.append([x.strip() for x in line.split(",")])
 
     def stop(self):
+        if self.nvml is not None:
+            self.halt.set()
+            self.t.join(timeout=5)
+            try:
+                self._sample()  # the state at the end of the timed region
+            except Exception:
+                pass
+            rows = self.rows
+            reasons = sorted({self.NAMES[i] for _, f in rows for i in range(4) if f[i]})
+            return {"sm_mhz": statistics.median(m for m, _ in rows),
+                    "sm_max_mhz": self.max_mhz, "reasons": reasons,
+                    "samples": len(rows), "source": "NVML, ~1 ms polling"}
         if self.proc is None:
             return None
         time.sleep(0.25)
@@ -135,13 +191,11 @@ class ClockSampler:
         if not rows:
             return None
         sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
-                 "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4)
+        reasons = sorted({self.NAMES[i] for r in rows for i in range(4)
                           if r[3 + i].lower() == "active"})
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": float(rows[0][1]) if rows[0][1].replace(".", "").isdigit() else None,
-                "reasons": reasons, "samples": len(rows)}
+                "reasons": reasons, "samples": len(rows), "source": "nvidia-smi, 200 ms"}
 
 
 # ----------------------------------------------------------------- CPU path

@@ -77,3 +77,36 @@ def test_spectral_plan_factorisation_covers_next_regular_lengths():
 def test_normwise_helper():
     assert normwise([1.0, 2.0], [1.0, 2.0]) == 0.0
     assert np.isclose(normwise([1.0, 2.2], [1.0, 2.0]), 0.1)
+
+
+def test_bench_clock_sampler_reads_nvml(monkeypatch):
+    """bench.py's clock record through a fake NVML: polled samples, the
+    median SM clock, and the reasons decoded from the event-reason bits."""
+    import os
+    import sys
+    import time
+    import types
+    fake = types.ModuleType("pynvml")
+    fake.NVML_CLOCK_SM = 1
+    fake.nvmlClocksEventReasonHwSlowdown = 0x8
+    fake.nvmlClocksEventReasonHwThermalSlowdown = 0x40
+    fake.nvmlClocksEventReasonSwThermalSlowdown = 0x20
+    fake.nvmlClocksEventReasonSwPowerCap = 0x4
+    fake.nvmlInit = lambda: None
+    def by_uuid(u):
+        raise RuntimeError("no such GPU")
+    fake.nvmlDeviceGetHandleByUUID = by_uuid
+    fake.nvmlDeviceGetHandleByIndex = lambda i: ("gpu", i)
+    fake.nvmlDeviceGetMaxClockInfo = lambda h, c: 1965
+    fake.nvmlDeviceGetClockInfo = lambda h, c: 1800
+    fake.nvmlDeviceGetCurrentClocksEventReasons = lambda h: 0x4 | 0x1
+    monkeypatch.setitem(sys.modules, "pynvml", fake)
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+    c = bench.ClockSampler(0)
+    time.sleep(0.02)
+    r = c.stop()
+    assert r["samples"] >= 3
+    assert r["sm_mhz"] == 1800.0 and r["sm_max_mhz"] == 1965.0
+    assert r["reasons"] == ["sw_power_cap"]
+    assert r["source"].startswith("NVML")
