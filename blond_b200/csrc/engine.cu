@@ -929,7 +929,6 @@ static int plain_ring_smem(const blond_engine* e, int ring) {
 template <int PREC, int SOLVER, bool LIK, bool KICK>
 static int launch_particles_t(blond_engine* e, const ParticleArgs& a, cudaStream_t s,
                               bool launch) {
-    static bool done_agg[64] = {false}, done_plain[64] = {false};
     const int smem = engine_smem(e);
     const bool agg = plain_agg(e);
     int rc;
@@ -954,8 +953,6 @@ static int launch_particles_t(blond_engine* e, const ParticleArgs& a, cudaStream
     grid = (grid + cl - 1) / cl * cl;
     const int ring = KICK ? e->ring : 0;
     auto k = plain_kernel<PREC, SOLVER, LIK, KICK>(agg, ring);
-    (void)done_agg;
-    (void)done_plain;
     if ((rc = allow_smem_once(k))) return rc;
     const int smem_ring = plain_ring_smem<PREC>(e, ring);
     if (smem_ring < 0) {
