@@ -10,7 +10,7 @@
  * array they pass.
  *
  * The bmath-level entry points mirror the reference's libblond exports
- * (blond/cpp_routines/*.cpp, bound by blond/utils/butils_wrap_cpp.py) with
+ * (the .cpp files of blond/cpp_routines, bound by blond/utils/butils_wrap_cpp.py) with
  * the same argument order and meaning; _f64 corresponds to
  * libblond_double.so and _f32 to libblond_single.so (blond_common.h:22-36).
  */
