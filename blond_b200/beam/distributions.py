@@ -11,8 +11,6 @@ import warnings
 import numpy as np
 import torch
 
-from .. import bmath as bm
-
 
 def _get_dE_from_dt(ring, rf_station, dt_amplitude: float) -> float:
     """Single-harmonic Hamiltonian dE amplitude (distributions.py:1367-1430)."""
