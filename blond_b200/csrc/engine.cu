@@ -458,7 +458,7 @@ particle_kernel(const ParticleArgs a) {
             // F32P64: thread 0 also prefetches into L2 the block's slice one
             // iteration beyond the ring, so each SM has twice the bytes in
             // flight without more shared memory (C2: particle pass 58.4 ->
-            // 54.0 us; for FP64 it cost 1.5 us, so it is left out there)
+            // 54.0 us; FP64 lost ~2 us a turn with it, so it is F32P64 only)
             if (PREC == PREC_F32P64 && threadIdx.x == 0) {
                 const int64_t pb = base + (int64_t)NST * stride;
                 if (pb < npairs) {
