@@ -36,7 +36,7 @@ UNIT = "particle-turns/s"
 WORKLOAD = ("1e7 protons 26 GeV/c, h=4620 4.5 MV, 2^14 slices, broadband "
             "resonator 5 MOhm/1 GHz/Q=1 via FFT (n_fft 16384), lik + kick + "
             "drift + slice per turn")
-BYTES_PER_PARTICLE = {"f64": 32, "f32p64": 24}  # read + write of dt and dE
+BYTES_PER_PARTICLE = {"f64": 32, "f32p64": 24, "q32p64": 24}  # read + write of dt and dE
 E2E_CHUNKS = 4
 
 
@@ -48,11 +48,15 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--particles", type=float, default=1e7)
     ap.add_argument("--slices", type=int, default=16384)
-    ap.add_argument("--precision", default="f64", choices=["f64", "f32p64"])
+    ap.add_argument("--precision", default="f64", choices=["f64", "f32p64", "q32p64"])
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="leave the C3 batch out of the default line")
+    ap.add_argument("--batched-error-turns", type=int, default=1000,
+                    help="turns after which the batched forms' rms errors are taken")
     ap.add_argument("--kernel", default="auto", choices=["auto", "tma", "plain"])
     ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5", "mtw"],
                     help="c2: the single-beam pipeline (default, the headline); "
@@ -418,17 +422,51 @@ def run_ours(args, world, rank, local):
     if rank == 0 and world == 1 and not args.no_mixed and args.precision == "f64":
         del fused, beam
         torch.cuda.empty_cache()
-        fm, bm_, _ = build_fused(n, S, W + K + kt + 4, "f32p64", args.kernel, shape=shape)
-        fm.track(W)
-        fm.prepare()
-        ms32 = time_turns(fm, K)
-        h32, p32 = fm.time_kernels(kt)
-        ach32 = BYTES_PER_PARTICLE["f32p64"] * n / (p32 / kt * 1e-3) / 1e9
-        out["mixed_precision"] = {"dtype": "f32p64", "value": n * K / (ms32 * 1e-3),
-                                  "ms_per_step": ms32 / K, "kernel_ms": p32 / kt,
-                                  "achieved_gbs": ach32, "frac": ach32 / peak,
-                                  "autotuned": fm.tuned}
-        del fm, bm_
+        for prec, key in (("f32p64", "mixed_precision"), ("q32p64", "fixed_point")):
+            fm, bm_, _ = build_fused(n, S, W + K + kt + 4, prec, args.kernel, shape=shape)
+            fm.track(W)
+            fm.prepare()
+            ms32 = time_turns(fm, K)
+            h32, p32 = fm.time_kernels(kt)
+            fm.check()
+            ach32 = BYTES_PER_PARTICLE[prec] * n / (p32 / kt * 1e-3) / 1e9
+            out[key] = {"dtype": prec, "value": n * K / (ms32 * 1e-3),
+                        "ms_per_step": ms32 / K, "kernel_ms": p32 / kt,
+                        "head_kernel_ms": h32 / kt,
+                        "achieved_gbs": ach32, "frac": ach32 / peak,
+                        "autotuned": fm.tuned}
+            del fm, bm_
+            torch.cuda.empty_cache()
+    if rank == 0 and world == 1 and not args.no_batched:
+        if "fused" in locals():
+            del fused, beam
+        torch.cuda.empty_cache()
+        T = max(args.batched_error_turns, W + K)
+        m = c3_measure(256, W, K, T, control=False)
+        q, f32, f64 = (m["runs"][k] for k in ("q32p64", "f32p64", "f64"))
+        nt = m["n_total"]
+        pp = q["autotuned"]["particle_pass_ms"]
+        eq, ef = m["errors"]["q32p64"], m["errors"]["f32p64"]
+        out["batched"] = {
+            "workload": C3_WORKLOAD, "beams": 256, "particles_total": nt,
+            "dtype": "q32p64", "value": q["value"], "unit": UNIT,
+            "ms_per_step": q["ms_per_step"], "steps": K,
+            "particle_pass_ms": pp,
+            "achieved_gbs": 24 * nt / (pp * 1e-3) / 1e9,
+            "frac": 24 * nt / (pp * 1e-3) / 1e9 / peak,
+            "turn_level_gbs": 24 * nt / (q["ms_per_step"] * 1e-3) / 1e9,
+            "ratio_to_plain_f64_value": q["value"] / value,
+            "rel_err_turns": m["turns"],
+            "rel_err_statistic": "in-window rms bunch length and energy spread per beam "
+                                 "vs the FP64 batch",
+            "beams_within_1e-5": int(np.sum(eq.max(axis=1) <= 1e-5)),
+            "max_rel_err": float(eq.max()),
+            "autotuned": q["autotuned"],
+            "f32p64": {"value": f32["value"], "ms_per_step": f32["ms_per_step"],
+                       "beams_within_1e-5": int(np.sum(ef.max(axis=1) <= 1e-5)),
+                       "max_rel_err": float(ef.max())},
+            "f64": {"value": f64["value"], "ms_per_step": f64["ms_per_step"]},
+        }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, turns, kind, cores, sec = cpu_reference(n, S, None, args.cpu_seconds)
         out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cores, "kind": kind,
@@ -643,72 +681,93 @@ def ct_stream():
     return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
 
 
-def run_c3(args):
-    """Batched F32P64 and FP64 vs every beam through its own FP64 engine
-    (the unbatched plain path), with the F32P64 error per beam."""
+def _c3_rel_errs(beams, other, ref):
+    """Per beam: relative error of the in-window rms bunch length and
+    energy spread of `other` against `ref` (both BatchTrackers)."""
+    out = []
+    for k, (_, _, p, _) in enumerate(beams):
+        x = (ref.coordinates(k)[0].cpu().numpy(), ref.energies(k).cpu().numpy())
+        y = (other.coordinates(k)[0].cpu().numpy(), other.energies(k).cpu().numpy())
+        w = (x[0] > p.cut_left) & (x[0] < p.cut_right)
+        out.append([abs(np.std(v[w]) / np.std(u[w]) - 1) for u, v in zip(x, y)])
+    return np.array(out)
+
+
+def _err_summary(errs):
+    return {"sigma_dt_median": float(np.median(errs[:, 0])),
+            "sigma_dt_p90": float(np.percentile(errs[:, 0], 90)),
+            "sigma_dt_max": float(errs[:, 0].max()),
+            "sigma_dE_median": float(np.median(errs[:, 1])),
+            "sigma_dE_p90": float(np.percentile(errs[:, 1], 90)),
+            "sigma_dE_max": float(errs[:, 1].max()),
+            "beams_within_1e-5": int(np.sum(errs.max(axis=1) <= 1e-5))}
+
+
+def c3_measure(n_beams, W, K, T_err, precisions=("q32p64", "f32p64", "f64"),
+               control=True, unbatched=False):
+    """C3: every precision batched (autotuned launch shape, graph-replayed
+    turns), timed over K turns after W, then tracked on (untimed) to turn
+    T_err, where each form's per-beam rms errors against FP64 are taken.
+    control: FP64 again from initial times moved by one ulp -- how far the
+    dynamics alone separate two runs that differ by rounding.  unbatched:
+    every beam through its own FP64 engine, one after the other."""
     import torch
     from blond_b200.batch import BatchTracker
     from blond_b200.engine import FusedTracker
     from blond_b200.trackers.tracker import RingAndRFTracker
-    W, K = max(3, args.warmup), args.steps
-    T_err = max(1000, W + K)  # turns after which the precision is compared
-    beams = c3_beams(args.beams, T_err + W + K + 4)
+    beams = c3_beams(n_beams, T_err + W + K + 4)
     n_total = sum(b.n_macroparticles for _, b, _, _ in beams)
-    res = {}
-    for prec in ("f32p64", "f64"):
+    res, trackers = {}, {}
+    for prec in precisions:
         bt = BatchTracker([(RingAndRFTracker(rf, b), p, t) for rf, b, p, t in beams],
                           precision=prec)
+        shape = bt.autotune()
         bt.track(W)
         bt.prepare()
         ms = time_turns(bt, K)
         bt.track(T_err - W - K)  # untimed, to the comparison turn
-        res[prec] = (n_total * K / (ms * 1e-3), ms / K, bt)
+        bt.check()
+        res[prec] = {"value": n_total * K / (ms * 1e-3), "ms_per_step": ms / K,
+                     "autotuned": shape}
+        trackers[prec] = bt
         for rf, _, _, _ in beams:
             rf.counter[0] = 0
-    # control: FP64 again from initial times moved by one ulp -- how far the
-    # dynamics alone separate two runs that differ by rounding
-    bp = BatchTracker([(RingAndRFTracker(rf, b), p, t) for rf, b, p, t in beams],
-                      precision="f64")
-    bp.dt.copy_(torch.nextafter(bp.dt, torch.full_like(bp.dt, float("inf"))))
-    bp._call("slice", ct_stream())
-    bp.track(T_err)
-    for rf, _, _, _ in beams:
-        rf.counter[0] = 0
-
-    # F32P64 (and the control) vs FP64 after W + K turns: rms bunch length /
-    # energy spread of the particles in the window
-    def rel_errs(other, ref):
-        out = []
-        for k, (_, _, p, _) in enumerate(beams):
-            x = [t.double().cpu().numpy() for t in ref.coordinates(k)]
-            y = [t.double().cpu().numpy() for t in other.coordinates(k)]
-            w = (x[0] > p.cut_left) & (x[0] < p.cut_right)
-            out.append([abs(np.std(v[w]) / np.std(u[w]) - 1) for u, v in zip(x, y)])
-        return np.array(out)
-
-    b32, b64 = res["f32p64"][2], res["f64"][2]
-    errs = rel_errs(b32, b64)
-    floor = rel_errs(bp, b64)
-    vals = {p: (res[p][0], res[p][1]) for p in res}
-    del b32, b64, bp, res
+    out = {"n_total": n_total, "turns": T_err, "runs": res}
+    if "f64" in trackers:
+        for prec in precisions:
+            if prec != "f64":
+                out.setdefault("errors", {})[prec] = _c3_rel_errs(
+                    beams, trackers[prec], trackers["f64"])
+        if control:
+            bp = BatchTracker([(RingAndRFTracker(rf, b), p, t) for rf, b, p, t in beams],
+                              precision="f64")
+            bp.dt.copy_(torch.nextafter(bp.dt, torch.full_like(bp.dt, float("inf"))))
+            bp._call("slice", ct_stream())
+            bp.track(T_err)
+            for rf, _, _, _ in beams:
+                rf.counter[0] = 0
+            out["control"] = _c3_rel_errs(beams, bp, trackers["f64"])
+            del bp
+    del trackers
     torch.cuda.empty_cache()
-    # the unbatched plain path: every beam through its own FP64 engine
-    engines = [FusedTracker(RingAndRFTracker(rf, b), p, t, precision="f64",
-                            turns_per_graph=K) for rf, b, p, t in beams]
-    for e in engines:
-        e.track(W)
-        e.prepare()
-    torch.cuda.synchronize()
-    s = torch.cuda.current_stream()
-    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    a.record(s)
-    for e in engines:
-        e.track(K)
-    b.record(s)
-    torch.cuda.synchronize()
-    ms_plain = a.elapsed_time(b)
-    plain = n_total * K / (ms_plain * 1e-3)
-    return vals, plain, ms_plain / K, errs, floor, n_total, T_err
+    if unbatched:
+        engines = [FusedTracker(RingAndRFTracker(rf, b), p, t, precision="f64",
+                                turns_per_graph=K) for rf, b, p, t in beams]
+        for e in engines:
+            e.track(W)
+            e.prepare()
+        torch.cuda.synchronize()
+        s = torch.cuda.current_stream()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s)
+        for e in engines:
+            e.track(K)
+        b.record(s)
+        torch.cuda.synchronize()
+        ms_plain = a.elapsed_time(b)
+        out["unbatched_f64"] = {"value": n_total * K / (ms_plain * 1e-3),
+                                "ms_per_step": ms_plain / K}
+    return out
 
 
 C5_WORKLOAD = ("1e8 protons 26 GeV/c, double RF h=4620/18480 4.5/0.45 MV (phi 0/pi), "
@@ -1058,36 +1117,30 @@ def main():
         return
     if args.workload == "c3" and args.impl == "ours":
         W, K = max(3, args.warmup), args.steps
-        vals, plain, ms_plain, errs, floor, n_total, T_err = run_c3(args)
+        m = c3_measure(args.beams, W, K, max(1000, W + K), unbatched=True)
+        q = m["runs"]["q32p64"]
+        peak = _peaks().get("hbm_gbs") or 6650.0
         print(json.dumps({
-            "metric": METRIC, "value": vals["f32p64"][0], "unit": UNIT, "n_gpus": 1,
-            "steps": K, "warmup": W, "ms_per_step": vals["f32p64"][1],
+            "metric": METRIC, "value": q["value"], "unit": UNIT, "n_gpus": 1,
+            "steps": K, "warmup": W, "ms_per_step": q["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32p64", "data": "synthetic",
+            "dtype": "q32p64", "data": "synthetic",
             "config": {"workload": C3_WORKLOAD, "beams": args.beams,
-                       "particles_total": n_total, "slices": 512, "n_fft": 512},
-            "batched_f64": {"value": vals["f64"][0], "ms_per_step": vals["f64"][1]},
-            "unbatched_plain_f64": {"value": plain, "ms_per_step": ms_plain},
-            "speedup_f32p64_batched_vs_unbatched_f64": vals["f32p64"][0] / plain,
-            "f32p64_rel_err_after_turns": {
-                "turns": T_err,
-                "statistic": "in-window rms of dt and dE, per beam, F32P64 vs FP64 batch",
-                "sigma_dt_median": float(np.median(errs[:, 0])),
-                "sigma_dt_p90": float(np.percentile(errs[:, 0], 90)),
-                "sigma_dt_max": float(errs[:, 0].max()),
-                "sigma_dE_median": float(np.median(errs[:, 1])),
-                "sigma_dE_p90": float(np.percentile(errs[:, 1], 90)),
-                "sigma_dE_max": float(errs[:, 1].max()),
-                "beams_within_1e-5": int(np.sum(errs.max(axis=1) <= 1e-5)),
-                "control_fp64_one_ulp": {
-                    "statistic": "the same, FP64 from initial dt moved by one ulp vs FP64",
-                    "sigma_dt_median": float(np.median(floor[:, 0])),
-                    "sigma_dt_p90": float(np.percentile(floor[:, 0], 90)),
-                    "sigma_dE_median": float(np.median(floor[:, 1])),
-                    "sigma_dE_p90": float(np.percentile(floor[:, 1], 90)),
-                    "beams_within_1e-5": int(np.sum(floor.max(axis=1) <= 1e-5))},
-                "beams_f32p64_within_1e-5_or_control": int(np.sum(
-                    errs.max(axis=1) <= np.maximum(1e-5, 2 * floor.max(axis=1))))},
+                       "particles_total": m["n_total"], "slices": 512, "n_fft": 512},
+            "runs": {k: {**v, "particle_pass_gbs": 24 * m["n_total"] /
+                         (v["autotuned"]["particle_pass_ms"] * 1e-3) / 1e9
+                         if k != "f64" else 32 * m["n_total"] /
+                         (v["autotuned"]["particle_pass_ms"] * 1e-3) / 1e9}
+                     for k, v in m["runs"].items()},
+            "hbm_peak_gbs": peak,
+            "unbatched_plain_f64": m["unbatched_f64"],
+            "speedup_q32p64_batched_vs_unbatched_f64":
+                q["value"] / m["unbatched_f64"]["value"],
+            "rel_err_after_turns": {
+                "turns": m["turns"],
+                "statistic": "in-window rms of dt and dE, per beam, vs the FP64 batch",
+                **{k: _err_summary(v) for k, v in m["errors"].items()},
+                "control_fp64_one_ulp": _err_summary(m["control"])},
             "gpu_launches": 2 * K,
         }), flush=True)
         return

@@ -26,6 +26,7 @@ OK = 0
 ERR_NAMES = {
     1: "invalid argument", 2: "size out of range", 3: "misaligned pointer",
     4: "CUDA error", 5: "unsupported", 6: "timeout", 7: "bad state",
+    8: "fixed-point energy out of range",
 }
 
 
@@ -87,11 +88,16 @@ _EXTRA = {
     "blond_batch_tune": [c_ptr, c_int],
     "blond_batch_get_profiles": [c_ptr, c_ptr, c_ptr],
     "blond_batch_get_induced_voltages": [c_ptr, c_ptr, c_ptr],
+    "blond_batch_set_energy_units": [c_ptr, c_ptr],
+    "blond_batch_check": [c_ptr, c_ptr],
+    "blond_batch_set_shape": [c_ptr, c_int, c_int, c_int, c_int, c_int],
+    "blond_batch_autotune": [c_ptr, c_int, c_ptr, ct.POINTER(c_int), ct.POINTER(c_dbl)],
     "blond_engine_bind_histogram": [c_ptr, c_ptr],
     "blond_engine_step": [c_ptr, c_int, c_ptr],
     "blond_engine_get_profile": [c_ptr, c_ptr, c_ptr],
     "blond_engine_get_induced_voltage": [c_ptr, c_ptr, c_ptr],
     "blond_engine_get_turn": [c_ptr, ct.POINTER(c_i64)],
+    "blond_engine_set_energy_unit": [c_ptr, c_dbl],
     "blond_engine_tune": [c_ptr, c_int, c_int, c_int],
     "blond_engine_set_histogram": [c_ptr, c_int],
     "blond_engine_set_prefetch": [c_ptr, c_int],
@@ -101,9 +107,9 @@ _EXTRA = {
     "blond_engine_time_kernels": [c_ptr, c_i64, ct.POINTER(c_dbl),
                                   ct.POINTER(c_dbl), c_ptr],
     "blond_turn_f64_noalloc": [c_ptr, c_ptr, c_i64, c_int, c_dbl, c_ptr, c_ptr, c_ptr,
-                               c_dbl, c_int] + [c_dbl] * 13 + [c_int, c_ptr, c_ptr,
-                                                              c_i64, c_dbl, c_ptr,
-                                                              c_ptr, c_ptr],
+                               c_dbl, c_int] + [c_dbl] * 13 + [c_int, c_ptr, c_i64,
+                                                              c_dbl, c_ptr, c_ptr,
+                                                              c_ptr],
     "blond_adjoint_deposit": [c_ptr, c_i64, c_int, c_dbl, c_dbl, c_ptr, c_ptr],
     "blond_adjoint_forward_turn": [c_int, c_ptr, c_ptr, c_ptr, c_ptr, c_i64, c_int,
                                    c_ptr, c_ptr, c_ptr, c_dbl, c_dbl, c_dbl, c_ptr,

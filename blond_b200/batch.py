@@ -23,7 +23,7 @@ import torch
 from scipy.constants import e
 
 from . import _lib
-from .engine import PREC, SOLVER, _host
+from .engine import PREC, SOLVER, _host, default_energy_unit, to_fixed
 from .impedances.impedance import InducedVoltageFreq, InducedVoltageTime
 
 
@@ -36,9 +36,12 @@ def _stream():
 
 
 class BatchTracker:
-    def __init__(self, items, precision: str = "f32p64", turns_per_graph: int = 50):
+    def __init__(self, items, precision: str = "f32p64", turns_per_graph: int = 50,
+                 energy_units=None):
         """items: list of (RingAndRFTracker, Profile, TotalInducedVoltage or
-        None), one per beam."""
+        None), one per beam.  'q32p64' stores each beam's energies as int32
+        counts of its own unit (energy_units, eV; by default 1.5 max|dE| of
+        the beam over the 2^31 - 1 counts of the grid)."""
         if precision not in PREC:
             raise ValueError(f"precision must be one of {list(PREC)}")
         self.items = list(items)
@@ -111,11 +114,22 @@ class BatchTracker:
         # coordinates of all beams, concatenated on the device
         counts = [b.n_macroparticles for b in beams]
         self.offsets = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
-        edtype = torch.float64 if precision == "f64" else torch.float32
         self.dt = torch.cat([b.dt.to(torch.float64) for b in beams]).contiguous()
-        self.dE = torch.cat([b.dE.to(edtype) for b in beams]).contiguous()
+        self.energy_units = None
+        if precision == "q32p64":
+            units = (list(energy_units) if energy_units is not None
+                     else [default_energy_unit(b.dE) for b in beams])
+            if len(units) != B:
+                raise ValueError("one energy unit per beam")
+            self.energy_units = np.ascontiguousarray(units, dtype=np.float64)
+            self.dE = torch.cat([to_fixed(b.dE, u) for b, u in zip(beams, units)]).contiguous()
+            self._call("set_energy_units", _p(self.energy_units))
+        else:
+            edtype = torch.float64 if precision == "f64" else torch.float32
+            self.dE = torch.cat([b.dE.to(edtype) for b in beams]).contiguous()
         self._call("bind_beams", ct.c_void_p(self.dt.data_ptr()),
                    ct.c_void_p(self.dE.data_ptr()), _p(self.offsets))
+        self.shape = None
         self._call("set_turn", int(rfs[0].counter[0]), _stream())
         self._call("slice", _stream())
 
@@ -136,6 +150,30 @@ class BatchTracker:
         least turns_per_graph turns builds it)."""
         self._call("prepare", _stream())
 
+    def set_shape(self, threads: int = 512, blocks_per_sm: int = 2,
+                  particles_per_thread: int = 4, chunk: int = 32768,
+                  aggregate: bool = False):
+        """Fix the particle pass's launch shape (blond_batch_set_shape)."""
+        self._call("set_shape", int(threads), int(blocks_per_sm), int(particles_per_thread),
+                   int(chunk), 1 if aggregate else 0)
+
+    def autotune(self, reps: int = 3) -> dict:
+        """Time every launch shape of the particle pass on these beams and
+        keep the fastest (blond_batch_autotune); the coordinates are left
+        as they were.  Returns the choice."""
+        cfg = (ct.c_int * 6)()
+        ms = ct.c_double()
+        self._call("autotune", int(reps), _stream(), cfg, ct.byref(ms))
+        self.shape = {"threads": cfg[0], "blocks_per_sm": cfg[1],
+                      "particles_per_thread": cfg[2], "chunk": cfg[3],
+                      "aggregate": bool(cfg[4]), "candidates": cfg[5],
+                      "particle_pass_ms": ms.value}
+        return self.shape
+
+    def check(self):
+        """Synchronise and raise if a fixed-point energy left its grid."""
+        self._call("check", _stream())
+
     def track(self, n_turns: int = 1):
         self._call("run", int(n_turns), _stream())
         for rf, beam in zip(self.rfs, self.beams):
@@ -155,9 +193,17 @@ class BatchTracker:
         return out
 
     def coordinates(self, b: int):
-        """(dt, dE) device views of beam b inside the batch arrays."""
+        """(dt, dE) device views of beam b inside the batch arrays (dE in
+        the engine's storage type)."""
         o0, o1 = int(self.offsets[b]), int(self.offsets[b + 1])
         return self.dt[o0:o1], self.dE[o0:o1]
+
+    def energies(self, b: int) -> torch.Tensor:
+        """Beam b's energies in eV as a float64 device tensor."""
+        dE = self.coordinates(b)[1].to(torch.float64)
+        if self.precision == "q32p64":
+            dE = dE * float(self.energy_units[b])
+        return dE
 
     def sync(self):
         """Copy coordinates, profiles and induced voltages back into the
@@ -165,9 +211,8 @@ class BatchTracker:
         prof = self.profiles_tensor()
         vind = self.induced_voltages_tensor() if self.tivs[0] is not None else None
         for b, (beam, p, v) in enumerate(zip(self.beams, self.profiles, self.tivs)):
-            dt, dE = self.coordinates(b)
-            beam.dt.copy_(dt)
-            beam.dE.copy_(dE)
+            beam.dt.copy_(self.coordinates(b)[0])
+            beam.dE.copy_(self.energies(b))
             p.n_macroparticles.copy_(prof[b])
             if v is not None:
                 v.induced_voltage = vind[b].to(p.n_macroparticles.dtype)

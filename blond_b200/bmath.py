@@ -431,8 +431,7 @@ def resonator_induced_voltage_1_turn(kappa1, n_macroparticles, bin_centers, bin_
 
 class B200Backend:
     """The hot-path subset of blond's MasterBackend attribute contract
-    (bmath_backends.py:61-201), backed by libblond_b200.  See
-    INTEGRATION.md for installing it into a reference ``bm`` object."""
+    (bmath_backends.py:61-201), backed by libblond_b200."""
 
     device = "GPU_B200"
 

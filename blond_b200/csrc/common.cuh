@@ -94,6 +94,7 @@ __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;"
 template <typename T> struct Vec2;
 template <> struct Vec2<double> { using type = double2; };
 template <> struct Vec2<float> { using type = float2; };
+template <> struct Vec2<int> { using type = int2; };
 
 __device__ __forceinline__ double dev_sin(double x) { return sin(x); }
 __device__ __forceinline__ float dev_sin(float x) { return sinf(x); }

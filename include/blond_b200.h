@@ -32,6 +32,7 @@ extern "C" {
 #define BLOND_ERR_UNSUPPORTED 5      /* e.g. an FFT length with a prime factor > 5 */
 #define BLOND_ERR_TIMEOUT 6          /* a bounded device-side wait gave up */
 #define BLOND_ERR_STATE 7            /* engine used before it was configured */
+#define BLOND_ERR_RANGE 8            /* a fixed-point energy left its 32-bit grid */
 
 /* drift solvers, as butils_wrap_cpp.drift maps them (butils_wrap_cpp.py:920-925) */
 #define BLOND_SOLVER_SIMPLE 0
@@ -42,6 +43,10 @@ extern "C" {
 #define BLOND_PREC_F64 0    /* dt, dE float64; all arithmetic float64 (plain) */
 #define BLOND_PREC_F32P64 1 /* dt float64, dE float32; RF phase argument and
                                drift in float64, kick arithmetic in float32 */
+#define BLOND_PREC_Q32P64 2 /* dt float64, dE int32 counts of a per-beam energy
+                               unit (set_energy_unit); kick and drift
+                               arithmetic in float64, the energy rounded to
+                               the unit once per turn */
 
 const char* blond_b200_last_error(void);
 int blond_b200_version(void);
@@ -290,9 +295,16 @@ int blond_engine_set_impedance(blond_engine* engine, int64_t n_fft,
 int blond_engine_set_inductive(blond_engine* engine, const double* z_over_n,
                                double scale);
 /* dt/dE: device arrays of n macro-particles in the engine's precision
- * (F64: both double; F32P64: dt double, dE float). */
+ * (F64: both double; F32P64: dt double, dE float; Q32P64: dt double, dE
+ * int32 counts of the energy unit). */
 int blond_engine_bind_beam(blond_engine* engine, void* dt, void* dE,
                            int64_t n);
+/* No counterpart in the reference (its energies are floating point).
+ * Q32P64 only, required before tracking: eV per count of the int32 dE.
+ * Every turn's energy change is formed in float64 and rounded once to a
+ * multiple of this unit; the grid spans +-(2^31 - 1) units, and a particle
+ * leaving it is reported by blond_engine_check as BLOND_ERR_RANGE. */
+int blond_engine_set_energy_unit(blond_engine* engine, double lsb);
 int blond_engine_set_turn(blond_engine* engine, int64_t turn, void* stream);
 /* Re-slice the bound beam into the profile (Profile.track()). */
 int blond_engine_slice(blond_engine* engine, void* stream);
@@ -304,7 +316,8 @@ int blond_engine_prepare(blond_engine* engine, void* stream);
 int blond_engine_run(blond_engine* engine, int64_t n_turns, void* stream);
 /* Synchronise `stream` and report a device-side failure of the runs so far:
  * BLOND_ERR_TIMEOUT if a bounded wait in a kernel gave up (the coordinates
- * are then not valid), else BLOND_OK.  Clears the flag. */
+ * are then not valid), BLOND_ERR_RANGE if a Q32P64 energy left its grid
+ * (saturated there), else BLOND_OK.  Clears the flag. */
 int blond_engine_check(blond_engine* engine, void* stream);
 
 /* The beam-phase loop inside the turn: replaces BeamFeedback.track()
@@ -441,6 +454,27 @@ int blond_batch_set_slicing(blond_batch* batch, const double* cut_left,
 int blond_batch_set_impedance(blond_batch* batch, int64_t n_fft, const double* impedance,
                               const double* scale);
 int blond_batch_bind_beams(blond_batch* batch, void* dt, void* dE, const int64_t* offsets);
+/* No counterpart in the reference.  Q32P64 only, required before tracking:
+ * host array of B energy units (eV per count of each beam's int32 dE), as
+ * blond_engine_set_energy_unit. */
+int blond_batch_set_energy_units(blond_batch* batch, const double* lsb);
+/* Synchronise `stream`; BLOND_ERR_RANGE if a Q32P64 energy left its beam's
+ * grid since the last check, else BLOND_OK.  Clears the flag. */
+int blond_batch_check(blond_batch* batch, void* stream);
+/* Launch shape of the particle pass: threads per block (multiple of 32,
+ * <= 1024), blocks per SM, particles per thread and iteration (2, 4, 8),
+ * chunk (particles of one block's piece of a beam, 1024..2^22) and
+ * warp-aggregated shared-memory deposits (0/1).  Default 512, 2, 4, 32768,
+ * 0.  The reference's GPU backend uses one fixed grid for every kernel
+ * (blond/gpu/__init__.py:47-50). */
+int blond_batch_set_shape(blond_batch* batch, int threads, int blocks_per_sm,
+                          int particles_per_thread, int chunk, int aggregate);
+/* Time every launch shape above on the bound beams (CUDA events; the
+ * coordinates and histograms are restored) and keep the fastest.
+ * config (host, 6 ints) = {threads, blocks_per_sm, particles_per_thread,
+ * chunk, aggregate, candidates tried}; best_ms = its particle pass. */
+int blond_batch_autotune(blond_batch* batch, int reps, void* stream, int* config,
+                         double* best_ms);
 int blond_batch_set_turn(blond_batch* batch, int64_t turn, void* stream);
 int blond_batch_slice(blond_batch* batch, void* stream);
 /* capture and upload the turn graph now (else the first long run does) */
@@ -460,18 +494,25 @@ int blond_batch_get_induced_voltages(blond_batch* batch, double* v, void* stream
  * pooling allocator) cannot call cudaMalloc, which may stall the whole
  * device and bypasses the host's accounting.  Nothing is allocated: the
  * temporaries live in a fixed file-scope device array of ~448 KB that every
- * device loading the library holds until the process exits.
+ * device loading the library holds until the process exits.  The array is
+ * committed when the library's device code is loaded on a device; with
+ * CUDA's lazy module loading (the default) that happens in the first call.
  *   - n_slices <= 16384, else BLOND_ERR_SIZE; n_fft as for the engine.
- *   - dt, dE, voltage, omega_rf, phi_rf, impedance (n_fft/2+1 complex),
- *     profile_out and induced_voltage_out (n_slices doubles) are device
- *     arrays; bin_centers is a HOST array of n_slices values.  Drift
- *     scalars are this turn's drift parameters (turn+1 values in the
- *     reference tracker), voltage/omega_rf/phi_rf this turn's RF column.
+ *   - dt, dE, voltage, omega_rf, phi_rf, impedance (n_fft/2+1 complex,
+ *     16-byte aligned), profile_out and induced_voltage_out (n_slices
+ *     doubles) are device arrays.  Drift scalars are this turn's drift
+ *     parameters (turn+1 values in the reference tracker), voltage/
+ *     omega_rf/phi_rf this turn's RF column; beta and energy must be > 0.
+ *   - The bin centres are those of the reference's Profile for the cuts:
+ *     the midpoints of numpy.linspace(cut_left, cut_right, n_slices + 1),
+ *     computed on the device with numpy's operations.
  *   - The first call on a device looks the scratch up
  *     (cudaGetSymbolAddress) and sets kernel attributes: make it before
- *     any stream capture.
+ *     any stream capture.  Every call only enqueues kernels on `stream`
+ *     (no copies, no synchronisation).
  *   - Every call shares the scratch: calls that overlap on the GPU (two
- *     streams, two threads) race.  The histogram is cleared by each call. */
+ *     streams, two threads) race.  Each call clears the histogram it
+ *     starts from. */
 int blond_turn_f64_noalloc(double* dt, double* dE, int64_t n, int n_rf,
                            double charge, const double* voltage,
                            const double* omega_rf, const double* phi_rf,
@@ -481,8 +522,8 @@ int blond_turn_f64_noalloc(double* dt, double* dE, int64_t n, int n_rf,
                            double alpha_0, double alpha_1, double alpha_2,
                            double beta, double energy, double cut_left,
                            double cut_right, int n_slices,
-                           const double* bin_centers, const double* impedance,
-                           int64_t n_fft, double iv_scale, double* profile_out,
+                           const double* impedance, int64_t n_fft,
+                           double iv_scale, double* profile_out,
                            double* induced_voltage_out, void* stream);
 
 /* ------------------------------------------------------------ adjoint segment

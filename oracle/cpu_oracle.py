@@ -172,3 +172,43 @@ def track_oracle(dt0, dE0, ring, rf, cuts, bin_centers, n_slices, n_turns,
         prof = histogram(dt, cl, cr, n_slices)
         profiles.append(prof)
     return dt, dE, np.array(profiles), vinds
+
+
+def track_oracle_fixed(dt0, q0, unit, ring, rf, cuts, bin_centers, n_slices, n_turns,
+                       impedance=None, intensity=1e10, start_turn=0):
+    """The fixed-point energy form (dE = q * unit, q an int32 count) on the
+    CPU, in the reference main-loop order: each turn's energy change -- the
+    induced-voltage kick (linear_interp_kick.cpp:21-71) then the RF kick
+    (kick.cpp:16-35), evaluated by the same routines on a zero energy
+    array, i.e. in float64 and in the reference's order -- is rounded once
+    to a whole number of units; the simple drift (drift.cpp:19-28) then
+    uses q * unit.  Returns (dt, q, profiles[n_turns+1]).
+    """
+    dt = np.array(dt0, dtype=np.float64)
+    q = np.array(q0, dtype=np.int64)
+    qc = float(rf.particle.charge)
+    ratio = intensity / len(dt)
+    cl, cr = cuts
+    bc = np.asarray(bin_centers, dtype=np.float64)
+    prof = histogram(dt, cl, cr, n_slices)
+    profiles = [prof]
+    for k in range(n_turns):
+        t = start_turn + k
+        inc = np.zeros_like(dt)
+        if impedance is not None:
+            n_fft, Z = impedance
+            v = induced_voltage(prof, Z, n_fft, qc, ratio, n_slices)
+            linear_interp_kick(dt, inc, v, bc, qc, 0.0)
+        kick(dt, inc, rf.voltage[:, t], rf.omega_rf[:, t], rf.phi_rf[:, t], qc,
+             -rf.delta_E[t])
+        q = q + np.rint(inc * (1.0 / unit)).astype(np.int64)
+        if np.abs(q).max() > 2**31 - 1:
+            raise OverflowError("energy beyond the 32-bit grid")
+        dE = q.astype(np.float64) * unit
+        drift(dt, dE, 0, rf.t_rev[t + 1], rf.length_ratio, rf.alpha_order,
+              rf.eta_0[t + 1], rf.eta_1[t + 1], rf.eta_2[t + 1],
+              rf.alpha_0[t + 1], rf.alpha_1[t + 1], rf.alpha_2[t + 1],
+              rf.beta[t + 1], rf.energy[t + 1])
+        prof = histogram(dt, cl, cr, n_slices)
+        profiles.append(prof)
+    return dt, q, np.array(profiles)

@@ -20,7 +20,11 @@ import sys
 import types
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-DEFAULT_REF = os.environ.get("BLOND_REFERENCE_ROOT", "/root/reference")
+# the reference checkout: BLOND_REFERENCE_ROOT, else a checkout named
+# "reference" beside this repository
+DEFAULT_REF = os.environ.get(
+    "BLOND_REFERENCE_ROOT",
+    os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference"))
 
 _STUB_ROOTS = ("matplotlib", "pylab", "mpl_toolkits", "h5py")
 

@@ -1,7 +1,7 @@
 """Generate the golden fixtures in tests/golden/ by running the REFERENCE.
 
-Run in a container that holds the reference checkout (default
-/root/reference, override with BLOND_REFERENCE_ROOT) after
+Run in a container that holds the reference checkout (BLOND_REFERENCE_ROOT,
+by default a checkout named ``reference`` beside this repository) after
 ``make -C oracle``:
 
     python tests/golden/gen_golden.py

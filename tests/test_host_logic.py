@@ -1,5 +1,6 @@
 """Host-side logic of the drop-in layer against the reference (no GPU)."""
 import numpy as np
+import pytest
 
 from conftest import golden, normwise
 from blond_b200.beam.beam import Proton
@@ -110,3 +111,46 @@ def test_bench_clock_sampler_reads_nvml(monkeypatch):
     assert r["sm_mhz"] == 1800.0 and r["sm_max_mhz"] == 1965.0
     assert r["reasons"] == ["sw_power_cap"]
     assert r["source"].startswith("NVML")
+
+
+def test_fixed_point_energy_unit_and_conversion():
+    import torch
+    from blond_b200.engine import Q32_MAX, default_energy_unit, to_fixed
+    dE = torch.tensor([-3e7, 1e6, 2.5e7, 0.0], dtype=torch.float64)
+    u = default_energy_unit(dE)
+    assert u == pytest.approx(1.5 * 3e7 / Q32_MAX)
+    q = to_fixed(dE, u)
+    assert q.dtype == torch.int32
+    assert int(q.abs().max()) <= Q32_MAX
+    assert float((q.double() * u - dE).abs().max()) <= u / 2 * (1 + 1e-12)
+    with pytest.raises(ValueError):
+        to_fixed(dE, u / 2)  # 3e7 eV is then 3e9 counts
+    assert default_energy_unit(torch.zeros(3, dtype=torch.float64)) > 0
+
+
+def test_fixed_point_restatement_approaches_the_fp64_oracle():
+    """The fixed-point oracle with a fine unit follows the FP64 oracle: after
+    30 turns the energies agree to the rounding the grid adds (at most half
+    a unit per turn), the times to that rounding carried by the drift
+    (~1.6e-18 s per eV per turn: ~1e-17 s, 3e-9 of max|dt|), and the
+    profiles to a particle or two."""
+    import cpu_oracle as o
+    from blond_b200.beam.beam import Proton
+    from blond_b200.beam.distributions import _get_dE_from_dt, bigaussian_arrays
+    from blond_b200.input_parameters.rf_parameters import RFStation
+    from blond_b200.input_parameters.ring import Ring
+    turns, n, S = 30, 20000, 256
+    ring = Ring(6911.5, 1 / 18**2, 26e9, Proton(), turns)
+    rf = RFStation(ring, [4620], [4.5e6], [0.0])
+    centre = (rf.phi_s[0] - rf.phi_rf[0, 0]) / rf.omega_rf[0, 0]
+    dt0, dE0 = bigaussian_arrays(n, 0.4e-9, _get_dE_from_dt(ring, rf, 0.4e-9), centre, 4)
+    cuts = (centre - 1.25e-9, centre + 1.25e-9)
+    edges = np.linspace(*cuts, S + 1)
+    bc = (edges[:-1] + edges[1:]) / 2
+    unit = 0.1  # eV: a grid of +-215 MeV
+    q0 = np.rint(dE0 / unit).astype(np.int64)
+    fdt, fq, fprof = o.track_oracle_fixed(dt0, q0, unit, ring, rf, cuts, bc, S, turns)
+    odt, odE, oprof, _ = o.track_oracle(dt0, q0 * unit, ring, rf, cuts, bc, S, turns)
+    assert np.max(np.abs(fq * unit - odE)) <= turns * unit
+    assert np.max(np.abs(fdt - odt)) / np.max(np.abs(odt)) < 1e-8
+    assert np.abs(fprof[-1] - oprof[-1]).sum() <= 2
