@@ -51,6 +51,7 @@ def _sig(real):
         "beam_phase": [P, P, real, real, real, real, c_int, P, P],
         "beam_phase_fast": [P, P, real, real, real, c_int, P, P],
         "beam_statistics": [P, P, P, c_i64, P, P, P, P],
+        "cut_limits": [P, c_i64, c_dbl, P, P, P, P],
     }
 
 
@@ -98,6 +99,8 @@ _EXTRA = {
     "blond_engine_get_induced_voltage": [c_ptr, c_ptr, c_ptr],
     "blond_engine_get_turn": [c_ptr, ct.POINTER(c_i64)],
     "blond_engine_set_energy_unit": [c_ptr, c_dbl],
+    "blond_engine_set_interpolation": [c_ptr, c_int],
+    "blond_engine_set_smooth": [c_ptr, c_int],
     "blond_engine_tune": [c_ptr, c_int, c_int, c_int],
     "blond_engine_set_histogram": [c_ptr, c_int],
     "blond_engine_set_prefetch": [c_ptr, c_int],

@@ -37,15 +37,10 @@ class CutOptions:
     def set_cuts(self, beam=None):
         """profile.py:175-211."""
         if self.cut_left is None and self.cut_right is None:
-            dt = beam.dt.double()
-            if self.n_sigma is None:
-                dt_min, dt_max = float(dt.min()), float(dt.max())
-                self.cut_left = dt_min - 0.05 * (dt_max - dt_min)
-                self.cut_right = dt_max + 0.05 * (dt_max - dt_min)
-            else:
-                mean, sigma = float(dt.mean()), float(dt.std(unbiased=False))
-                self.cut_left = mean - self.n_sigma * sigma / 2
-                self.cut_right = mean + self.n_sigma * sigma / 2
+            # one device reduction (blond_cut_limits): min/max -/+ 5 % of the
+            # spread, or mean -/+ n_sigma sigma / 2; read back once
+            cuts = bm.cut_limits(beam.dt, self.n_sigma).cpu().numpy()
+            self.cut_left, self.cut_right = float(cuts[0]), float(cuts[1])
         else:
             self.cut_left = float(self.convert_coordinates(self.cut_left, self.cuts_unit))
             self.cut_right = float(self.convert_coordinates(self.cut_right, self.cuts_unit))

@@ -307,6 +307,24 @@ def beam_statistics(dt, dE, id=None, out=None, scratch=None, ticket=None):
     return out
 
 
+def cut_limits(dt, n_sigma=None, scratch=None, ticket=None):
+    """The automatic frame of CutOptions.set_cuts (profile.py:185-195) by a
+    device reduction: a float64 device tensor [cut_left, cut_right] --
+    min/max -/+ 5 % of the spread when n_sigma is None (the reference's
+    bits), else mean -/+ n_sigma sigma / 2.  No synchronisation."""
+    dev = dt.device
+    if scratch is None:
+        scratch = torch.empty(STATS_SCRATCH, dtype=torch.float64, device=dev)
+    if ticket is None:
+        ticket = torch.zeros(1, dtype=torch.int32, device=dev)
+    out = torch.empty(2, dtype=torch.float64, device=dev)
+    dt = dt.contiguous()
+    _lib.call(f"blond_cut_limits_{_suffix(dt)}", _ptr(dt), dt.numel(),
+              float(n_sigma) if n_sigma is not None else 0.0, _ptr(out), _ptr(scratch),
+              _ptr(ticket), _stream())
+    return out
+
+
 # ------------------------------------------------------ time-domain wakes
 def interp(x, xp, fp, left=None, right=None, period=None, *, x_shift=0.0):
     """numpy.interp(x + x_shift, xp, fp, left, right) on the device in
@@ -429,14 +447,52 @@ def resonator_induced_voltage_1_turn(kappa1, n_macroparticles, bin_centers, bin_
     return v, deltaT
 
 
-class B200Backend:
-    """The hot-path subset of blond's MasterBackend attribute contract
-    (bmath_backends.py:61-201), backed by libblond_b200."""
+def not_implemented(*args, **kwargs):
+    """Stands in for an attribute of the backend contract this library does
+    not provide (the reference's GpuBackend does the same for its gaps,
+    bmath_backends.py:750-759)."""
+    raise NotImplementedError("not provided by the B200 backend (outside the "
+                              "tracking hot path)")
 
-    device = "GPU_B200"
+
+# Every attribute the reference's backend contract declares
+# (MasterBackend.__init__, bmath_backends.py:61-185), in its order.
+MASTER_ATTRIBUTES = (
+    "precision", "device", "histogram2d", "maximum", "minimum", "amax", "roll",
+    "fftconvolve", "pi", "diff", "uint", "empty", "sign", "vectorize", "hstack",
+    "arctan", "arcsin", "sqrt", "trapezoid", "reshape", "exp", "int32", "delete",
+    "unique", "abs", "zeros", "floor", "resize", "take", "round", "fabs", "float64",
+    "meshgrid", "mean", "append", "argmax", "dot", "double", "sum", "cumsum", "cos",
+    "concatenate", "full", "asarray", "ones", "uint32", "histogram", "unwrap", "ceil",
+    "interp", "std", "empty_like", "min", "max", "cosh", "linspace", "array",
+    "gradient", "isnan", "hamming", "clip", "where", "isinf", "sin", "zeros_like",
+    "arange", "loadtxt", "convolve", "fliplr", "log", "heaviside", "absolute",
+    "float32", "ascontiguousarray", "complex64", "copy", "poly1d", "invert", "all",
+    "int64", "count_nonzero", "nonzero", "log10", "real", "argsort", "complex128",
+    "irfft", "rfft", "rfftfreq", "random", "fft", "slice_beam", "drift",
+    "sparse_histogram", "distribution_from_tomoscope", "set_random_seed",
+    "synchrotron_radiation_full", "kick", "fast_resonator", "beam_phase_fast",
+    "rf_volt_comp", "slice_smooth", "linear_interp_kick", "music_track_multiturn",
+    "music_track", "synchrotron_radiation", "beam_phase",
+    "resonator_induced_voltage_1_turn",
+)
+
+
+class B200Backend:
+    """A complete backend for the reference's bmath object: every attribute
+    of its contract (MasterBackend, bmath_backends.py:61-201) is set, so
+    the reference's verify_backend (:203-228) accepts it.  As the
+    reference's GpuBackend works on CuPy arrays, this one works on torch
+    CUDA tensors: the hot-path routines are libblond_b200's kernels, the
+    array functions torch's CUDA equivalents of the numpy names, and the
+    routines outside the tracking hot path (synchrotron radiation, MuSiC,
+    tomoscope import, sparse slicing) raise NotImplementedError."""
 
     def __init__(self):
+        T = torch
         self.precision = precision
+        self.device = "GPU_B200"
+        # hot path: libblond_b200
         self.kick = kick
         self.drift = drift
         self.slice_beam = slice_beam
@@ -451,6 +507,40 @@ class B200Backend:
         self.beam_phase = beam_phase
         self.beam_phase_fast = beam_phase_fast
         self.resonator_induced_voltage_1_turn = resonator_induced_voltage_1_turn
+        # array functions on CUDA tensors
+        for name in ("maximum", "minimum", "amax", "roll", "diff", "empty", "sign",
+                     "hstack", "arctan", "arcsin", "sqrt", "trapezoid", "reshape", "exp",
+                     "unique", "abs", "zeros", "floor", "take", "round", "meshgrid", "mean",
+                     "argmax", "dot", "sum", "cumsum", "cos", "concatenate", "full", "asarray",
+                     "ones", "ceil", "std", "empty_like", "min", "max", "cosh", "linspace",
+                     "gradient", "isnan", "clip", "where", "isinf", "sin", "zeros_like",
+                     "arange", "fliplr", "log", "heaviside", "absolute", "all",
+                     "count_nonzero", "nonzero", "log10", "real", "argsort", "histogram"):
+            setattr(self, name, getattr(T, name))
+        self.fabs = T.abs
+        self.array = T.tensor
+        self.copy = T.clone
+        self.invert = T.bitwise_not
+        self.hamming = T.hamming_window
+        self.ascontiguousarray = lambda a, dtype=None: (
+            T.as_tensor(a, dtype=dtype).contiguous())
+        self.append = lambda a, b: T.cat([T.as_tensor(a).reshape(-1),
+                                          T.as_tensor(b).reshape(-1)])
+        self.pi = float(np.pi)
+        for name, dt in (("int32", T.int32), ("int64", T.int64), ("uint32", T.uint32),
+                         ("uint", T.uint64), ("float32", T.float32), ("float64", T.float64),
+                         ("double", T.float64), ("complex64", T.complex64),
+                         ("complex128", T.complex128)):
+            setattr(self, name, dt)
+        self.fft = T.fft
+        self.random = T.random
+        self.set_random_seed = T.manual_seed
+        # outside the hot path
+        for name in ("histogram2d", "fftconvolve", "vectorize", "delete", "resize",
+                     "unwrap", "loadtxt", "convolve", "poly1d", "sparse_histogram",
+                     "distribution_from_tomoscope", "synchrotron_radiation_full",
+                     "synchrotron_radiation", "music_track_multiturn", "music_track"):
+            setattr(self, name, not_implemented)
 
     def use_precision(self, p: str = "double"):
         use_precision(p)

@@ -115,6 +115,29 @@ __device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, 
 __device__ __forceinline__ double div_rn(double a, double b) { return __ddiv_rn(a, b); }
 __device__ __forceinline__ float div_rn(float a, float b) { return __fdiv_rn(a, b); }
 
+// ------------------------------------------------------ smooth deposit weights
+// histogram.cpp:75-132.  Weights of a particle at f = (dt-cut_left)*inv_w,
+// k = (int)f, d = f-k: bin k gets 0.5-d; bin k+1 (d > 0.5) or k-1 (else)
+// gets 0.5+d.  The bmath kernel accumulates them with floating-point
+// atomics (the summation order, not the set of terms, differs from the
+// reference's); the fused turn in 64-bit fixed point (engine.cu).
+template <typename T>
+__device__ __forceinline__ void smooth_weights(T a, T cut_left, T inv_w, T lo,
+                                               T hi, int S, int& k, int& k2,
+                                               double& w1, double& w2) {
+    k = -1;
+    k2 = -1;
+    if (!(a >= lo && a <= hi)) return;  // also rejects NaN
+    const T f = (a - cut_left) * inv_w;
+    k = (int)f;
+    const T d = f - (T)k;
+    k2 = d > T(0.5) ? (int)((double)f + 1.0) : (int)((double)f - 1.0);
+    w1 = 0.5 - (double)d;
+    w2 = 0.5 + (double)d;
+    if (k < 0 || k >= S) k = -1;
+    if (k2 < 0 || k2 >= S) k2 = -1;
+}
+
 // ------------------------------------------------------------ drift solvers
 // drift.cpp:29-76.  The expressions of the 'legacy' and 'exact' solvers
 // cancel (1/(1-x)-1 with x ~ 1e-6), so they are evaluated operation by

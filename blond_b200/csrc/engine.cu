@@ -69,6 +69,15 @@ struct blond_engine {
     void* dE = nullptr;
     int64_t n = 0;
     double lsb = 0.0;  // Q32P64: eV per count of dE (blond_engine_set_energy_unit)
+    // interpolated tracker (blond_engine_set_interpolation): RF + induced
+    // voltage interpolated from the table, no separate RF kick
+    bool interp = false;
+    // smooth slicing (blond_engine_set_smooth): fixed-point accumulator,
+    // its bits per particle and the last-block ticket
+    bool smooth = false;
+    long long* d_acc64 = nullptr;
+    int* d_smooth_ticket = nullptr;
+    int smooth_bits = 0;
     // tuning
     int threads = 512;
     int blocks_per_sm = 2;
@@ -342,6 +351,11 @@ static ParticleArgs particle_args(blond_engine* e) {
     a.lsb = e->lsb;
     a.inv_lsb = e->lsb > 0 ? 1.0 / e->lsb : 0.0;
     a.err = e->d_err;
+    if (e->interp) {
+        a.n_rf = 0;
+        a.interp = 1;
+    }
+    a.no_deposit = e->smooth ? 1 : 0;
     return a;
 }
 
@@ -375,7 +389,95 @@ static int launch_particles_range(blond_engine* e, int64_t off, int64_t cnt,
     return launch_particles_a(e, a, true, s, true);
 }
 
+// Smooth slicing inside the fused turn (Profile with smooth=True,
+// profile.py:764-773), the weights of histogram.cpp:75-132 (bin k gets
+// 0.5 - d, which may be negative, its neighbour 0.5 + d).  Each weight is
+// rounded to a multiple of 2^-bits and accumulated with 64-bit integer
+// atomics -- in shared memory when the profile fits, then into the global
+// accumulator -- so the sum does not depend on the order of the atomics and
+// every run gives the same bits.  bits = min(52, 62 - ceil(log2(1.5 n + 2)))
+// keeps |sum| below 2^62.  The block that takes the last ticket converts the
+// accumulator into the float64 profile and zeroes it.
+constexpr int kSmoothThreads = 512;
+
+__global__ void __launch_bounds__(kSmoothThreads)
+smooth_deposit_kernel(const double* __restrict__ dt, int64_t n, double cut_left, double inv_w,
+                      double lo, double hi, int S, int bits, int use_smem,
+                      unsigned long long* __restrict__ acc, double* __restrict__ profile,
+                      int* __restrict__ ticket) {
+    extern __shared__ unsigned long long sacc[];
+    if (use_smem) {
+        for (int k = threadIdx.x; k < S; k += blockDim.x) sacc[k] = 0ull;
+        __syncthreads();
+    }
+    unsigned long long* dst = use_smem ? sacc : acc;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        int k, k2;
+        double w1 = 0.0, w2 = 0.0;
+        smooth_weights<double>(dt[i], cut_left, inv_w, lo, hi, S, k, k2, w1, w2);
+        if (k >= 0) atomicAdd(&dst[k], (unsigned long long)llrint(ldexp(w1, bits)));
+        if (k2 >= 0) atomicAdd(&dst[k2], (unsigned long long)llrint(ldexp(w2, bits)));
+    }
+    __shared__ bool last;
+    __syncthreads();
+    if (use_smem)
+        for (int k = threadIdx.x; k < S; k += blockDim.x)
+            if (sacc[k]) atomicAdd(&acc[k], sacc[k]);
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(ticket, 1) == (int)gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    for (int k = threadIdx.x; k < S; k += blockDim.x) {
+        const long long v = (long long)atomicExch(&acc[k], 0ull);
+        profile[k] = ldexp((double)v, -bits);
+    }
+    if (threadIdx.x == 0) *ticket = 0;
+}
+
+static int smooth_bits_for(int64_t n) {
+    int lg = 0;
+    while (lg < 62 && (1ll << lg) < 3 * n / 2 + 2) ++lg;
+    return std::min(52, 62 - lg);
+}
+
+static int launch_smooth_deposit(blond_engine* e, cudaStream_t s) {
+    const double w = (e->cut_right - e->cut_left) / e->S;
+    const double lo = e->cut_left + w * 0.5, hi = e->cut_right - w * 0.5;
+    const int limit = device_info().max_smem_optin - 1024;
+    const size_t smem = sizeof(unsigned long long) * (size_t)e->S;
+    const bool use_smem = (int64_t)smem <= limit;
+    static std::mutex mu;
+    static std::set<int> done;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if (!done.count(device_info().device)) {
+            BB_CUDA(cudaFuncSetAttribute(smooth_deposit_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, limit));
+            done.insert(device_info().device);
+        }
+    }
+    const int grid = particle_grid(e->n, kSmoothThreads, use_smem && smem > 96 * 1024 ? 1 : 2);
+    smooth_deposit_kernel<<<grid, kSmoothThreads, use_smem ? smem : 0, s>>>(
+        static_cast<const double*>(e->dt), e->n, e->cut_left, e->inv_w, lo, hi, e->S,
+        e->smooth_bits, use_smem ? 1 : 0, reinterpret_cast<unsigned long long*>(e->d_acc64),
+        e->d_profile, e->d_smooth_ticket);
+    BB_LAUNCH_CHECK();
+    return BLOND_OK;
+}
+
 static int launch_profile(blond_engine* e, bool clear, cudaStream_t s) {
+    // smooth slicing: the deposit pass wrote the profile; the head only
+    // advances the turn counter
+    if (e->smooth) {
+        if (clear) {
+            profile_kernel<<<1, 32, 0, s>>>(e->d_hist, e->d_profile, 0, 1, e->d_turn);
+            BB_LAUNCH_CHECK();
+        }
+        return BLOND_OK;
+    }
     const int threads = 256;
     const int grid = std::min(64, (e->S + threads - 1) / threads);
     profile_kernel<<<grid, threads, 0, s>>>(e->d_hist, e->d_profile, e->S, clear ? 1 : 0,
@@ -432,8 +534,57 @@ static int launch_head(blond_engine* e, cudaStream_t s) {
     return launch_feedback_turn(a, nullptr, e->d_fb_ticket, 0, s);
 }
 
+// Head of an interpolated turn without an impedance (tracker.py:586-601
+// with total_voltage = rf_voltage): profile <- histogram (cleared), the
+// interpolation table of the RF voltage at the bin centres (rf_volt_comp,
+// kick.cpp:37-51) with the turn's acceleration kick in the offsets
+// (linear_interp_kick.cpp:44-47), turn counter += 1.  One CTA, so every
+// thread reads the counter before thread 0 moves it.
+__global__ void __launch_bounds__(1024)
+interp_head_kernel(int* hist, double* profile, int S, long long* turn_p, const double* V,
+                   const double* om, const double* ph, int n_rf, const double* acc,
+                   const double* bc, double charge, double inv_w, void* table,
+                   int table_f32, long long n_turns) {
+    long long turn = *turn_p;
+    if (turn >= n_turns) turn = n_turns - 1;
+    for (int k = threadIdx.x; k < S; k += blockDim.x) {
+        profile[k] = (double)hist[k];
+        hist[k] = 0;
+    }
+    const double* Vt = V + turn * n_rf;
+    const double* omt = om + turn * n_rf;
+    const double* pht = ph + turn * n_rf;
+    const double acc_t = acc[turn];
+    auto rfv = [&](double x) {
+        double s = 0.0;
+        for (int j = 0; j < n_rf; ++j) s += Vt[j] * sin(omt[j] * x + pht[j]);
+        return s;
+    };
+    for (int n = threadIdx.x; n < S - 1; n += blockDim.x) {
+        const double a0 = rfv(bc[n]), a1 = rfv(bc[n + 1]);
+        if (!table_f32) {
+            const double slope = charge * (a1 - a0) * inv_w;
+            const double offset = (charge * a0 - bc[n] * slope) + acc_t;
+            reinterpret_cast<double2*>(table)[n] = make_double2(slope, offset);
+        } else {
+            reinterpret_cast<float2*>(table)[n] =
+                make_float2((float)(charge * a0 + acc_t), (float)(charge * (a1 - a0) * inv_w));
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) *turn_p = *turn_p + 1;
+}
+
 static int launch_spectral_head(blond_engine* e, cudaStream_t s, bool loop) {
-    if (!(e->has_fft || e->has_ind)) return launch_profile(e, true, s);
+    if (!(e->has_fft || e->has_ind)) {
+        if (!e->interp) return launch_profile(e, true, s);
+        interp_head_kernel<<<1, 1024, 0, s>>>(
+            e->d_hist, e->d_profile, e->S, e->d_turn, e->d_V, e->d_om, e->d_ph, e->n_rf,
+            e->d_acc, e->d_bc, e->charge, e->lik_inv_w, e->d_table,
+            e->precision == BLOND_PREC_F32P64 ? 1 : 0, e->n_turns);
+        BB_LAUNCH_CHECK();
+        return BLOND_OK;
+    }
     if (!e->has_fft) {
         set_error("engine: an inductive impedance needs an FFT impedance in this build");
         return BLOND_ERR_UNSUPPORTED;
@@ -442,9 +593,12 @@ static int launch_spectral_head(blond_engine* e, cudaStream_t s, bool loop) {
     P.p = e->plan;
     P.mode = SPEC_FORWARD | SPEC_MULTIPLY | SPEC_INVERSE;
     P.pdl = e->pdl ? 1 : 0;
-    P.in_i32 = e->d_hist;
     P.n_in = e->S;
     P.profile_out = e->d_profile;
+    if (e->smooth)
+        P.in_f64 = e->d_profile;  // the smooth deposit's profile (read only)
+    else
+        P.in_i32 = e->d_hist;
     P.H = e->d_H;
     P.out = e->d_vind;
     P.n_out = std::min<int64_t>(e->S, e->plan.N);
@@ -456,6 +610,13 @@ static int launch_spectral_head(blond_engine* e, cudaStream_t s, bool loop) {
     P.charge = e->charge;
     P.inv_w = e->lik_inv_w;
     P.bc = e->d_bc;
+    if (e->interp) {
+        P.rf_V = e->d_V;
+        P.rf_om = e->d_om;
+        P.rf_ph = e->d_ph;
+        P.rf_n = e->n_rf;
+        P.rf_acc = e->d_acc;
+    }
     P.turn = e->d_turn;
     P.bump_turn = 1;
     P.twg = e->d_tw;
@@ -471,7 +632,8 @@ static int launch_spectral_head(blond_engine* e, cudaStream_t s, bool loop) {
 static int launch_turn(blond_engine* e, cudaStream_t s) {
     int rc = launch_head(e, s);
     if (rc) return rc;
-    return launch_particles(e, true, s);
+    if ((rc = launch_particles(e, true, s))) return rc;
+    return e->smooth ? launch_smooth_deposit(e, s) : BLOND_OK;
 }
 
 static int check_ready(blond_engine* e) {
@@ -561,7 +723,8 @@ int blond_engine_destroy(blond_engine* e) {
                     (void*)e->d_ind, (void*)e->d_fb_table, (void*)e->d_fb_on_time,
                     (void*)e->d_fb_state, (void*)e->d_fb_trace, (void*)e->d_fb_partials, (void*)e->d_fb_ticket,
                     (void*)e->d_turn, (void*)e->d_err, (void*)e->own_hist, (void*)e->d_profile,
-                    (void*)e->d_vind, e->d_table})
+                    (void*)e->d_vind, e->d_table, (void*)e->d_acc64,
+                    (void*)e->d_smooth_ticket})
         free_ptr(p);
     delete e;
     return BLOND_OK;
@@ -694,6 +857,37 @@ int blond_engine_bind_beam(blond_engine* e, void* dt, void* dE, int64_t n) {
     e->dt = dt;
     e->dE = dE;
     e->n = n;
+    e->smooth_bits = smooth_bits_for(n);
+    e->graph_dirty = true;
+    return BLOND_OK;
+}
+
+int blond_engine_set_interpolation(blond_engine* e, int on) {
+    BB_CHECK_ARG(e, "engine_set_interpolation: null engine");
+    if (on && e->has_fb && (e->fb.machine == BLOND_FB_SPS_RL || !e->has_fft)) {
+        set_error("engine_set_interpolation: not with the SPS_RL loop or a beam-phase loop "
+                  "without an FFT impedance");
+        return BLOND_ERR_UNSUPPORTED;
+    }
+    e->interp = on != 0;
+    e->graph_dirty = true;
+    return BLOND_OK;
+}
+
+int blond_engine_set_smooth(blond_engine* e, int on) {
+    BB_CHECK_ARG(e, "engine_set_smooth: null engine");
+    if (on && (e->has_fb || e->d_hist != e->own_hist)) {
+        set_error("engine_set_smooth: smooth slicing is not built with a beam-phase loop or "
+                  "a caller-bound (sharded) histogram");
+        return BLOND_ERR_UNSUPPORTED;
+    }
+    if (on && !e->d_acc64) {
+        BB_CUDA(cudaMalloc((void**)&e->d_acc64, sizeof(long long) * (size_t)e->S));
+        BB_CUDA(cudaMemset(e->d_acc64, 0, sizeof(long long) * (size_t)e->S));
+        BB_CUDA(cudaMalloc((void**)&e->d_smooth_ticket, sizeof(int)));
+        BB_CUDA(cudaMemset(e->d_smooth_ticket, 0, sizeof(int)));
+    }
+    e->smooth = on != 0;
     e->graph_dirty = true;
     return BLOND_OK;
 }
@@ -724,6 +918,7 @@ int blond_engine_slice(blond_engine* e, void* stream) {
         return BLOND_ERR_STATE;
     }
     cudaStream_t s = as_stream(stream);
+    if (e->smooth) return launch_smooth_deposit(e, s);
     BB_CUDA(cudaMemsetAsync(e->d_hist, 0, sizeof(int) * e->S, s));
     int rc = launch_particles(e, false, s);
     if (rc) return rc;
@@ -742,6 +937,11 @@ int blond_engine_step(blond_engine* e, int part, void* stream) {
     BB_CHECK_ARG(e && part >= 1 && part <= 3, "engine_step: part must be 1, 2 or 3");
     int rc = check_ready(e);
     if (rc) return rc;
+    if (e->smooth) {
+        set_error("engine_step: the step-by-step (sharded) turn deposits integer counts; "
+                  "smooth slicing runs through blond_engine_run");
+        return BLOND_ERR_UNSUPPORTED;
+    }
     cudaStream_t s = as_stream(stream);
     if (part == 3) return launch_profile(e, false, s);
     BB_CHECK_SIZE(e->host_turn < e->n_turns, "engine_step: turn %lld beyond the programme",
@@ -1040,6 +1240,11 @@ int blond_engine_track_host(blond_engine* e, double* host_dt, void* host_dE,
                  "engine_track_host: bad argument (chunks in 1..256)");
     int rc = check_ready(e);
     if (rc) return rc;
+    if (e->smooth) {
+        set_error("engine_track_host: smooth slicing reads the whole beam after the pass; "
+                  "track device-resident coordinates");
+        return BLOND_ERR_UNSUPPORTED;
+    }
     BB_CHECK_SIZE(e->host_turn + n_turns <= e->n_turns,
                   "engine_track_host: turns exceed the programme");
     if (n_turns == 0) return BLOND_OK;
@@ -1158,6 +1363,15 @@ int blond_engine_set_feedback(blond_engine* e, int machine, int delay, double ga
     BB_CHECK_ARG(sample_dE >= 1, "engine_set_feedback: sample_dE must be >= 1");
     BB_CHECK_ARG(machine != BLOND_FB_PSB || (on_time && n_on_time >= 1),
                  "engine_set_feedback: the PSB loop needs its on-time turns");
+    if (e->smooth) {
+        set_error("engine_set_feedback: not with smooth slicing");
+        return BLOND_ERR_UNSUPPORTED;
+    }
+    if (e->interp && (machine == BLOND_FB_SPS_RL || !e->has_fft)) {
+        set_error("engine_set_feedback: an interpolated turn takes no SPS_RL loop, and other "
+                  "loops only with an FFT impedance");
+        return BLOND_ERR_UNSUPPORTED;
+    }
     if (machine == BLOND_FB_SPS_RL && e->precision == BLOND_PREC_Q32P64) {
         set_error("engine_set_feedback: the SPS_RL loop's energy average is not built for "
                   "fixed-point energies (Q32P64)");

@@ -57,6 +57,12 @@ struct ParticleArgs {
     // sticky error word: bit 0 a bounded wait gave up, bit 1 an energy left
     // its 32-bit grid (Q32P64)
     int* err;
+    // interpolated tracker: the RF kick and the acceleration kick are part
+    // of the interpolation table, so the pass runs with n_rf = 0 and acc 0
+    int interp;
+    // smooth slicing: a separate deposit pass makes the profile, this pass
+    // deposits nothing
+    int no_deposit;
 };
 
 enum { PREC_F64 = 0, PREC_F32P64 = 1, PREC_Q32P64 = 2 };
@@ -474,7 +480,7 @@ particle_kernel(const ParticleArgs a) {
             c.ph[j] = a.ph[t_idx * a.n_rf + j];
         }
         if (threadIdx.x == 0) {
-            c.acc = a.acc[t_idx];
+            c.acc = a.interp ? 0.0 : a.acc[t_idx];
             c.d = a.drift[t_idx + 1];
         }
     }
@@ -504,8 +510,10 @@ particle_kernel(const ParticleArgs a) {
                 b0 = engine_bin(tt.x, a.cut_left, a.inv_w, a.S);
                 b1 = engine_bin(tt.y, a.cut_left, a.inv_w, a.S);
             }
-            deposit(hd, b0, WARP_AGG, 0xffffffffu);
-            deposit(hd, b1, WARP_AGG, 0xffffffffu);
+            if (!a.no_deposit) {
+                deposit(hd, b0, WARP_AGG, 0xffffffffu);
+                deposit(hd, b1, WARP_AGG, 0xffffffffu);
+            }
         }
     } else {
         // the ring sits after the (16-byte aligned) histogram
@@ -555,8 +563,10 @@ particle_kernel(const ParticleArgs a) {
                 b0 = engine_bin(tt.x, a.cut_left, a.inv_w, a.S);
                 b1 = engine_bin(tt.y, a.cut_left, a.inv_w, a.S);
             }
-            deposit(hd, b0, WARP_AGG, 0xffffffffu);
-            deposit(hd, b1, WARP_AGG, 0xffffffffu);
+            if (!a.no_deposit) {
+                deposit(hd, b0, WARP_AGG, 0xffffffffu);
+                deposit(hd, b1, WARP_AGG, 0xffffffffu);
+            }
             slot = slot + 1 == NST ? 0 : slot + 1;
         }
         ring_wait<0>();  // nothing may land in shared memory after the flush
@@ -571,7 +581,7 @@ particle_kernel(const ParticleArgs a) {
             dE[a.n - 1] = e;
         }
         const int b = engine_bin(t, a.cut_left, a.inv_w, a.S);
-        if (b >= 0) atomicAdd(&hd[b], 1);
+        if (b >= 0 && !a.no_deposit) atomicAdd(&hd[b], 1);
     }
     if (!a.global_hist) cluster_flush(sh, a.hist, a.S);
 }
@@ -656,7 +666,7 @@ particle_kernel_tma(const ParticleArgs a, int* err) {
         c.ph[j] = a.ph[t_idx * a.n_rf + j];
     }
     if (threadIdx.x == 0) {
-        c.acc = a.acc[t_idx];
+        c.acc = a.interp ? 0.0 : a.acc[t_idx];
         c.d = a.drift[t_idx + 1];
         for (int s = 0; s < nst; ++s) mbar_init(&full[s], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -698,8 +708,12 @@ particle_kernel_tma(const ParticleArgs a, int* err) {
                 track_pair<PREC, SOLVER, LIK>(tt.x, tt.y, ee.x, ee.y, c, a, order);
                 stream_store(reinterpret_cast<double2*>(dt + base) + p, tt, pol);
                 stream_store(reinterpret_cast<E2*>(dE + base) + p, ee, pol);
-                block_deposit<HIST>(sh, half, a.hist, engine_bin(tt.x, a.cut_left, a.inv_w, a.S));
-                block_deposit<HIST>(sh, half, a.hist, engine_bin(tt.y, a.cut_left, a.inv_w, a.S));
+                if (!a.no_deposit) {
+                    block_deposit<HIST>(sh, half, a.hist,
+                                        engine_bin(tt.x, a.cut_left, a.inv_w, a.S));
+                    block_deposit<HIST>(sh, half, a.hist,
+                                        engine_bin(tt.y, a.cut_left, a.inv_w, a.S));
+                }
             }
         }
         // stage s fully consumed; the failure decision is block-uniform
@@ -726,7 +740,7 @@ particle_kernel_tma(const ParticleArgs a, int* err) {
             track_one<PREC, SOLVER, LIK, true, true, false>(t, e, c, a, sh, order);
             dt[i] = t;
             dE[i] = e;
-            const int b = engine_bin(t, a.cut_left, a.inv_w, a.S);
+            const int b = a.no_deposit ? -1 : engine_bin(t, a.cut_left, a.inv_w, a.S);
             if (HIST == HIST_PACKED)
                 deposit_packed(reinterpret_cast<unsigned*>(sh), half, a.hist, b);
             else if (b >= 0)

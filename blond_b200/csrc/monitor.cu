@@ -129,6 +129,142 @@ int stats_impl(const T* dt, const T* dE, const int64_t* id, int64_t n, double* s
     return BLOND_OK;
 }
 
+// ------------------------------------------------------------ cut limits
+// CutOptions.set_cuts without given cuts (beam/profile.py:185-195):
+//   n_sigma <= 0 (None): cut_left = min - 0.05 (max - min),
+//                        cut_right = max + 0.05 (max - min);
+//   n_sigma > 0:         cut_left/right = mean -/+ n_sigma sigma / 2
+//                        (numpy's mean and population std).
+// min and max are exact, so the first form gives the reference's bits; the
+// last block evaluates the expressions in the reference's order without
+// contraction.  NaN in dt propagates as in numpy.  The mean and std use
+// shifted sums (shift = dt[0]), so they agree with numpy's pairwise sums to
+// rounding (~1e-16 relative), not bit for bit.
+constexpr int kCutThreads = 256;
+
+template <typename T>
+__global__ void __launch_bounds__(kCutThreads)
+cut_limits_kernel(const T* __restrict__ x, int64_t n, double n_sigma, double* __restrict__ out,
+                  double* __restrict__ part, int* __restrict__ ticket) {
+    const bool minmax = !(n_sigma > 0);
+    const double shift = (double)x[0];
+    // minmax: (min, max, nan flag); moments: (S1, S2) of x - shift
+    double a = minmax ? INFINITY : 0.0, b = minmax ? -INFINITY : 0.0, nan = 0.0;
+    const int64_t G = (int64_t)gridDim.x * kCutThreads;
+    for (int64_t i0 = blockIdx.x * (int64_t)kCutThreads + threadIdx.x; i0 < n; i0 += 4 * G) {
+        T v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int64_t i = i0 + u * G;
+            v[u] = i < n ? x[i] : x[i0];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const double d = (double)v[u];
+            if (minmax) {
+                if (d != d) nan = 1.0;
+                a = fmin(a, d);
+                b = fmax(b, d);
+            } else if (i0 + u * G < n) {
+                const double e = d - shift;
+                a += e;
+                b += e * e;
+            }
+        }
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int d = 16; d > 0; d >>= 1) {
+        const double oa = __shfl_down_sync(0xffffffffu, a, d);
+        const double ob = __shfl_down_sync(0xffffffffu, b, d);
+        nan = fmax(nan, __shfl_down_sync(0xffffffffu, nan, d));
+        if (minmax) {
+            a = fmin(a, oa);
+            b = fmax(b, ob);
+        } else {
+            a += oa;
+            b += ob;
+        }
+    }
+    __shared__ double sh[kCutThreads / 32][3];
+    __shared__ bool last;
+    if (lane == 0) {
+        sh[warp][0] = a;
+        sh[warp][1] = b;
+        sh[warp][2] = nan;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < kCutThreads / 32; ++w) {
+            if (minmax) {
+                a = fmin(a, sh[w][0]);
+                b = fmax(b, sh[w][1]);
+            } else {
+                a += sh[w][0];
+                b += sh[w][1];
+            }
+            nan = fmax(nan, sh[w][2]);
+        }
+        part[3 * (size_t)blockIdx.x] = a;
+        part[3 * (size_t)blockIdx.x + 1] = b;
+        part[3 * (size_t)blockIdx.x + 2] = nan;
+        __threadfence();
+        last = atomicAdd(ticket, 1) == (int)gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last || threadIdx.x != 0) return;
+    __threadfence();
+    // the last block combines the partials in block order
+    a = minmax ? INFINITY : 0.0;
+    b = minmax ? -INFINITY : 0.0;
+    nan = 0.0;
+    for (int q = 0; q < (int)gridDim.x; ++q) {
+        if (minmax) {
+            a = fmin(a, part[3 * q]);
+            b = fmax(b, part[3 * q + 1]);
+        } else {
+            a += part[3 * q];
+            b += part[3 * q + 1];
+        }
+        nan = fmax(nan, part[3 * q + 2]);
+    }
+    *ticket = 0;
+    if (minmax) {
+        if (nan != 0.0) a = b = NAN;
+        // dt_min - 0.05 * (dt_max - dt_min), dt_max + 0.05 * (dt_max - dt_min)
+        const double w = __dmul_rn(0.05, __dsub_rn(b, a));
+        out[0] = __dsub_rn(a, w);
+        out[1] = __dadd_rn(b, w);
+    } else {
+        const double cnt = (double)n;
+        const double m = a / cnt;
+        const double mean = shift + m;
+        const double sigma = sqrt(fmax(b / cnt - m * m, 0.0));
+        // mean - n_sigma * sigma / 2, mean + n_sigma * sigma / 2
+        const double h = __ddiv_rn(__dmul_rn(n_sigma, sigma), 2.0);
+        out[0] = __dsub_rn(mean, h);
+        out[1] = __dadd_rn(mean, h);
+    }
+}
+
+template <typename T>
+int cut_limits_impl(const T* dt, int64_t n, double n_sigma, double* cuts, double* scratch,
+                    int* ticket, void* stream) {
+    clear_error();
+    BB_CHECK_ARG(dt && cuts && scratch && ticket, "cut_limits: null pointer");
+    BB_CHECK_SIZE(n >= 1, "cut_limits: n = %lld (>= 1 required)", (long long)n);
+    BB_CHECK_ARG(aligned(dt, sizeof(T)) && aligned(cuts, 8) && aligned(scratch, 8) &&
+                     aligned(ticket, 4),
+                 "cut_limits: misaligned array");
+    const DeviceInfo& d = device_info();
+    int64_t grid = (n + kCutThreads - 1) / kCutThreads;
+    grid = grid < (int64_t)d.sm_count * 8 ? grid : (int64_t)d.sm_count * 8;
+    if (grid > BLOND_STATS_MAX_BLOCKS) grid = BLOND_STATS_MAX_BLOCKS;
+    cut_limits_kernel<T><<<(int)grid, kCutThreads, 0, as_stream(stream)>>>(
+        dt, n, n_sigma, cuts, scratch, ticket);
+    BB_LAUNCH_CHECK();
+    return BLOND_OK;
+}
+
 }  // namespace
 }  // namespace bb
 
@@ -146,6 +282,16 @@ int blond_beam_statistics_f32(const float* dt, const float* dE, const int64_t* i
                               int64_t n, double* stats, double* scratch, int* ticket,
                               void* stream) {
     return stats_impl<float>(dt, dE, id, n, stats, scratch, ticket, stream);
+}
+
+int blond_cut_limits_f64(const double* dt, int64_t n, double n_sigma, double* cuts,
+                         double* scratch, int* ticket, void* stream) {
+    return cut_limits_impl<double>(dt, n, n_sigma, cuts, scratch, ticket, stream);
+}
+
+int blond_cut_limits_f32(const float* dt, int64_t n, double n_sigma, double* cuts,
+                         double* scratch, int* ticket, void* stream) {
+    return cut_limits_impl<float>(dt, n, n_sigma, cuts, scratch, ticket, stream);
 }
 
 }  // extern "C"

@@ -289,27 +289,7 @@ static int histogram_impl(const T* dt, T* out, T cut_left, T cut_right,
 }
 
 // ------------------------------------------------------- smooth histogram
-// histogram.cpp:75-132.  Weights of a particle at f = (dt-cut_left)*inv_w,
-// k = (int)f, d = f-k: bin k gets 0.5-d; bin k+1 (d > 0.5) or k-1 (else)
-// gets 0.5+d.  Accumulated with floating-point atomics, so the summation
-// order (not the set of terms) differs from the reference's.
-template <typename T>
-__device__ __forceinline__ void smooth_weights(T a, T cut_left, T inv_w, T lo,
-                                               T hi, int S, int& k, int& k2,
-                                               double& w1, double& w2) {
-    k = -1;
-    k2 = -1;
-    if (!(a >= lo && a <= hi)) return;  // also rejects NaN
-    const T f = (a - cut_left) * inv_w;
-    k = (int)f;
-    const T d = f - (T)k;
-    k2 = d > T(0.5) ? (int)((double)f + 1.0) : (int)((double)f - 1.0);
-    w1 = 0.5 - (double)d;
-    w2 = 0.5 + (double)d;
-    if (k < 0 || k >= S) k = -1;
-    if (k2 < 0 || k2 >= S) k2 = -1;
-}
-
+// (smooth_weights: common.cuh)
 template <typename T>
 __global__ void __launch_bounds__(kThreads)
 smooth_histogram_kernel(const T* __restrict__ dt, T* __restrict__ out,

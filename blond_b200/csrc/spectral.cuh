@@ -91,6 +91,16 @@ struct SpecParams {
     int table_f32;            // 0: double2 {slope, offset}; 1: float2 {qV, slope}
     double charge, inv_w;     // inv_w = (S-1)/(bc[S-1]-bc[0])
     const double* bc;
+    // interpolated tracker (RingAndRFTracker(interpolation=True),
+    // trackers/tracker.py:586-601): the table interpolates the RF voltage at
+    // the bin centres (rf_volt_comp, kick.cpp:37-51) plus the induced
+    // voltage, with the turn's acceleration kick in the offsets; rf_V/om/ph
+    // are the turn-major [n_turns+1][rf_n] programmes, acc [n_turns]
+    const double* rf_V;       // nullptr: the table holds the induced voltage only
+    const double* rf_om;
+    const double* rf_ph;
+    int rf_n;
+    const double* rf_acc;
     long long* turn;          // device turn counter (read; incremented if bump)
     int bump_turn;
     // twiddle tables precomputed for this plan (make_spec_twiddles), or
@@ -649,6 +659,18 @@ spectral_kernel(const SpecParams P, const typename SpecLoopArg<FB>::type LP) {
     if (!g_table && !P.bump_turn) return;
     if (g_table) {
         const int64_t nt = P.n_out - 1;
+        // interpolated tracker: total voltage = RF voltage at the bin centre
+        // + induced voltage (tracker.py:589-592), acc in the offsets
+        const bool rfi = P.rf_V != nullptr;
+        const double* Vt = rfi ? P.rf_V + turn * P.rf_n : nullptr;
+        const double* omt = rfi ? P.rf_om + turn * P.rf_n : nullptr;
+        const double* pht = rfi ? P.rf_ph + turn * P.rf_n : nullptr;
+        const double acc_t = rfi ? P.rf_acc[turn] : 0.0;
+        auto rfv = [&](double x) {
+            double s = 0.0;
+            for (int j = 0; j < P.rf_n; ++j) s += Vt[j] * sin(omt[j] * x + pht[j]);
+            return s;
+        };
         for (int e = tid; e < per; e += nth) {
             const int b = e % Bc, m1 = e / Bc;
             const int64_t m = (int64_t)c * Bc + b + (int64_t)M2 * m1;
@@ -659,17 +681,21 @@ spectral_kernel(const SpecParams P, const typename SpecLoopArg<FB>::type LP) {
             for (int h = 0; h < 2; ++h) {
                 const int64_t n = 2 * m + h;
                 if (n >= nt) continue;
-                const double a0 = h == 0 ? v0 : v1;
-                const double a1 = h == 0 ? v1 : (b + 1 < Bc ? vloc[e + 1] : nbr[m1]);
+                double a0 = h == 0 ? v0 : v1;
+                double a1 = h == 0 ? v1 : (b + 1 < Bc ? vloc[e + 1] : nbr[m1]);
                 const double bcn = p.prefetch ? bcs[2 * e + h] : g_bc[n];
+                if (rfi) {
+                    a0 = rfv(bcn) + a0;
+                    a1 = rfv(g_bc[n + 1]) + a1;
+                }
                 if (!P.table_f32) {
-                    // linear_interp_kick.cpp:44-47 with acc = 0
+                    // linear_interp_kick.cpp:44-47 (acc = 0 unless interpolated)
                     const double slope = P.charge * (a1 - a0) * inv_w;
-                    const double offset = P.charge * a0 - bcn * slope;
+                    const double offset = (P.charge * a0 - bcn * slope) + acc_t;
                     reinterpret_cast<double2*>(g_table)[n] = make_double2(slope, offset);
                 } else {
                     reinterpret_cast<float2*>(g_table)[n] =
-                        make_float2((float)(P.charge * a0),
+                        make_float2((float)(P.charge * a0 + acc_t),
                                     (float)(P.charge * (a1 - a0) * inv_w));
                 }
             }

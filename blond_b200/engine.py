@@ -135,11 +135,11 @@ class FusedTracker:
                  energy_unit: float | None = None):
         if precision not in PREC:
             raise ValueError(f"precision must be one of {list(PREC)}")
-        if tracker.interpolation:
-            raise NotImplementedError("the fused engine tracks the "
-                                      "non-interpolated kick")
-        if getattr(profile, "smooth", False):
-            raise NotImplementedError("the fused engine deposits with slice_beam")
+        if tracker.interpolation and getattr(tracker, "profile", profile) is not profile:
+            raise ValueError("an interpolated tracker interpolates over its own profile: "
+                             "pass that profile")
+        if getattr(profile, "smooth", False) and process_group is not None:
+            raise NotImplementedError("smooth slicing of a sharded beam")
         rf = tracker.rf_params
         beam = tracker.beam
         self.tracker, self.profile, self.tiv = tracker, profile, total_induced_voltage
@@ -165,6 +165,12 @@ class FusedTracker:
                       float(profile.cut_right), _p(bc))
         if total_induced_voltage is not None:
             self._set_impedance(total_induced_voltage, beam, rf)
+        if tracker.interpolation:
+            # RF + induced voltage interpolated from one table, no RF kick
+            self.eng.call("set_interpolation", 1)
+        if getattr(profile, "smooth", False):
+            # slice_smooth weights, deposited after each particle pass
+            self.eng.call("set_smooth", 1)
         self.loop = getattr(tracker, "beamFB", None)
         # coordinates
         if beam.dt.dtype != torch.float64:

@@ -161,6 +161,22 @@ int blond_beam_statistics_f32(const float* dt, const float* dE,
                               const int64_t* id, int64_t n, double* stats,
                               double* scratch, int* ticket, void* stream);
 
+/* ------------------------------------------------------------ cut limits
+ * replaces the automatic frame of CutOptions.set_cuts() beam/profile.py:185-195
+ * (cut_left and cut_right both None).  Writes 2 doubles to the device array
+ * cuts: n_sigma <= 0 (the reference's None): dt_min - 0.05 (dt_max - dt_min)
+ * and dt_max + 0.05 (dt_max - dt_min), bit-identical to the reference (min
+ * and max are exact, the expressions are evaluated in its order); n_sigma > 0:
+ * mean -/+ n_sigma sigma / 2 with numpy's mean and population std, to
+ * rounding (~1e-16 relative).  NaN in dt gives NaN cuts, as numpy.  The _f32
+ * variant reads float dt and evaluates in float64.  scratch:
+ * BLOND_STATS_SCRATCH doubles, ticket: one int that is 0 before the first
+ * call (0 again after every call). */
+int blond_cut_limits_f64(const double* dt, int64_t n, double n_sigma, double* cuts,
+                         double* scratch, int* ticket, void* stream);
+int blond_cut_limits_f32(const float* dt, int64_t n, double n_sigma, double* cuts,
+                         double* scratch, int* ticket, void* stream);
+
 /* ------------------------------------------------------------ impedance setup
  * replaces fast_resonator_real_imag() cpp_routines/fast_resonator.cpp:19-74
  * re/im accumulate (+= / -=); index 0 (DC) is untouched. */
@@ -305,6 +321,21 @@ int blond_engine_bind_beam(blond_engine* engine, void* dt, void* dE,
  * multiple of this unit; the grid spans +-(2^31 - 1) units, and a particle
  * leaving it is reported by blond_engine_check as BLOND_ERR_RANGE. */
 int blond_engine_set_energy_unit(blond_engine* engine, double lsb);
+/* RingAndRFTracker(interpolation=True) (trackers/tracker.py:586-601): each
+ * turn's head interpolates the RF voltage at the bin centres (rf_volt_comp,
+ * kick.cpp:37-51) plus the induced voltage, with the turn's acceleration
+ * kick in the offsets (linear_interp_kick.cpp:44-47), and the particle pass
+ * applies that one interpolated kick instead of the RF kick.  on = 0/1.
+ * Not with the SPS_RL beam-phase loop, nor with another loop unless there
+ * is an FFT impedance. */
+int blond_engine_set_interpolation(blond_engine* engine, int on);
+/* Profile with OtherSlicesOptions(smooth=True) (beam/profile.py:764-773):
+ * each turn ends with a deposit pass of the reference's slice_smooth
+ * weights (histogram.cpp:75-132) accumulated in 64-bit fixed point (2^-b
+ * per unit weight, b = min(52, 62 - ceil(log2(1.5 n + 2))); the same bits
+ * every run), which is the profile the next turn's induced voltage uses.
+ * on = 0/1.  Not with a beam-phase loop or a bound (sharded) histogram. */
+int blond_engine_set_smooth(blond_engine* engine, int on);
 int blond_engine_set_turn(blond_engine* engine, int64_t turn, void* stream);
 /* Re-slice the bound beam into the profile (Profile.track()). */
 int blond_engine_slice(blond_engine* engine, void* stream);

@@ -35,6 +35,8 @@ mtw_tracks.npz        multi-turn wakes in mtw_mode 'time' (InducedVoltageFreq,
                       InducedVoltageTime) tracked over several turns.
 profile_fits.npz      Profile fit options 'gaussian', 'rms', 'fwhm'.
 beam_phase.npz        the reference's compiled beam_phase / beam_phase_fast.
+cut_options.npz       CutOptions.set_cuts without given cuts (default and
+                      n_sigma frames) on the unit-test dt and a bigaussian.
 beam_feedback.npz     BeamFeedback (every machine type) tracked for 200 turns:
                       per-turn beam phase, phase error, frequency correction,
                       mean dt, the final RF frequency/phase rows and a sample
@@ -630,6 +632,29 @@ def gen_beam_feedback():
     save("beam_feedback.npz", **out)
 
 
+def gen_cut_options():
+    """CutOptions.set_cuts (beam/profile.py:175-211) without given cuts --
+    the default frame (min/max -/+ 5 %) and n_sigma frames -- on the
+    reference's unit-test dt and on a seeded bigaussian bunch."""
+    dt_unit = np.load(os.path.join(
+        REF, "unittests/beam_profile/dt_coordinates.npz"))["arr_0"]
+    ring, rf = c1_machine(10)
+    bunch = Beam(ring, 20000, 1e10)
+    bigaussian(ring, rf, bunch, 0.4e-9, seed=11)
+    # the unit-test dt is profile_golden.npz's `dt`
+    out = {"dt_bunch": np.array(bunch.dt)}
+    for name, dt in (("unit", dt_unit), ("bunch", np.array(bunch.dt))):
+        b = Beam(ring, len(dt), 1e10)
+        b.dt = dt
+        for tag, kw in (("default", {}), ("nsigma3", {"n_sigma": 3}),
+                        ("nsigma55", {"n_sigma": 5.5})):
+            co = CutOptions(n_slices=64, **kw)
+            co.set_cuts(b)
+            out[f"{name}_{tag}"] = np.array([co.cut_left, co.cut_right])
+            out[f"{name}_{tag}_bc"] = np.array(co.bin_centers)
+    save("cut_options.npz", **out)
+
+
 def run_reference_profile_test():
     """Run the reference's own profile unit test (its literal expected
     counts) against oracle/_ref before the fixture is trusted."""
@@ -646,6 +671,10 @@ def run_reference_profile_test():
 
 if __name__ == "__main__":
     bm.use_cpp()
+    if len(sys.argv) > 1:  # only the named generators, e.g. gen_cut_options
+        for name in sys.argv[1:]:
+            globals()[name]()
+        sys.exit(0)
     run_reference_profile_test()
     gen_profile_golden()
     gen_kernels()

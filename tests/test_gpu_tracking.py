@@ -401,3 +401,100 @@ def test_track_host_matches_device_tracking(cuda, precision, chunks):
     if precision == "f64":
         assert normwise(out[1][0], g["dt"]) < 1e-11
         np.testing.assert_array_equal(out[1][2], g["profiles"][-1])
+
+
+@pytest.mark.parametrize("turns_per_graph", [1, 4])
+@pytest.mark.parametrize("kernel", ["plain", "tma"])
+def test_fused_interpolated_tracker_matches_reference(cuda, turns_per_graph, kernel):
+    """RingAndRFTracker(interpolation=True) through the fused engine: the
+    head interpolates RF voltage at the bin centres + induced voltage, the
+    particle pass applies that one kick (tracker.py:586-601), against the
+    reference objects' run (track_interp.npz)."""
+    name = "track_interp.npz"
+    g = golden(name)
+    ring, rf, beam = build(g)
+    prof = make_profile(g, beam)
+    tiv = TotalInducedVoltage(beam, prof, impedance_objects(name, beam, prof, rf))
+    tracker = RingAndRFTracker(rf, beam, solver=str(g["solver"][0]), interpolation=True,
+                               profile=prof, total_induced_voltage=tiv)
+    fused = FusedTracker(tracker, prof, tiv, precision="f64",
+                         turns_per_graph=turns_per_graph, kernel=kernel)
+    nt = int(g["n_turns"][0])
+    fused.track(nt - 1)
+    assert normwise(fused.induced_voltage_tensor().cpu().numpy(), g["vind"][nt - 2]) < 1e-10
+    np.testing.assert_array_equal(fused.profile_tensor().cpu().numpy(), g["profiles"][nt - 1])
+    fused.track(1)
+    assert normwise(beam.dt.cpu().numpy(), g["dt"]) < 1e-11
+    assert normwise(beam.dE.cpu().numpy(), g["dE"]) < 1e-11
+    np.testing.assert_array_equal(fused.profile_tensor().cpu().numpy(), g["profiles"][-1])
+
+
+@pytest.mark.parametrize("precision", ["f64", "q32p64"])
+def test_fused_interpolated_tracker_without_impedance(cuda, precision):
+    """Interpolated RF kick only (no induced voltage), double RF with an
+    acceleration-free programme: the fused engine against the drop-in
+    objects (bmath rf_volt_comp + linear_interp_kick, turn by turn)."""
+    n, S, turns = 20001, 300, 6
+    res = []
+    for fused_path in (False, True):
+        ring = Ring(6911.5, 1 / 18**2, 26e9, Proton(), turns)
+        rf = RFStation(ring, [4620, 4 * 4620], [4.5e6, 0.45e6], [0.0, np.pi], n_rf=2)
+        centre = (rf.phi_s[0] - rf.phi_rf[0, 0]) / rf.omega_rf[0, 0]
+        from blond_b200.beam.distributions import bigaussian_arrays
+        rng = np.random.default_rng(3)
+        dt0 = centre + 0.5e-9 * rng.standard_normal(n)
+        dE0 = 2e7 * rng.standard_normal(n)
+        beam = Beam(ring, n, 1e10, dt=dt0, dE=dE0)
+        prof = Profile(beam, CutOptions(cut_left=centre - 1.5e-9, cut_right=centre + 1.5e-9,
+                                        n_slices=S))
+        tracker = RingAndRFTracker(rf, beam, interpolation=True, profile=prof)
+        if fused_path:
+            f = FusedTracker(tracker, prof, precision=precision, turns_per_graph=4)
+            f.track(turns)
+            f.sync()
+        else:
+            for _ in range(turns):
+                tracker.track()
+                prof.track()
+        res.append((beam.dt.cpu().numpy(), beam.dE.cpu().numpy(),
+                    prof.n_macroparticles.cpu().numpy()))
+    (dt_a, dE_a, p_a), (dt_b, dE_b, p_b) = res
+    tol = 1e-12 if precision == "f64" else 1e-8
+    assert normwise(dt_b, dt_a) < tol
+    assert normwise(dE_b, dE_a) < tol
+    if precision == "f64":
+        np.testing.assert_array_equal(p_b, p_a)
+    else:
+        assert np.abs(p_b - p_a).sum() <= 4
+
+
+@pytest.mark.parametrize("kernel", ["plain", "tma"])
+def test_fused_smooth_slicing_matches_reference(cuda, kernel):
+    """Profile(smooth=True) through the fused engine: the slice_smooth
+    weights (histogram.cpp:75-132, negative entries included) deposited in
+    64-bit fixed point after every particle pass, the induced voltage of
+    that profile, against the reference objects' run (track_smooth.npz):
+    coordinates 1e-11, profiles and induced voltages 1e-10 normwise; two
+    runs give the same bits."""
+    name = "track_smooth.npz"
+    g = golden(name)
+    out = []
+    for _ in range(2):
+        ring, rf, beam = build(g)
+        prof = make_profile(g, beam, smooth=True)
+        tiv = TotalInducedVoltage(beam, prof, impedance_objects(name, beam, prof, rf))
+        fused = FusedTracker(RingAndRFTracker(rf, beam, solver=str(g["solver"][0])), prof,
+                             tiv, precision="f64", turns_per_graph=2, kernel=kernel)
+        nt = int(g["n_turns"][0])
+        assert normwise(fused.profile_tensor().cpu().numpy(), g["profiles"][0]) < 1e-10
+        fused.track(nt - 1)
+        assert normwise(fused.induced_voltage_tensor().cpu().numpy(), g["vind"][nt - 2]) < 1e-10
+        fused.track(1)
+        assert normwise(beam.dt.cpu().numpy(), g["dt"]) < 1e-11
+        assert normwise(beam.dE.cpu().numpy(), g["dE"]) < 1e-11
+        p = fused.profile_tensor().cpu().numpy()
+        assert normwise(p, g["profiles"][-1]) < 1e-10
+        assert p.min() < 0 or g["profiles"][-1].min() >= 0
+        out.append((beam.dt.cpu().numpy(), p))
+    for a, b in zip(*out):
+        np.testing.assert_array_equal(a, b)
