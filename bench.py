@@ -57,7 +57,7 @@ def parse():
                     help="leave the C3 batch out of the default line")
     ap.add_argument("--batched-error-turns", type=int, default=1000,
                     help="turns after which the batched forms' rms errors are taken")
-    ap.add_argument("--kernel", default="auto", choices=["auto", "tma", "plain"])
+    ap.add_argument("--kernel", default="auto", choices=["auto", "tma", "plain", "stab"])
     ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5", "mtw"],
                     help="c2: the single-beam pipeline (default, the headline); "
                          "c3: 256-beam double-RF batch; c4: adjoint gradient; "
@@ -321,8 +321,8 @@ def build_fused(n, S, n_turns, precision, kernel="auto", seed=0, group=None, sha
     else:
         threads, bps, ring = shape
         fused = FusedTracker(tracker, prof, tiv, precision=precision, turns_per_graph=50,
-                             kernel="plain", threads=threads, blocks_per_sm=bps,
-                             process_group=group, tune="fixed")
+                             kernel="plain" if kernel == "auto" else kernel, threads=threads,
+                             blocks_per_sm=bps, process_group=group, tune="fixed")
         fused.eng.call("set_prefetch", ring)
     return fused, beam, iv.n_fft
 
@@ -442,7 +442,7 @@ def run_ours(args, world, rank, local):
             del fused, beam
         torch.cuda.empty_cache()
         T = max(args.batched_error_turns, W + K)
-        m = c3_measure(256, W, K, T, control=False)
+        m = c3_measure(256, W, K, T, controls=("shift",))
         q, f32, f64 = (m["runs"][k] for k in ("q32p64", "f32p64", "f64"))
         nt = m["n_total"]
         pp = q["autotuned"]["particle_pass_ms"]
@@ -466,6 +466,11 @@ def run_ours(args, world, rank, local):
                        "beams_within_1e-5": int(np.sum(ef.max(axis=1) <= 1e-5)),
                        "max_rel_err": float(ef.max())},
             "f64": {"value": f64["value"], "ms_per_step": f64["ms_per_step"]},
+            "control_fp64_dE_plus_0.01eV": {
+                "what": "FP64 from energies moved by 0.01 eV vs FP64: the beams' own "
+                        "sensitivity after the same turns",
+                "beams_within_1e-5": int(np.sum(m["controls"]["shift"].max(axis=1) <= 1e-5)),
+                "max_rel_err": float(m["controls"]["shift"].max())},
         }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, turns, kind, cores, sec = cpu_reference(n, S, None, args.cpu_seconds)
@@ -704,13 +709,15 @@ def _err_summary(errs):
 
 
 def c3_measure(n_beams, W, K, T_err, precisions=("q32p64", "f32p64", "f64"),
-               control=True, unbatched=False):
+               controls=("ulp", "shift"), unbatched=False):
     """C3: every precision batched (autotuned launch shape, graph-replayed
     turns), timed over K turns after W, then tracked on (untimed) to turn
     T_err, where each form's per-beam rms errors against FP64 are taken.
-    control: FP64 again from initial times moved by one ulp -- how far the
-    dynamics alone separate two runs that differ by rounding.  unbatched:
-    every beam through its own FP64 engine, one after the other."""
+    controls -- how far the dynamics alone separate two FP64 runs: "ulp",
+    FP64 again from initial times moved by one ulp (no bin changes);
+    "shift", FP64 from initial energies moved by 0.01 eV (1e-10 of the
+    spread, ten times below the Q32P64 grid).  unbatched: every beam
+    through its own FP64 engine, one after the other."""
     import torch
     from blond_b200.batch import BatchTracker
     from blond_b200.engine import FusedTracker
@@ -738,15 +745,18 @@ def c3_measure(n_beams, W, K, T_err, precisions=("q32p64", "f32p64", "f64"),
             if prec != "f64":
                 out.setdefault("errors", {})[prec] = _c3_rel_errs(
                     beams, trackers[prec], trackers["f64"])
-        if control:
+        for ctl in controls:
             bp = BatchTracker([(RingAndRFTracker(rf, b), p, t) for rf, b, p, t in beams],
                               precision="f64")
-            bp.dt.copy_(torch.nextafter(bp.dt, torch.full_like(bp.dt, float("inf"))))
+            if ctl == "ulp":
+                bp.dt.copy_(torch.nextafter(bp.dt, torch.full_like(bp.dt, float("inf"))))
+            else:
+                bp.dE.add_(0.01)
             bp._call("slice", ct_stream())
             bp.track(T_err)
             for rf, _, _, _ in beams:
                 rf.counter[0] = 0
-            out["control"] = _c3_rel_errs(beams, bp, trackers["f64"])
+            out.setdefault("controls", {})[ctl] = _c3_rel_errs(beams, bp, trackers["f64"])
             del bp
     del trackers
     torch.cuda.empty_cache()
@@ -1140,7 +1150,8 @@ def main():
                 "turns": m["turns"],
                 "statistic": "in-window rms of dt and dE, per beam, vs the FP64 batch",
                 **{k: _err_summary(v) for k, v in m["errors"].items()},
-                "control_fp64_one_ulp": _err_summary(m["control"])},
+                "control_fp64_one_ulp": _err_summary(m["controls"]["ulp"]),
+                "control_fp64_dE_plus_0.01eV": _err_summary(m["controls"]["shift"])},
             "gpu_launches": 2 * K,
         }), flush=True)
         return

@@ -96,7 +96,40 @@ template <> struct Vec2<double> { using type = double2; };
 template <> struct Vec2<float> { using type = float2; };
 template <> struct Vec2<int> { using type = int2; };
 
-__device__ __forceinline__ double dev_sin(double x) { return sin(x); }
+// sin(x) of an RF phase argument.  The FP64 particle passes spend much of
+// their issue slots on this sine, so it is written for the arguments they
+// see (|x| up to ~1e3 rad): Cody-Waite reduction by pi (W. J. Cody and
+// W. Waite, "Software Manual for the Elementary Functions", 1980) with pi
+// split in three parts -- the first two with 30 significant bits, so k P1
+// and k P2 are exact for |k| < 2^23 -- to r in [-pi/2, pi/2], then the
+// Taylor series of sin through r^21 (the next term is below 1.2e-18 on that
+// interval) by Horner's rule in r^2, and sin(x) = (-1)^k sin(r).  No
+// branch on the quadrant, so a warp's particles stay converged.  Beyond
+// |x| = 1e7 (and for NaN / inf) CUDA's sin is used.  Within a few units in
+// the last place of the correctly rounded sine (tested against numpy).
+__device__ __forceinline__ double rf_sin(double x) {
+    if (!(fabs(x) < 1e7)) return sin(x);
+    const double k = rint(x * 0.3183098861837907);  // 1 / pi
+    double r = fma(-k, 3.1415926553308964, x);       // P1
+    r = fma(-k, -1.7411031384001463e-09, r);          // P2
+    r = fma(-k, -7.00686879617986e-19, r);            // P3
+    const double r2 = r * r;
+    // (-1)^n / (2n + 1)!, n = 10 .. 1
+    double p = 1.9572941063391263e-20;
+    p = fma(p, r2, -8.22063524662433e-18);
+    p = fma(p, r2, 2.8114572543455206e-15);
+    p = fma(p, r2, -7.647163731819816e-13);
+    p = fma(p, r2, 1.6059043836821613e-10);
+    p = fma(p, r2, -2.505210838544172e-08);
+    p = fma(p, r2, 2.7557319223985893e-06);
+    p = fma(p, r2, -0.0001984126984126984);
+    p = fma(p, r2, 0.008333333333333333);
+    p = fma(p, r2, -0.16666666666666666);
+    const double s = fma(r * r2, p, r);
+    return (static_cast<long long>(k) & 1) ? -s : s;
+}
+
+__device__ __forceinline__ double dev_sin(double x) { return rf_sin(x); }
 __device__ __forceinline__ float dev_sin(float x) { return sinf(x); }
 __device__ __forceinline__ double dev_floor(double x) { return floor(x); }
 __device__ __forceinline__ float dev_floor(float x) { return floorf(x); }
@@ -114,6 +147,47 @@ __device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(
 __device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
 __device__ __forceinline__ double div_rn(double a, double b) { return __ddiv_rn(a, b); }
 __device__ __forceinline__ float div_rn(float a, float b) { return __fdiv_rn(a, b); }
+
+// Bin centre i of S slices over [lo, hi] as the reference's Profile forms
+// it (beam/profile.py:207-211): edges = numpy.linspace(lo, hi, S + 1),
+// which numpy evaluates as i * step + lo with step = (hi - lo) / S and the
+// last edge set to hi; centre i = (edge_i + edge_{i+1}) / 2.  Every
+// operation rounds on its own (no contraction), on the host and the device,
+// so both give numpy's bits.
+__host__ __device__ inline double linspace_edge(double lo, double hi, int S, int i) {
+    if (i >= S) return hi;
+#ifdef __CUDA_ARCH__
+    const double step = __ddiv_rn(__dsub_rn(hi, lo), (double)S);
+    return __dadd_rn(__dmul_rn((double)i, step), lo);
+#else
+    const volatile double step = (hi - lo) / (double)S;
+    const volatile double x = (double)i * step;
+    return x + lo;
+#endif
+}
+__host__ __device__ inline double linspace_centre(double lo, double hi, int S, int i) {
+#ifdef __CUDA_ARCH__
+    return __dmul_rn(__dadd_rn(linspace_edge(lo, hi, S, i), linspace_edge(lo, hi, S, i + 1)),
+                     0.5);
+#else
+    const volatile double sum = linspace_edge(lo, hi, S, i) + linspace_edge(lo, hi, S, i + 1);
+    return sum / 2;
+#endif
+}
+
+// Entry k of the induced kick's interpolation table from the voltages at bin
+// centres k and k+1 (linear_interp_kick.cpp:44-47):
+//   slope  = charge (V_{k+1} - V_k) inv_w
+//   offset = (charge V_k - bc_k slope) + acc
+// every operation rounded on its own, so the head kernel that writes the
+// table and a particle pass that forms entries from a voltage-only copy give
+// the same bits.
+__device__ __forceinline__ double2 lik_entry(double v0, double v1, double bc, double charge,
+                                             double inv_w, double acc) {
+    const double slope = __dmul_rn(__dmul_rn(charge, __dsub_rn(v1, v0)), inv_w);
+    const double offset = __dadd_rn(__dsub_rn(__dmul_rn(charge, v0), __dmul_rn(bc, slope)), acc);
+    return make_double2(slope, offset);
+}
 
 // ------------------------------------------------------ smooth deposit weights
 // histogram.cpp:75-132.  Weights of a particle at f = (dt-cut_left)*inv_w,

@@ -38,6 +38,9 @@ struct blond_engine {
     double cut_left = 0, cut_right = 0, inv_w = 0;
     double* d_bc = nullptr;
     double bc0 = 0, lik_inv_w = 0, bw = 0, dbc = 0;
+    // the bin centres are numpy.linspace midpoints of the cuts, bit for bit
+    // (the shared-table pass recomputes them)
+    bool bc_linspace = false;
     // impedance
     bool has_fft = false;
     SpecPlan plan = {};
@@ -82,7 +85,8 @@ struct blond_engine {
     int threads = 512;
     int blocks_per_sm = 2;
     int turns_per_graph = 50;
-    int variant = 0;  // 0: TMA-pipelined particle pass, 1: plain loads
+    int variant = 0;  // 0: TMA-pipelined particle pass, 1: plain loads,
+                      // 2: plain loads with the table in shared memory
     int hist_mode = -1;  // -1 automatic, else HIST_AGG/I32/PACKED/GLOBAL
     int ring = 0;        // plain pass: prefetch ring stages (0 = direct loads)
     int cluster = 1;     // plain pass: blocks whose histograms merge on chip
@@ -245,9 +249,66 @@ static int plain_ring_smem(const blond_engine* e, int ring) {
     return bytes <= limit ? bytes : -1;
 }
 
+// Dynamic shared memory of the shared-table pass (table, packed histogram,
+// ring), or -1 when the pass does not apply: it needs the head's induced
+// voltage alone as the table source (an FFT impedance, no interpolated RF
+// voltage), integer deposits, linspace bin centres, and room for it all.
+template <int PREC>
+static int stab_smem(const blond_engine* e, int ring) {
+    if (!e->has_fft || e->interp || e->smooth || !e->bc_linspace) return -1;
+    const size_t bytes = pad16(stab_table_bytes<PREC>(e->S)) +
+                         pad16((size_t)((e->S + 1) / 2) * 4) +
+                         (size_t)ring * kEngineThreads * ring_bytes<PREC>();
+    const size_t limit = (size_t)device_info().max_smem_optin - sizeof(TurnConsts) - 1024;
+    return bytes <= limit ? (int)bytes : -1;
+}
+
+template <int PREC, int SOLVER>
+static int launch_stab(blond_engine* e, const ParticleArgs& a, cudaStream_t s, bool launch) {
+    const int ring = e->ring ? 2 : 0;
+    const int smem = stab_smem<PREC>(e, ring);
+    if (smem < 0) {
+        set_error("engine: the shared-table pass does not apply to this engine");
+        return BLOND_ERR_UNSUPPORTED;
+    }
+    auto k = ring ? particle_kernel_stab<PREC, SOLVER, 2> : particle_kernel_stab<PREC, SOLVER, 0>;
+    int rc;
+    if ((rc = allow_smem_once(k))) return rc;
+    if (launch) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(device_info().sm_count, 1, 1);
+        cfg.blockDim = dim3(kEngineThreads, 1, 1);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = s;
+        cudaLaunchAttribute attr[1];
+        int na = 0;
+        if (e->pdl) {
+            attr[na].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+            attr[na].val.programmaticStreamSerializationAllowed = 1;
+            ++na;
+        }
+        cfg.attrs = attr;
+        cfg.numAttrs = na;
+        BB_CUDA(cudaLaunchKernelEx(&cfg, k, a));
+    }
+    BB_LAUNCH_CHECK();
+    return BLOND_OK;
+}
+
 template <int PREC, int SOLVER, bool LIK, bool KICK>
 static int launch_particles_t(blond_engine* e, const ParticleArgs& a, cudaStream_t s,
                               bool launch) {
+    if constexpr (KICK) {
+        if (e->variant == 2) {
+            if constexpr (LIK) {
+                return launch_stab<PREC, SOLVER>(e, a, s, launch);
+            } else {
+                set_error("engine: the shared-table pass does not apply to this engine "
+                          "(no interpolated kick)");
+                return BLOND_ERR_UNSUPPORTED;
+            }
+        }
+    }
     const int smem = engine_smem(e);
     const bool agg = plain_agg(e);
     int rc;
@@ -310,7 +371,8 @@ template <int PREC>
 static int launch_particles_p(blond_engine* e, const ParticleArgs& a, bool kick,
                               cudaStream_t s, bool launch) {
     if (!kick) return launch_particles_t<PREC, 0, false, false>(e, a, s, launch);
-    const bool lik = e->has_fft || e->has_ind;
+    // the interpolated tracker kicks through the table even without impedance
+    const bool lik = e->has_fft || e->has_ind || e->interp;
     switch (e->solver) {
         case 0:
             return lik ? launch_particles_t<PREC, 0, true, true>(e, a, s, launch)
@@ -356,6 +418,9 @@ static ParticleArgs particle_args(blond_engine* e) {
         a.interp = 1;
     }
     a.no_deposit = e->smooth ? 1 : 0;
+    a.vind = e->d_vind;
+    a.cut_right = e->cut_right;
+    a.bc_step = (e->cut_right - e->cut_left) / (double)e->S;
     return a;
 }
 
@@ -534,56 +599,66 @@ static int launch_head(blond_engine* e, cudaStream_t s) {
     return launch_feedback_turn(a, nullptr, e->d_fb_ticket, 0, s);
 }
 
-// Head of an interpolated turn without an impedance (tracker.py:586-601
-// with total_voltage = rf_voltage): profile <- histogram (cleared), the
-// interpolation table of the RF voltage at the bin centres (rf_volt_comp,
-// kick.cpp:37-51) with the turn's acceleration kick in the offsets
-// (linear_interp_kick.cpp:44-47), turn counter += 1.  One CTA, so every
-// thread reads the counter before thread 0 moves it.
+// The interpolated tracker's table (tracker.py:586-601): the RF voltage at
+// the bin centres (rf_volt_comp, kick.cpp:37-51) plus the induced voltage
+// (vind, when there is an impedance: the head wrote it), with the turn's
+// acceleration kick in the offsets (linear_interp_kick.cpp:44-47).  Without
+// an impedance this kernel is the whole head: it also converts (and clears)
+// the histogram and advances the turn counter -- then it runs as one CTA,
+// so every thread reads the counter before thread 0 moves it.  After a
+// spectral head (which advanced the counter) it reads turn - 1.
 __global__ void __launch_bounds__(1024)
-interp_head_kernel(int* hist, double* profile, int S, long long* turn_p, const double* V,
-                   const double* om, const double* ph, int n_rf, const double* acc,
-                   const double* bc, double charge, double inv_w, void* table,
-                   int table_f32, long long n_turns) {
-    long long turn = *turn_p;
+interp_table_kernel(int* hist, double* profile, int S, long long* turn_p, int head,
+                    const double* V, const double* om, const double* ph, int n_rf,
+                    const double* acc, const double* bc, const double* vind, double charge,
+                    double inv_w, void* table, int table_f32, long long n_turns) {
+    long long turn = *turn_p - (head ? 0 : 1);
+    if (turn < 0) turn = 0;
     if (turn >= n_turns) turn = n_turns - 1;
-    for (int k = threadIdx.x; k < S; k += blockDim.x) {
-        profile[k] = (double)hist[k];
-        hist[k] = 0;
-    }
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+    if (head)
+        for (int k = tid; k < S; k += nth) {
+            profile[k] = (double)hist[k];
+            hist[k] = 0;
+        }
     const double* Vt = V + turn * n_rf;
     const double* omt = om + turn * n_rf;
     const double* pht = ph + turn * n_rf;
     const double acc_t = acc[turn];
-    auto rfv = [&](double x) {
+    auto total = [&](int k) {
         double s = 0.0;
-        for (int j = 0; j < n_rf; ++j) s += Vt[j] * sin(omt[j] * x + pht[j]);
-        return s;
+        for (int j = 0; j < n_rf; ++j) s += Vt[j] * rf_sin(omt[j] * bc[k] + pht[j]);
+        return vind ? s + vind[k] : s;  // rf_voltage + induced_voltage
     };
-    for (int n = threadIdx.x; n < S - 1; n += blockDim.x) {
-        const double a0 = rfv(bc[n]), a1 = rfv(bc[n + 1]);
+    for (int n = tid; n < S - 1; n += nth) {
+        const double a0 = total(n), a1 = total(n + 1);
         if (!table_f32) {
-            const double slope = charge * (a1 - a0) * inv_w;
-            const double offset = (charge * a0 - bc[n] * slope) + acc_t;
-            reinterpret_cast<double2*>(table)[n] = make_double2(slope, offset);
+            reinterpret_cast<double2*>(table)[n] = lik_entry(a0, a1, bc[n], charge, inv_w, acc_t);
         } else {
             reinterpret_cast<float2*>(table)[n] =
                 make_float2((float)(charge * a0 + acc_t), (float)(charge * (a1 - a0) * inv_w));
         }
     }
-    __syncthreads();
-    if (threadIdx.x == 0) *turn_p = *turn_p + 1;
+    if (head) {
+        __syncthreads();
+        if (threadIdx.x == 0) *turn_p = *turn_p + 1;
+    }
+}
+
+static int launch_interp_table(blond_engine* e, cudaStream_t s, bool head) {
+    const int grid = head ? 1 : std::min(device_info().sm_count, (e->S + 255) / 256);
+    interp_table_kernel<<<grid, head ? 1024 : 256, 0, s>>>(
+        e->d_hist, e->d_profile, e->S, e->d_turn, head ? 1 : 0, e->d_V, e->d_om, e->d_ph,
+        e->n_rf, e->d_acc, e->d_bc, head ? nullptr : e->d_vind, e->charge, e->lik_inv_w,
+        e->d_table, e->precision == BLOND_PREC_F32P64 ? 1 : 0, e->n_turns);
+    BB_LAUNCH_CHECK();
+    return BLOND_OK;
 }
 
 static int launch_spectral_head(blond_engine* e, cudaStream_t s, bool loop) {
     if (!(e->has_fft || e->has_ind)) {
         if (!e->interp) return launch_profile(e, true, s);
-        interp_head_kernel<<<1, 1024, 0, s>>>(
-            e->d_hist, e->d_profile, e->S, e->d_turn, e->d_V, e->d_om, e->d_ph, e->n_rf,
-            e->d_acc, e->d_bc, e->charge, e->lik_inv_w, e->d_table,
-            e->precision == BLOND_PREC_F32P64 ? 1 : 0, e->n_turns);
-        BB_LAUNCH_CHECK();
-        return BLOND_OK;
+        return launch_interp_table(e, s, true);
     }
     if (!e->has_fft) {
         set_error("engine: an inductive impedance needs an FFT impedance in this build");
@@ -610,23 +685,22 @@ static int launch_spectral_head(blond_engine* e, cudaStream_t s, bool loop) {
     P.charge = e->charge;
     P.inv_w = e->lik_inv_w;
     P.bc = e->d_bc;
-    if (e->interp) {
-        P.rf_V = e->d_V;
-        P.rf_om = e->d_om;
-        P.rf_ph = e->d_ph;
-        P.rf_n = e->n_rf;
-        P.rf_acc = e->d_acc;
-    }
     P.turn = e->d_turn;
     P.bump_turn = 1;
     P.twg = e->d_tw;
+    // the interpolated tracker's table (RF + induced voltage) follows the head
+    if (e->interp) P.table = nullptr;
+    int rc;
     if (loop) {
         SpecLoop L;
         L.ticket = e->d_fb_ticket;
         L.fb = fb_args(e);
-        return launch_spectral_loop(P, L, s);
+        rc = launch_spectral_loop(P, L, s);
+    } else {
+        rc = launch_spectral(P, s);
     }
-    return launch_spectral(P, s);
+    if (rc || !e->interp) return rc;
+    return launch_interp_table(e, s, false);
 }
 
 static int launch_turn(blond_engine* e, cudaStream_t s) {
@@ -798,6 +872,9 @@ int blond_engine_set_slicing(blond_engine* e, double cut_left, double cut_right,
     e->lik_inv_w = (S - 1) / (bc[S - 1] - bc[0]);  // linear_interp_kick.cpp:31-33
     e->bw = 1.0 / e->lik_inv_w;
     e->dbc = bc[1] - bc[0];
+    e->bc_linspace = true;
+    for (int k = 0; k < S && e->bc_linspace; ++k)
+        e->bc_linspace = bc[k] == linspace_centre(cut_left, cut_right, S, k);
     int rc = upload((void**)&e->d_bc, bc, sizeof(double) * S);
     if (rc) return rc;
     e->slicing_set = true;
@@ -953,7 +1030,8 @@ int blond_engine_step(blond_engine* e, int part, void* stream) {
 }
 
 int blond_engine_set_kernel(blond_engine* e, int variant) {
-    BB_CHECK_ARG(e && (variant == 0 || variant == 1), "engine_set_kernel: variant 0 or 1");
+    BB_CHECK_ARG(e && variant >= 0 && variant <= 2,
+                 "engine_set_kernel: variant 0 (staged), 1 (plain) or 2 (shared table)");
     e->variant = variant;
     e->graph_dirty = true;
     return BLOND_OK;
@@ -1087,6 +1165,11 @@ int blond_engine_autotune(blond_engine* e, int reps, void* stream, int* config,
         const TmaPlan p = f64 ? tma_plan<PREC_F64>(e->S, h) : tma_plan<PREC_F32P64>(e->S, h);
         if (p.stages) cands.push_back({0, kTmaThreads, 1, h, 0, 1});
     }
+    // the shared-table pass (packed histogram), with and without the ring
+    for (int ring : {0, 2}) {
+        const int sm = f64 ? stab_smem<PREC_F64>(e, ring) : stab_smem<PREC_F32P64>(e, ring);
+        if (sm >= 0) cands.push_back({2, kEngineThreads, 1, HIST_PACKED, ring, 1});
+    }
     const Cand old = {e->variant, e->threads, e->blocks_per_sm, e->hist_mode, e->ring,
                       e->cluster};
     cudaEvent_t a = nullptr, b = nullptr;
@@ -1152,8 +1235,8 @@ int blond_engine_autotune(blond_engine* e, int reps, void* stream, int* config,
     e->cluster = use.cluster;
     e->graph_dirty = true;
     config[0] = use.variant;
-    config[1] = use.variant == 0 ? kTmaThreads : use.threads;
-    config[2] = use.variant == 0 ? 1 : use.bps;
+    config[1] = use.variant == 1 ? use.threads : (use.variant == 0 ? kTmaThreads : kEngineThreads);
+    config[2] = use.variant == 1 ? use.bps : 1;
     config[3] = use.hist;
     config[4] = use.ring;
     config[5] = use.cluster;
@@ -1514,33 +1597,6 @@ static NoAllocScratch* noalloc_scratch() {
         ptr[dev] = reinterpret_cast<NoAllocScratch*>(p);
     }
     return ptr[dev];
-}
-
-// Bin centre i of S slices over [lo, hi] as the reference's Profile forms
-// it (beam/profile.py:207-211): edges = numpy.linspace(lo, hi, S + 1),
-// which numpy evaluates as i * step + lo with step = (hi - lo) / S and the
-// last edge set to hi; centre i = (edge_i + edge_{i+1}) / 2.  Every
-// operation rounds on its own (no contraction), on the host and the device,
-// so both give numpy's bits.
-__host__ __device__ inline double linspace_edge(double lo, double hi, int S, int i) {
-    if (i >= S) return hi;
-#ifdef __CUDA_ARCH__
-    const double step = __ddiv_rn(__dsub_rn(hi, lo), (double)S);
-    return __dadd_rn(__dmul_rn((double)i, step), lo);
-#else
-    const volatile double step = (hi - lo) / (double)S;
-    const volatile double x = (double)i * step;
-    return x + lo;
-#endif
-}
-__host__ __device__ inline double linspace_centre(double lo, double hi, int S, int i) {
-#ifdef __CUDA_ARCH__
-    return __dmul_rn(__dadd_rn(linspace_edge(lo, hi, S, i), linspace_edge(lo, hi, S, i + 1)),
-                     0.5);
-#else
-    const volatile double sum = linspace_edge(lo, hi, S, i) + linspace_edge(lo, hi, S, i + 1);
-    return sum / 2;
-#endif
 }
 
 // This call's constants, passed to the set-up kernel by value.

@@ -63,6 +63,11 @@ struct ParticleArgs {
     // smooth slicing: a separate deposit pass makes the profile, this pass
     // deposits nothing
     int no_deposit;
+    // shared-table pass (particle_kernel_stab): the induced voltage the head
+    // wrote, and the slicing frame whose numpy.linspace midpoints are the
+    // bin centres (bc_step = (cut_right - cut_left) / S)
+    const double* vind;
+    double cut_right, bc_step;
 };
 
 enum { PREC_F64 = 0, PREC_F32P64 = 1, PREC_Q32P64 = 2 };
@@ -100,6 +105,33 @@ __device__ __forceinline__ int q32_add(int q, double inc, const ParticleArgs& a)
     return (int)r;
 }
 
+// Table sources of the induced kick: the global table the head wrote, or a
+// copy in shared memory (F64 / Q32P64: the induced voltage only, entries
+// formed per particle with lik_entry; F32P64: the float2 table itself).
+enum { TAB_GLOBAL = 0, TAB_SHARED = 1 };
+
+// numpy.linspace midpoint k (linspace_centre) with the step precomputed.
+__device__ __forceinline__ double bin_centre(const ParticleArgs& a, int k) {
+    const double e0 = __dadd_rn(__dmul_rn((double)k, a.bc_step), a.cut_left);
+    const double e1 = k + 1 >= a.S ? a.cut_right
+                                   : __dadd_rn(__dmul_rn((double)(k + 1), a.bc_step), a.cut_left);
+    return __dmul_rn(__dadd_rn(e0, e1), 0.5);
+}
+
+template <int PREC, int TAB>
+__device__ __forceinline__ typename TableEntry<PREC>::T table_at(const ParticleArgs& a,
+                                                                 const void* stab, int k) {
+    using TB = typename TableEntry<PREC>::T;
+    if constexpr (TAB == TAB_GLOBAL) {
+        return __ldg(reinterpret_cast<const TB*>(a.table) + k);
+    } else if constexpr (PREC == PREC_F32P64) {
+        return reinterpret_cast<const float2*>(stab)[k];
+    } else {
+        const double* V = reinterpret_cast<const double*>(stab);
+        return lik_entry(V[k], V[k + 1], bin_centre(a, k), a.charge, a.lik_inv_w, 0.0);
+    }
+}
+
 struct TurnConsts {
     double V[kMaxRfEngine], om[kMaxRfEngine], ph[kMaxRfEngine];
     float Vf[kMaxRfEngine];
@@ -114,11 +146,13 @@ __device__ __forceinline__ double reduce_2pi(double x) {
     return fma(-rint(x * inv2pi), twopi, x);
 }
 
-template <int PREC, int SOLVER, bool LIK, bool KICK, bool HIST, bool WARP_AGG>
+template <int PREC, int SOLVER, bool LIK, bool KICK, bool HIST, bool WARP_AGG,
+          int TAB = TAB_GLOBAL>
 __device__ __forceinline__ void track_one(double& t,
                                           typename Coord<PREC>::E& e,
                                           const TurnConsts& c,
-                                          const ParticleArgs& a, int* sh, int order) {
+                                          const ParticleArgs& a, int* sh, int order,
+                                          const void* stab = nullptr) {
     using E = typename Coord<PREC>::E;
     if (KICK) {
         if constexpr (PREC == PREC_Q32P64) {
@@ -127,23 +161,22 @@ __device__ __forceinline__ void track_one(double& t,
             if (LIK) {
                 const double f = floor((t - a.bc0) * a.lik_inv_w);
                 if (f >= 0.0 && f < (double)(a.S - 1)) {
-                    const double2 tb = __ldg(reinterpret_cast<const double2*>(a.table) + (int)f);
-                    inc = t * tb.x + tb.y;
+                    const double2 tb = table_at<PREC, TAB>(a, stab, (int)f);
+                    inc = __fma_rn(t, tb.x, tb.y);
                 }
             }
             double s = 0.0;
-            for (int j = 0; j < a.n_rf; ++j) s += c.V[j] * sin(c.om[j] * t + c.ph[j]);
+            for (int j = 0; j < a.n_rf; ++j) s += c.V[j] * rf_sin(c.om[j] * t + c.ph[j]);
             e = q32_add(e, inc + (a.charge * s + c.acc), a);
         } else {
             if (LIK) {
                 const double f = floor((t - a.bc0) * a.lik_inv_w);
                 if (f >= 0.0 && f < (double)(a.S - 1)) {
                     const int k = (int)f;
+                    const auto tb = table_at<PREC, TAB>(a, stab, k);
                     if (PREC == PREC_F64) {
-                        const double2 tb = __ldg(reinterpret_cast<const double2*>(a.table) + k);
-                        e += t * tb.x + tb.y;
+                        e = __dadd_rn(e, __fma_rn(t, tb.x, tb.y));
                     } else {
-                        const float2 tb = __ldg(reinterpret_cast<const float2*>(a.table) + k);
                         const float x = (float)(t - (a.bc0 + (double)k * a.bw));
                         e += __fmaf_rn(tb.y, x, tb.x);
                     }
@@ -151,7 +184,7 @@ __device__ __forceinline__ void track_one(double& t,
             }
             if (PREC == PREC_F64) {
                 double s = 0.0;
-                for (int j = 0; j < a.n_rf; ++j) s += c.V[j] * sin(c.om[j] * t + c.ph[j]);
+                for (int j = 0; j < a.n_rf; ++j) s += c.V[j] * rf_sin(c.om[j] * t + c.ph[j]);
                 e += a.charge * s + c.acc;
             } else {
                 float s = 0.0f;
@@ -177,12 +210,12 @@ __device__ __forceinline__ void track_one(double& t,
 // the longest-latency loads of the pass) issued before the RF sines so their
 // latency overlaps the sine arithmetic.  Same operations, in the same order
 // per particle, as two calls of track_one.
-template <int PREC, int SOLVER, bool LIK>
+template <int PREC, int SOLVER, bool LIK, int TAB = TAB_GLOBAL>
 __device__ __forceinline__ void track_pair(double& t0, double& t1,
                                            typename Coord<PREC>::E& e0,
                                            typename Coord<PREC>::E& e1,
                                            const TurnConsts& c, const ParticleArgs& a,
-                                           int order) {
+                                           int order, const void* stab = nullptr) {
     using E = typename Coord<PREC>::E;
     using TB = typename TableEntry<PREC>::T;
     bool in0 = false, in1 = false;
@@ -194,8 +227,8 @@ __device__ __forceinline__ void track_pair(double& t0, double& t1,
         in0 = f0 >= 0.0 && f0 < (double)(a.S - 1);
         in1 = f1 >= 0.0 && f1 < (double)(a.S - 1);
         const int k0 = in0 ? (int)f0 : 0, k1 = in1 ? (int)f1 : 0;
-        tb0 = __ldg(reinterpret_cast<const TB*>(a.table) + k0);
-        tb1 = __ldg(reinterpret_cast<const TB*>(a.table) + k1);
+        tb0 = table_at<PREC, TAB>(a, stab, k0);
+        tb1 = table_at<PREC, TAB>(a, stab, k1);
         if (PREC == PREC_F32P64) {
             // offsets from the slice centre, needed before t changes
             x0f = (float)(t0 - (a.bc0 + (double)k0 * a.bw));
@@ -206,11 +239,11 @@ __device__ __forceinline__ void track_pair(double& t0, double& t1,
         // the turn's whole energy change in float64, rounded once per particle
         double x0 = 0.0, x1 = 0.0;
         for (int j = 0; j < a.n_rf; ++j) {
-            x0 += c.V[j] * sin(c.om[j] * t0 + c.ph[j]);
-            x1 += c.V[j] * sin(c.om[j] * t1 + c.ph[j]);
+            x0 += c.V[j] * rf_sin(c.om[j] * t0 + c.ph[j]);
+            x1 += c.V[j] * rf_sin(c.om[j] * t1 + c.ph[j]);
         }
-        const double i0 = (LIK && in0) ? t0 * tb0.x + tb0.y : 0.0;
-        const double i1 = (LIK && in1) ? t1 * tb1.x + tb1.y : 0.0;
+        const double i0 = (LIK && in0) ? __fma_rn(t0, tb0.x, tb0.y) : 0.0;
+        const double i1 = (LIK && in1) ? __fma_rn(t1, tb1.x, tb1.y) : 0.0;
         e0 = q32_add(e0, i0 + (a.charge * x0 + c.acc), a);
         e1 = q32_add(e1, i1 + (a.charge * x1 + c.acc), a);
     } else {
@@ -218,8 +251,8 @@ __device__ __forceinline__ void track_pair(double& t0, double& t1,
         if (PREC == PREC_F64) {
             double x0 = 0.0, x1 = 0.0;
             for (int j = 0; j < a.n_rf; ++j) {
-                x0 += c.V[j] * sin(c.om[j] * t0 + c.ph[j]);
-                x1 += c.V[j] * sin(c.om[j] * t1 + c.ph[j]);
+                x0 += c.V[j] * rf_sin(c.om[j] * t0 + c.ph[j]);
+                x1 += c.V[j] * rf_sin(c.om[j] * t1 + c.ph[j]);
             }
             s0 = (E)x0;
             s1 = (E)x1;
@@ -234,8 +267,8 @@ __device__ __forceinline__ void track_pair(double& t0, double& t1,
         }
         if (LIK) {
             if (PREC == PREC_F64) {
-                if (in0) e0 += t0 * tb0.x + tb0.y;
-                if (in1) e1 += t1 * tb1.x + tb1.y;
+                if (in0) e0 = __dadd_rn(e0, __fma_rn(t0, tb0.x, tb0.y));
+                if (in1) e1 = __dadd_rn(e1, __fma_rn(t1, tb1.x, tb1.y));
             } else {
                 if (in0) e0 += __fmaf_rn(tb0.y, x0f, tb0.x);
                 if (in1) e1 += __fmaf_rn(tb1.y, x1f, tb1.x);
@@ -584,6 +617,154 @@ particle_kernel(const ParticleArgs a) {
         if (b >= 0 && !a.no_deposit) atomicAdd(&hd[b], 1);
     }
     if (!a.global_hist) cluster_flush(sh, a.hist, a.S);
+}
+
+// ------------------------------------------------- shared-table plain pass
+// The plain pass with the induced kick's table in shared memory.  F64 and
+// Q32P64 keep only the induced voltage (8 B per slice: 128 KB at 2^14
+// slices, where the {slope, offset} table is 256 KB); each particle forms
+// its entry with lik_entry from V_k, V_{k+1} and the bin centre, which gives
+// the head's table entry bit for bit.  F32P64 keeps the float2 table.  A
+// gather then costs a shared-memory access instead of an L2 round trip --
+// the global-table pass's top stall (long scoreboard on the table loads,
+// L1 hit rate ~25 %).  One 1024-thread block per SM holds the table, the
+// packed 16-bit block histogram (deposit_packed, exact under wraps) and the
+// prefetch ring; the block copies the table after the head has completed.
+__device__ __forceinline__ void copy16_async(void* smem, const void* gmem) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                     (uint32_t)__cvta_generic_to_shared(smem)), "l"(gmem) : "memory");
+}
+
+// Bytes of the shared table (before padding to 16) for S slices.
+template <int PREC>
+__host__ __device__ constexpr size_t stab_table_bytes(int S) {
+    return PREC == PREC_F32P64 ? (size_t)(S - 1) * 8 : (size_t)S * 8;
+}
+__host__ __device__ constexpr size_t pad16(size_t x) { return (x + 15) & ~(size_t)15; }
+
+template <int PREC, int SOLVER, int NST>
+__global__ void __launch_bounds__(kEngineThreads, 1)
+particle_kernel_stab(const ParticleArgs a) {
+    using E = typename Coord<PREC>::E;
+    using E2 = typename Vec2<E>::type;
+    extern __shared__ __align__(16) unsigned char dsm[];
+    __shared__ TurnConsts c;
+    pdl_launch_dependents();
+    const int S = a.S;
+    const int half = (S + 1) / 2;
+    const size_t tbytes = stab_table_bytes<PREC>(S);
+    const size_t tpad = pad16(tbytes), hpad = pad16((size_t)half * 4);
+    const void* stab = dsm;
+    unsigned* sh = reinterpret_cast<unsigned*>(dsm + tpad);
+    for (int k = threadIdx.x; k < half; k += blockDim.x) sh[k] = 0u;
+    pdl_wait();  // the head's table / voltage, counter and cleared histogram
+    long long t_idx = a.turn ? (*a.turn - 1) : 0;
+    if (t_idx < 0) t_idx = 0;
+    if (t_idx >= a.n_turns) t_idx = a.n_turns - 1;
+    for (int j = threadIdx.x; j < a.n_rf; j += blockDim.x) {
+        c.V[j] = a.V[t_idx * a.n_rf + j];
+        c.Vf[j] = (float)c.V[j];
+        c.om[j] = a.om[t_idx * a.n_rf + j];
+        c.ph[j] = a.ph[t_idx * a.n_rf + j];
+    }
+    if (threadIdx.x == 0) {
+        c.acc = a.interp ? 0.0 : a.acc[t_idx];
+        c.d = a.drift[t_idx + 1];
+    }
+    // the table (L2-resident): 16-byte asynchronous copies, one group
+    {
+        const char* src = reinterpret_cast<const char*>(PREC == PREC_F32P64 ? a.table
+                                                                            : (const void*)a.vind);
+        const size_t n16 = tbytes / 16;
+        for (size_t q = threadIdx.x; q < n16; q += blockDim.x) copy16_async(dsm + 16 * q, src + 16 * q);
+        if (threadIdx.x == 0 && (tbytes & 15))
+            *reinterpret_cast<double*>(dsm + 16 * n16) =
+                *reinterpret_cast<const double*>(src + 16 * n16);
+        ring_commit();
+    }
+    double* dt = reinterpret_cast<double*>(a.dt);
+    E* dE = reinterpret_cast<E*>(a.dE);
+    const int64_t npairs = a.n / 2;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int order = a.order;
+    const int lane = threadIdx.x & 31;
+    int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31);
+    const uint64_t pol = evict_first_policy();
+    if (NST == 0) {
+        ring_wait<0>();
+        __syncthreads();  // every thread's part of the table has landed
+        for (; base < npairs; base += stride) {
+            const int64_t p = base + lane;
+            int b0 = -1, b1 = -1;
+            if (p < npairs) {
+                double2 tt = stream_load(reinterpret_cast<const double2*>(dt) + p, pol);
+                E2 ee = stream_load(reinterpret_cast<const E2*>(dE) + p, pol);
+                track_pair<PREC, SOLVER, true, TAB_SHARED>(tt.x, tt.y, ee.x, ee.y, c, a, order,
+                                                           stab);
+                stream_store(reinterpret_cast<double2*>(dt) + p, tt, pol);
+                stream_store(reinterpret_cast<E2*>(dE) + p, ee, pol);
+                b0 = engine_bin(tt.x, a.cut_left, a.inv_w, S);
+                b1 = engine_bin(tt.y, a.cut_left, a.inv_w, S);
+            }
+            deposit_packed(sh, half, a.hist, b0);
+            deposit_packed(sh, half, a.hist, b1);
+        }
+    } else {
+        double2* rdt = reinterpret_cast<double2*>(dsm + tpad + hpad);
+        E2* rdE = reinterpret_cast<E2*>(rdt + (size_t)NST * blockDim.x);
+        const double2* gdt = reinterpret_cast<const double2*>(dt);
+        const E2* gdE = reinterpret_cast<const E2*>(dE);
+        auto fill = [&](int slot, int64_t p) {
+            if (p < npairs) {
+                ring_copy16(&rdt[slot * blockDim.x + threadIdx.x], &gdt[p], pol);
+                if (sizeof(E2) == 16) ring_copy16(&rdE[slot * blockDim.x + threadIdx.x], &gdE[p], pol);
+                else ring_copy8(&rdE[slot * blockDim.x + threadIdx.x], &gdE[p], pol);
+            }
+            ring_commit();
+        };
+#pragma unroll
+        for (int s = 0; s < NST - 1; ++s) fill(s, base + s * stride + lane);
+        // groups complete in order: the table's (the oldest) has landed
+        ring_wait<NST - 1>();
+        __syncthreads();
+        int slot = 0;
+        for (; base < npairs; base += stride) {
+            fill(slot == 0 ? NST - 1 : slot - 1, base + (NST - 1) * stride + lane);
+            ring_wait<NST - 1>();
+            const int64_t p = base + lane;
+            int b0 = -1, b1 = -1;
+            if (p < npairs) {
+                double2 tt = rdt[slot * blockDim.x + threadIdx.x];
+                E2 ee = rdE[slot * blockDim.x + threadIdx.x];
+                track_pair<PREC, SOLVER, true, TAB_SHARED>(tt.x, tt.y, ee.x, ee.y, c, a, order,
+                                                           stab);
+                stream_store(reinterpret_cast<double2*>(dt) + p, tt, pol);
+                stream_store(reinterpret_cast<E2*>(dE) + p, ee, pol);
+                b0 = engine_bin(tt.x, a.cut_left, a.inv_w, S);
+                b1 = engine_bin(tt.y, a.cut_left, a.inv_w, S);
+            }
+            deposit_packed(sh, half, a.hist, b0);
+            deposit_packed(sh, half, a.hist, b1);
+            slot = slot + 1 == NST ? 0 : slot + 1;
+        }
+        ring_wait<0>();
+    }
+    // odd tail particle
+    if ((a.n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+        double t = dt[a.n - 1];
+        E e = dE[a.n - 1];
+        track_one<PREC, SOLVER, true, true, true, false, TAB_SHARED>(t, e, c, a, nullptr, order,
+                                                                      stab);
+        dt[a.n - 1] = t;
+        dE[a.n - 1] = e;
+        deposit_packed(sh, half, a.hist, engine_bin(t, a.cut_left, a.inv_w, S));
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < half; k += blockDim.x) {
+        const unsigned v = sh[k];
+        if (v & 0xffffu) atomicAdd(&a.hist[k], (int)(v & 0xffffu));
+        if ((v >> 16) && k + half < S) atomicAdd(&a.hist[k + half], (int)(v >> 16));
+    }
 }
 
 // ------------------------------------------------------ TMA-pipelined pass

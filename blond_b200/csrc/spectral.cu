@@ -8,8 +8,11 @@
 
 namespace bb {
 
+// Radix passes of a length-L transform: as few as possible (each pass is a
+// block barrier and a shared-memory round trip), radix 8 first.
 static void radix_schedule(int L, int* r, int& n) {
     n = 0;
+    while (L % 8 == 0) { r[n++] = 8; L /= 8; }
     while (L % 4 == 0) { r[n++] = 4; L /= 4; }
     while (L % 2 == 0) { r[n++] = 2; L /= 2; }
     while (L % 3 == 0) { r[n++] = 3; L /= 3; }

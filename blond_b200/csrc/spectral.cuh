@@ -91,16 +91,6 @@ struct SpecParams {
     int table_f32;            // 0: double2 {slope, offset}; 1: float2 {qV, slope}
     double charge, inv_w;     // inv_w = (S-1)/(bc[S-1]-bc[0])
     const double* bc;
-    // interpolated tracker (RingAndRFTracker(interpolation=True),
-    // trackers/tracker.py:586-601): the table interpolates the RF voltage at
-    // the bin centres (rf_volt_comp, kick.cpp:37-51) plus the induced
-    // voltage, with the turn's acceleration kick in the offsets; rf_V/om/ph
-    // are the turn-major [n_turns+1][rf_n] programmes, acc [n_turns]
-    const double* rf_V;       // nullptr: the table holds the induced voltage only
-    const double* rf_om;
-    const double* rf_ph;
-    int rf_n;
-    const double* rf_acc;
     long long* turn;          // device turn counter (read; incremented if bump)
     int bump_turn;
     // twiddle tables precomputed for this plan (make_spec_twiddles), or
@@ -180,8 +170,39 @@ __device__ __forceinline__ double2 crot_s(double2 a, double s) {
     return make_double2(-s * a.y, s * a.x);
 }
 
-// In-place R-point DFT (R = 2, 3, 4, 5) of v, sign s of the exponent.
+// 4-point DFT of (a, b, c, d) in place, sign s of the exponent.
+__device__ __forceinline__ void dft4(double2& a, double2& b, double2& c, double2& d, double s) {
+    const double2 s02 = cadd(a, c), d02 = csub(a, c);
+    const double2 s13 = cadd(b, d), d13 = crot_s(csub(b, d), s);
+    a = cadd(s02, s13);
+    c = csub(s02, s13);
+    b = cadd(d02, d13);
+    d = csub(d02, d13);
+}
+
+// In-place R-point DFT (R = 2, 3, 4, 5, 8) of v, sign s of the exponent;
+// 8 = 2 x 4 (decimation in time).  (A radix-16 butterfly needs enough
+// registers to make the kernel spill around the non-inlined pass.)
 __device__ __forceinline__ void small_dft(double2* v, int R, double s) {
+    if (R == 8) {
+        double2 e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+        double2 o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+        dft4(e0, e1, e2, e3, s);
+        dft4(o0, o1, o2, o3, s);
+        const double h = 0.70710678118654752440;
+        o1 = cmul(o1, make_double2(h, s * h));
+        o2 = crot_s(o2, s);
+        o3 = cmul(o3, make_double2(-h, s * h));
+        v[0] = cadd(e0, o0);
+        v[4] = csub(e0, o0);
+        v[1] = cadd(e1, o1);
+        v[5] = csub(e1, o1);
+        v[2] = cadd(e2, o2);
+        v[6] = csub(e2, o2);
+        v[3] = cadd(e3, o3);
+        v[7] = csub(e3, o3);
+        return;
+    }
     if (R == 2) {
         const double2 a = v[0], b = v[1];
         v[0] = cadd(a, b);
@@ -234,9 +255,9 @@ __device__ __noinline__ void stockham_pass(const double2* __restrict__ src,
         const int j = lgB >= 0 ? (idx >> lgB) : idx / B;
         const int k = lgNs >= 0 ? (j & (Ns - 1)) : j % Ns;
         const int jq = lgNs >= 0 ? (j >> lgNs) : j / Ns;
-        double2 v[5];
+        double2 v[8];
 #pragma unroll
-        for (int t = 0; t < 5; ++t) {
+        for (int t = 0; t < 8; ++t) {
             if (t < R) {
                 double2 x = src[(j + t * LR) * B + b];
                 if (t > 0 && k > 0) {
@@ -250,7 +271,7 @@ __device__ __noinline__ void stockham_pass(const double2* __restrict__ src,
         small_dft(v, R, s);
         const int d = jq * Ns * R + k;
 #pragma unroll
-        for (int t = 0; t < 5; ++t)
+        for (int t = 0; t < 8; ++t)
             if (t < R) dst[(d + t * Ns) * B + b] = v[t];
     }
 }
@@ -659,18 +680,6 @@ spectral_kernel(const SpecParams P, const typename SpecLoopArg<FB>::type LP) {
     if (!g_table && !P.bump_turn) return;
     if (g_table) {
         const int64_t nt = P.n_out - 1;
-        // interpolated tracker: total voltage = RF voltage at the bin centre
-        // + induced voltage (tracker.py:589-592), acc in the offsets
-        const bool rfi = P.rf_V != nullptr;
-        const double* Vt = rfi ? P.rf_V + turn * P.rf_n : nullptr;
-        const double* omt = rfi ? P.rf_om + turn * P.rf_n : nullptr;
-        const double* pht = rfi ? P.rf_ph + turn * P.rf_n : nullptr;
-        const double acc_t = rfi ? P.rf_acc[turn] : 0.0;
-        auto rfv = [&](double x) {
-            double s = 0.0;
-            for (int j = 0; j < P.rf_n; ++j) s += Vt[j] * sin(omt[j] * x + pht[j]);
-            return s;
-        };
         for (int e = tid; e < per; e += nth) {
             const int b = e % Bc, m1 = e / Bc;
             const int64_t m = (int64_t)c * Bc + b + (int64_t)M2 * m1;
@@ -681,21 +690,16 @@ spectral_kernel(const SpecParams P, const typename SpecLoopArg<FB>::type LP) {
             for (int h = 0; h < 2; ++h) {
                 const int64_t n = 2 * m + h;
                 if (n >= nt) continue;
-                double a0 = h == 0 ? v0 : v1;
-                double a1 = h == 0 ? v1 : (b + 1 < Bc ? vloc[e + 1] : nbr[m1]);
+                const double a0 = h == 0 ? v0 : v1;
+                const double a1 = h == 0 ? v1 : (b + 1 < Bc ? vloc[e + 1] : nbr[m1]);
                 const double bcn = p.prefetch ? bcs[2 * e + h] : g_bc[n];
-                if (rfi) {
-                    a0 = rfv(bcn) + a0;
-                    a1 = rfv(g_bc[n + 1]) + a1;
-                }
                 if (!P.table_f32) {
-                    // linear_interp_kick.cpp:44-47 (acc = 0 unless interpolated)
-                    const double slope = P.charge * (a1 - a0) * inv_w;
-                    const double offset = (P.charge * a0 - bcn * slope) + acc_t;
-                    reinterpret_cast<double2*>(g_table)[n] = make_double2(slope, offset);
+                    // linear_interp_kick.cpp:44-47 with acc = 0
+                    reinterpret_cast<double2*>(g_table)[n] =
+                        lik_entry(a0, a1, bcn, P.charge, inv_w, 0.0);
                 } else {
                     reinterpret_cast<float2*>(g_table)[n] =
-                        make_float2((float)(P.charge * a0 + acc_t),
+                        make_float2((float)(P.charge * a0),
                                     (float)(P.charge * (a1 - a0) * inv_w));
                 }
             }

@@ -193,15 +193,16 @@ class FusedTracker:
         self.eng.call("bind_beam", ct.c_void_p(self.dt.data_ptr()),
                       ct.c_void_p(self.dE.data_ptr()), int(beam.n_macroparticles))
         self.eng.call("tune", int(threads), int(blocks_per_sm), int(turns_per_graph))
-        if kernel not in ("auto", "tma", "plain"):
-            raise ValueError("kernel must be 'auto', 'tma' or 'plain'")
+        if kernel not in ("auto", "tma", "plain", "stab"):
+            raise ValueError("kernel must be 'auto', 'tma', 'plain' or 'stab' (the plain "
+                             "pass with the table in shared memory)")
         self.kernel_requested = kernel
         if kernel == "auto":
             # measured on the B200 (C2 workload): plain loads win for FP64
             # (87 vs 107 us), the bulk-copy pipeline ties or wins for F32P64
             kernel = "plain" if precision == "f64" else "tma"
         self.kernel = kernel
-        self.eng.call("set_kernel", 0 if kernel == "tma" else 1)
+        self.eng.call("set_kernel", {"tma": 0, "plain": 1, "stab": 2}[kernel])
         # the autotuner picks block size, grid (particles per thread),
         # histogram layout and staged vs plain pass on the first track() or
         # prepare(), unless the caller fixed any of them
@@ -355,7 +356,7 @@ class FusedTracker:
         self.eng.call("autotune", int(reps), _stream(), cfg, ct.byref(ms))
         names = {-1: "auto", 0: "smem-warp-aggregated", 1: "smem-int", 2: "smem-packed16",
                  3: "global"}
-        self.tuned = {"kernel": "tma" if cfg[0] == 0 else "plain", "threads": cfg[1],
+        self.tuned = {"kernel": {0: "tma", 1: "plain", 2: "stab"}[cfg[0]], "threads": cfg[1],
                       "blocks_per_sm": cfg[2], "histogram": names.get(cfg[3], cfg[3]),
                       "prefetch_stages": cfg[4], "cluster": cfg[5], "candidates": cfg[6],
                       "particle_pass_ms": ms.value}

@@ -395,7 +395,12 @@ int blond_engine_get_feedback(blond_engine* engine, double* state,
                               void* stream);
 /* Particle-pass implementation: 0 = bulk-copy (TMA) pipelined (default;
  * falls back to 1 when the profile is too long for its shared memory),
- * 1 = plain loads. */
+ * 1 = plain loads, 2 = plain loads with the interpolation table in shared
+ * memory (the induced voltage for F64 / Q32P64, entries formed per particle
+ * with the head's rounding) and a packed 16-bit histogram; 2 needs an FFT
+ * impedance, a non-interpolated kick, integer slicing, bin centres that are
+ * numpy.linspace midpoints of the cuts, and the shared memory for it
+ * (BLOND_ERR_UNSUPPORTED otherwise). */
 int blond_engine_set_kernel(blond_engine* engine, int variant);
 /* Device copies of the current state (n_slices doubles each). */
 int blond_engine_get_profile(blond_engine* engine, double* profile,
@@ -447,11 +452,12 @@ int blond_engine_set_prefetch(blond_engine* engine, int stages);
  * global flush per cluster. */
 int blond_engine_set_cluster(blond_engine* engine, int blocks);
 /* Autotuner: times every feasible particle-pass configuration (plain pass:
- * 256/512 threads x 1/2/4 blocks per SM x histogram layouts x prefetch
- * ring 0/2/4 x clusters of 1/2; staged pass: histogram layouts) on the
- * bound beam, `reps` (1..10) launches each after one warm-up, keeps the
- * fastest and restores the coordinates and the histogram.  config[7]
- * receives {variant (0 staged, 1 plain), threads, blocks per SM, histogram
+ * 256/512/1024 threads x 1/2/4 blocks per SM x histogram layouts x prefetch
+ * ring 0/2/4 x clusters of 1/2; staged pass: histogram layouts; shared-table
+ * pass: ring 0/2) on the bound beam, `reps` (1..10) launches each after one
+ * warm-up, keeps the fastest and restores the coordinates and the
+ * histogram.  config[7] receives {variant (0 staged, 1 plain, 2 shared
+ * table), threads, blocks per SM, histogram
  * layout, ring stages, cluster blocks, candidates timed}; best_ms the
  * particle-pass time of the winner.  Not inside stream capture; allocates
  * a snapshot of the coordinates for the duration of the call. */

@@ -102,3 +102,32 @@ def test_cluster_merged_histograms_match(cuda, precision, cluster, hist):
     f.track(nt)
     np.testing.assert_array_equal(f.dt.cpu().numpy(), ref[0])
     np.testing.assert_array_equal(f.profile_tensor().cpu().numpy(), ref[1])
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32p64", "q32p64"])
+@pytest.mark.parametrize("ring", [0, 2])
+def test_shared_table_pass_gives_the_global_table_bits(cuda, precision, ring):
+    """The plain pass with the table in shared memory (the induced voltage
+    only for F64 / Q32P64, entries formed per particle; the float2 table
+    for F32P64) and a packed histogram, at C2's 2^14 slices on 2e6
+    particles: the same bits as the plain pass over the global table."""
+    import bench
+    out = []
+    for kernel in ("plain", "stab"):
+        fused, beam, _ = bench.build_fused(2_000_000, 16384, 4, precision, kernel=kernel)
+        fused.eng.call("set_prefetch", ring if kernel == "stab" else 2)
+        fused.eng.call("tune", 1024, 1, 2)
+        fused.track(4)
+        fused.check()
+        out.append((fused.dt.cpu().numpy(), fused.dE.cpu().numpy(),
+                    fused.profile_tensor().cpu().numpy(),
+                    fused.induced_voltage_tensor().cpu().numpy()))
+    for a, b in zip(*out):
+        np.testing.assert_array_equal(a, b)
+
+
+def test_shared_table_pass_is_refused_where_it_does_not_apply(cuda):
+    from blond_b200 import BlondB200Error
+    g, beam, f = fused_for("track_rf.npz", precision="f64", kernel="stab")
+    with pytest.raises(BlondB200Error, match="shared-table"):
+        f.track(1)
