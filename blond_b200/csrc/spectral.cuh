@@ -37,7 +37,7 @@ namespace bb {
 
 namespace cg = cooperative_groups;
 
-constexpr int kSpecThreads = 512;
+constexpr int kSpecThreads = 256;  // 8 warps: one per transform in the FFT phases; 255 registers
 constexpr int kMaxPasses = 24;
 constexpr int kMaxCluster = 16;
 constexpr int64_t kMaxClusterFFT = 131072;  // real length N
@@ -276,10 +276,76 @@ __device__ __noinline__ void stockham_pass(const double2* __restrict__ src,
     }
 }
 
+// B transforms of length L = 32 P (P = 1, 2, 4, 8) held interleaved in a
+// (element (b, i) at a[i * B + b]), transformed in place with one warp per
+// transform: lane l holds elements l + 32 q (q < P) in registers; radix-2
+// decimation in frequency, the butterflies of span >= 32 inside a lane, the
+// spans 16 .. 1 across lanes with shuffles (no block barrier inside a
+// transform), the results written back in natural order (the output of
+// decimation in frequency sits at the bit-reversed index).  tw[q] =
+// exp(-2 pi i q / L); the inverse uses the conjugates.  The Stockham passes
+// keep only 2-4 warps of a block busy, each on a long dependent chain, and
+// need a block barrier per pass; here every transform is one warp's
+// register-resident work.  Ends with __syncthreads().
+template <int P>
+__device__ __forceinline__ void warp_fft(double2* a, int B, const double2* __restrict__ tw,
+                                      bool inverse, int lgL) {
+    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int L = 32 * P;
+    const double sg = inverse ? -1.0 : 1.0;  // sign of the twiddles' imaginary parts
+    for (int b = threadIdx.x >> 5; b < B; b += nw) {
+        double2 v[P];
+#pragma unroll
+        for (int q = 0; q < P; ++q) v[q] = a[(lane + 32 * q) * B + b];
+        // spans h = 32 hq >= 32: both elements in this lane
+#pragma unroll
+        for (int hq = P / 2; hq >= 1; hq >>= 1) {
+#pragma unroll
+            for (int q = 0; q < P; ++q) {
+                if (q & hq) continue;
+                const int i = lane + 32 * q;  // the pair's lower index
+                const int e = (i & (64 * hq - 1)) * (L / (64 * hq));
+                double2 w = tw[e];
+                w.y *= sg;
+                const double2 x = v[q], y = v[q + hq];
+                v[q] = cadd(x, y);
+                v[q + hq] = cmul(csub(x, y), w);
+            }
+        }
+        // spans h = 16 .. 1: the partner is lane l ^ h
+#pragma unroll
+        for (int h = 16; h >= 1; h >>= 1) {
+            const bool upper = (lane & h) != 0;
+            double2 w = upper ? tw[(lane & (h - 1)) * (L / (2 * h))] : make_double2(1.0, 0.0);
+            w.y *= sg;
+#pragma unroll
+            for (int q = 0; q < P; ++q) {
+                double2 p;
+                p.x = __shfl_xor_sync(0xffffffffu, v[q].x, h);
+                p.y = __shfl_xor_sync(0xffffffffu, v[q].y, h);
+                v[q] = upper ? cmul(csub(p, v[q]), w) : cadd(v[q], p);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < P; ++q) {
+            const int k = (int)(__brev((unsigned)(lane + 32 * q)) >> (32 - lgL));
+            a[k * B + b] = v[q];
+        }
+    }
+    __syncthreads();
+}
+
 // B transforms of length L, interleaved, starting in a[]; returns the buffer
 // (a or b) that holds the result.  Ends with __syncthreads().
 __device__ double2* batch_fft(double2* a, double2* b, int L, int B, const int* radices,
                               int npass, const double2* tw, bool inverse) {
+    switch (L) {
+        case 32: warp_fft<1>(a, B, tw, inverse, 5); return a;
+        case 64: warp_fft<2>(a, B, tw, inverse, 6); return a;
+        case 128: warp_fft<4>(a, B, tw, inverse, 7); return a;
+        case 256: warp_fft<8>(a, B, tw, inverse, 8); return a;
+        default: break;
+    }
     const double s = inverse ? 1.0 : -1.0;
     const int lgB = (B & (B - 1)) == 0 ? __ffs(B) - 1 : -1;
     int Ns = 1;
