@@ -405,9 +405,10 @@ def run_ours(args, world, rank, local):
                                    "int32 histogram all-reduce (NCCL) per turn")
                    if world > 1 else "1 GPU"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": _traffic(args.precision, n),
-                     "kernel": f"particle_kernel{'_tma' if fused.kernel == 'tma' else ''} "
-                               "(lik+kick+drift+deposit)",
+                     "frac": achieved / peak,
+                     "traffic": _traffic(args.precision, n, fused.kernel),
+                     "kernel": {"tma": "particle_kernel_tma", "stab": "particle_kernel_stab"}
+                               .get(fused.kernel, "particle_kernel") + " (lik+kick+drift+deposit)",
                      "kernel_ms": part_avg, "head_kernel_ms": head_avg,
                      "bytes_per_particle": BYTES_PER_PARTICLE[args.precision],
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst copy)"
@@ -488,10 +489,15 @@ def _peaks():
         return {}
 
 
-def _traffic(precision, n):
+def _traffic(precision, n, kernel="plain"):
     """DRAM bytes per launch of the particle kernel from the committed ncu
-    summary (scaled to n particles), or None."""
-    path = os.path.join(ROOT, "profiles", "particle_kernel_c2.txt")
+    summary of that kernel (scaled to n particles), or None."""
+    name = {"stab": "particle_kernel_stab_c2.txt", "plain": "particle_kernel_c2.txt"}.get(kernel)
+    if precision == "q32p64" and kernel == "plain":
+        name = "particle_kernel_q32_c2.txt"
+    if name is None:
+        return None
+    path = os.path.join(ROOT, "profiles", name)
     try:
         for line in open(path):
             if line.startswith(f"traffic_bytes_per_particle_{precision}:"):

@@ -90,6 +90,7 @@ struct blond_engine {
     int hist_mode = -1;  // -1 automatic, else HIST_AGG/I32/PACKED/GLOBAL
     int ring = 0;        // plain pass: prefetch ring stages (0 = direct loads)
     int cluster = 1;     // plain pass: blocks whose histograms merge on chip
+    bool l2_ahead = false;  // shared-table pass: L2 prefetch beyond the ring
     // programmatic dependent launch between the turn's head and particle
     // pass: each kernel lets the next one launch and set up early
     bool pdl = true;
@@ -419,6 +420,7 @@ static ParticleArgs particle_args(blond_engine* e) {
     }
     a.no_deposit = e->smooth ? 1 : 0;
     a.vind = e->d_vind;
+    a.l2_ahead = e->l2_ahead ? 1 : 0;
     a.cut_right = e->cut_right;
     a.bc_step = (e->cut_right - e->cut_left) / (double)e->S;
     return a;
@@ -1078,6 +1080,13 @@ int blond_engine_set_cluster(blond_engine* e, int blocks) {
     return BLOND_OK;
 }
 
+int blond_engine_set_l2_prefetch(blond_engine* e, int on) {
+    BB_CHECK_ARG(e, "engine_set_l2_prefetch: null engine");
+    e->l2_ahead = on != 0;
+    e->graph_dirty = true;
+    return BLOND_OK;
+}
+
 int blond_engine_set_prefetch(blond_engine* e, int stages) {
     BB_CHECK_ARG(e && (stages == 0 || stages == 2 || stages == 4),
                  "engine_set_prefetch: stages must be 0, 2 or 4");
@@ -1133,7 +1142,7 @@ int blond_engine_autotune(blond_engine* e, int reps, void* stream, int* config,
     BB_CUDA(cudaMemcpyAsync(sdE, e->dE, esz * n, cudaMemcpyDeviceToDevice, s));
     BB_CUDA(cudaMemcpyAsync(shist, e->d_hist, sizeof(int) * e->S, cudaMemcpyDeviceToDevice,
                             s));
-    struct Cand { int variant, threads, bps, hist, ring, cluster; };
+    struct Cand { int variant, threads, bps, hist, ring, cluster, l2 = 0; };
     std::vector<Cand> cands;
     std::vector<int> plain_modes;
     if (global_hist(e)) plain_modes = {HIST_GLOBAL};
@@ -1168,10 +1177,11 @@ int blond_engine_autotune(blond_engine* e, int reps, void* stream, int* config,
     // the shared-table pass (packed histogram), with and without the ring
     for (int ring : {0, 2}) {
         const int sm = f64 ? stab_smem<PREC_F64>(e, ring) : stab_smem<PREC_F32P64>(e, ring);
-        if (sm >= 0) cands.push_back({2, kEngineThreads, 1, HIST_PACKED, ring, 1});
+        if (sm >= 0) cands.push_back({2, kEngineThreads, 1, HIST_PACKED, ring, 1, 0});
+        if (sm >= 0 && ring) cands.push_back({2, kEngineThreads, 1, HIST_PACKED, ring, 1, 1});
     }
     const Cand old = {e->variant, e->threads, e->blocks_per_sm, e->hist_mode, e->ring,
-                      e->cluster};
+                      e->cluster, e->l2_ahead ? 1 : 0};
     cudaEvent_t a = nullptr, b = nullptr;
     cudaEventCreate(&a);
     cudaEventCreate(&b);
@@ -1182,6 +1192,7 @@ int blond_engine_autotune(blond_engine* e, int reps, void* stream, int* config,
         e->hist_mode = c.hist;
         e->ring = c.ring;
         e->cluster = c.cluster;
+        e->l2_ahead = c.l2 != 0;
         if (c.variant == 1) {
             e->threads = c.threads;
             e->blocks_per_sm = c.bps;
@@ -1233,6 +1244,7 @@ int blond_engine_autotune(blond_engine* e, int reps, void* stream, int* config,
     e->hist_mode = use.hist;
     e->ring = use.ring;
     e->cluster = use.cluster;
+    e->l2_ahead = use.l2 != 0;
     e->graph_dirty = true;
     config[0] = use.variant;
     config[1] = use.variant == 1 ? use.threads : (use.variant == 0 ? kTmaThreads : kEngineThreads);
@@ -1240,7 +1252,8 @@ int blond_engine_autotune(blond_engine* e, int reps, void* stream, int* config,
     config[3] = use.hist;
     config[4] = use.ring;
     config[5] = use.cluster;
-    config[6] = (int)cands.size();
+    config[6] = use.l2;
+    config[7] = (int)cands.size();
     *best_ms = best < 1e30 ? best : 0.0;
     return rc;
 }

@@ -68,6 +68,9 @@ struct ParticleArgs {
     // bin centres (bc_step = (cut_right - cut_left) / S)
     const double* vind;
     double cut_right, bc_step;
+    // shared-table pass: thread 0 also prefetches the block's slice one
+    // iteration beyond the ring into L2
+    int l2_ahead;
 };
 
 enum { PREC_F64 = 0, PREC_F32P64 = 1, PREC_Q32P64 = 2 };
@@ -730,6 +733,16 @@ particle_kernel_stab(const ParticleArgs a) {
         int slot = 0;
         for (; base < npairs; base += stride) {
             fill(slot == 0 ? NST - 1 : slot - 1, base + (NST - 1) * stride + lane);
+            if (a.l2_ahead && threadIdx.x == 0) {
+                const int64_t pb = base + (int64_t)NST * stride;
+                if (pb < npairs) {
+                    const int64_t cnt = min((int64_t)blockDim.x, npairs - pb);
+                    if (((uintptr_t)(gdt + pb) & 15) == 0)
+                        l2_prefetch(gdt + pb, (uint32_t)(cnt * 16), pol);
+                    if (((uintptr_t)(gdE + pb) & 15) == 0 && ((cnt * sizeof(E2)) & ~(int64_t)15))
+                        l2_prefetch(gdE + pb, (uint32_t)((cnt * sizeof(E2)) & ~(int64_t)15), pol);
+                }
+            }
             ring_wait<NST - 1>();
             const int64_t p = base + lane;
             int b0 = -1, b1 = -1;

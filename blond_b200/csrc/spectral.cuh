@@ -39,7 +39,12 @@ namespace cg = cooperative_groups;
 
 constexpr int kSpecThreads = 256;  // 8 warps: one per transform in the FFT phases; 255 registers
 constexpr int kMaxPasses = 24;
-constexpr int kMaxCluster = 16;
+// Largest cluster of the FFT (16: the non-portable maximum); a build may
+// define BB_MAX_CLUSTER to compare smaller clusters.
+#ifndef BB_MAX_CLUSTER
+#define BB_MAX_CLUSTER 16
+#endif
+constexpr int kMaxCluster = BB_MAX_CLUSTER;
 constexpr int64_t kMaxClusterFFT = 131072;  // real length N
 constexpr int64_t kMaxDirectDFT = 4096;
 

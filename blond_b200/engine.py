@@ -351,14 +351,15 @@ class FusedTracker:
         """Run the engine's autotuner now (blond_engine_autotune): times
         every feasible particle-pass configuration on this beam, keeps the
         fastest and leaves the beam untouched.  Returns the choice."""
-        cfg = (ct.c_int * 7)()
+        cfg = (ct.c_int * 8)()
         ms = ct.c_double()
         self.eng.call("autotune", int(reps), _stream(), cfg, ct.byref(ms))
         names = {-1: "auto", 0: "smem-warp-aggregated", 1: "smem-int", 2: "smem-packed16",
                  3: "global"}
         self.tuned = {"kernel": {0: "tma", 1: "plain", 2: "stab"}[cfg[0]], "threads": cfg[1],
                       "blocks_per_sm": cfg[2], "histogram": names.get(cfg[3], cfg[3]),
-                      "prefetch_stages": cfg[4], "cluster": cfg[5], "candidates": cfg[6],
+                      "prefetch_stages": cfg[4], "cluster": cfg[5],
+                      "l2_prefetch": bool(cfg[6]), "candidates": cfg[7],
                       "particle_pass_ms": ms.value}
         self.kernel = self.tuned["kernel"]
         return self.tuned

@@ -447,6 +447,10 @@ int blond_engine_set_histogram(blond_engine* engine, int mode);
 /* Plain pass: depth of the per-thread cp.async prefetch ring (0 = direct
  * loads, 2 or 4 stages). */
 int blond_engine_set_prefetch(blond_engine* engine, int stages);
+/* Shared-table pass: thread 0 of each block also prefetches the block's
+ * slice one iteration beyond the ring into L2 (cp.async.bulk.prefetch);
+ * on = 0/1. */
+int blond_engine_set_l2_prefetch(blond_engine* engine, int on);
 /* Plain pass: blocks (1, 2, 4, 8) of a thread-block cluster whose shared
  * histograms are summed through distributed shared memory before one
  * global flush per cluster. */
@@ -456,9 +460,10 @@ int blond_engine_set_cluster(blond_engine* engine, int blocks);
  * ring 0/2/4 x clusters of 1/2; staged pass: histogram layouts; shared-table
  * pass: ring 0/2) on the bound beam, `reps` (1..10) launches each after one
  * warm-up, keeps the fastest and restores the coordinates and the
- * histogram.  config[7] receives {variant (0 staged, 1 plain, 2 shared
+ * histogram.  config[8] receives {variant (0 staged, 1 plain, 2 shared
  * table), threads, blocks per SM, histogram
- * layout, ring stages, cluster blocks, candidates timed}; best_ms the
+ * layout, ring stages, cluster blocks, L2 prefetch (0/1), candidates
+ * timed}; best_ms the
  * particle-pass time of the winner.  Not inside stream capture; allocates
  * a snapshot of the coordinates for the duration of the call. */
 int blond_engine_autotune(blond_engine* engine, int reps, void* stream, int* config,

@@ -105,8 +105,8 @@ def test_cluster_merged_histograms_match(cuda, precision, cluster, hist):
 
 
 @pytest.mark.parametrize("precision", ["f64", "f32p64", "q32p64"])
-@pytest.mark.parametrize("ring", [0, 2])
-def test_shared_table_pass_gives_the_global_table_bits(cuda, precision, ring):
+@pytest.mark.parametrize("ring,l2", [(0, 0), (2, 0), (2, 1)])
+def test_shared_table_pass_gives_the_global_table_bits(cuda, precision, ring, l2):
     """The plain pass with the table in shared memory (the induced voltage
     only for F64 / Q32P64, entries formed per particle; the float2 table
     for F32P64) and a packed histogram, at C2's 2^14 slices on 2e6
@@ -116,6 +116,7 @@ def test_shared_table_pass_gives_the_global_table_bits(cuda, precision, ring):
     for kernel in ("plain", "stab"):
         fused, beam, _ = bench.build_fused(2_000_000, 16384, 4, precision, kernel=kernel)
         fused.eng.call("set_prefetch", ring if kernel == "stab" else 2)
+        fused.eng.call("set_l2_prefetch", l2 if kernel == "stab" else 0)
         fused.eng.call("tune", 1024, 1, 2)
         fused.track(4)
         fused.check()
