@@ -57,7 +57,7 @@ def parse():
                     help="leave the C3 batch out of the default line")
     ap.add_argument("--batched-error-turns", type=int, default=1000,
                     help="turns after which the batched forms' rms errors are taken")
-    ap.add_argument("--kernel", default="auto", choices=["auto", "tma", "plain", "stab"])
+    ap.add_argument("--kernel", default="auto", choices=["auto", "tma", "plain", "stab", "packed"])
     ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5", "mtw"],
                     help="c2: the single-beam pipeline (default, the headline); "
                          "c3: 256-beam double-RF batch; c4: adjoint gradient; "
@@ -407,7 +407,8 @@ def run_ours(args, world, rank, local):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak,
                      "traffic": _traffic(args.precision, n, fused.kernel),
-                     "kernel": {"tma": "particle_kernel_tma", "stab": "particle_kernel_stab"}
+                     "kernel": {"tma": "particle_kernel_tma", "stab": "particle_kernel_stab",
+                                "packed": "particle_kernel_stab<TAB_GLOBAL>"}
                                .get(fused.kernel, "particle_kernel") + " (lik+kick+drift+deposit)",
                      "kernel_ms": part_avg, "head_kernel_ms": head_avg,
                      "bytes_per_particle": BYTES_PER_PARTICLE[args.precision],
@@ -822,54 +823,66 @@ def build_c5(n, n_turns, precision, seed=0):
 
 
 def run_c5(args):
-    """F32P64 (the C5 precision) and FP64 on the same bunch; the F32P64
-    error is the in-window rms of dt and dE after the timed turns."""
+    """Q32P64 (the chosen form), F32P64 and FP64 on the same bunch, and an
+    FP64 control from energies moved by 0.01 eV; each form's error is the
+    in-window rms of dt and dE after the timed turns, against FP64."""
     import torch
     W, K = max(3, args.warmup), args.steps
     kt = min(K, 20)
     n = int(args.particles) if args.particles != 1e7 else int(1e8)
     res, coords = {}, {}
     peak = _peaks().get("hbm_gbs") or 6650.0
-    for prec in ("f32p64", "f64"):
+    for prec, shift in (("q32p64", 0.0), ("f32p64", 0.0), ("f64", 0.0), ("f64", 0.01)):
+        key = prec if not shift else "control_fp64_dE_plus_0.01eV"
         fused, beam, prof, n_fft = build_c5(n, W + K + kt + 4, prec)
+        if shift:
+            fused.dE.add_(shift)
+            fused.eng.call("slice", ct_stream())
         fused.track(W)
         fused.prepare()
         torch.cuda.synchronize()
-        clocks = ClockSampler(0) if prec == "f32p64" else None
+        clocks = ClockSampler(0) if prec == "q32p64" else None
         ms = time_turns(fused, K)
         clk = clocks.stop() if clocks else None
         fused.check()
         w = (fused.dt > prof.cut_left) & (fused.dt < prof.cut_right)
-        coords[prec] = (fused.dt[w].std().item(), fused.dE.double()[w].std().item())
-        head_ms, part_ms = fused.time_kernels(kt)
-        ach = BYTES_PER_PARTICLE[prec] * n / (part_ms / kt * 1e-3) / 1e9
-        res[prec] = {"value": n * K / (ms * 1e-3), "ms_per_step": ms / K,
-                     "kernel_ms": part_ms / kt, "head_kernel_ms": head_ms / kt,
-                     "achieved_gbs": ach, "frac": ach / peak, "clocks": clk,
-                     "kernel": fused.kernel, "autotuned": fused.tuned}
+        coords[key] = (fused.dt[w].std().item(), fused.energies()[w].std().item())
+        if not shift:
+            head_ms, part_ms = fused.time_kernels(kt)
+            ach = BYTES_PER_PARTICLE[prec] * n / (part_ms / kt * 1e-3) / 1e9
+            res[prec] = {"value": n * K / (ms * 1e-3), "ms_per_step": ms / K,
+                         "kernel_ms": part_ms / kt, "head_kernel_ms": head_ms / kt,
+                         "achieved_gbs": ach, "frac": ach / peak, "clocks": clk,
+                         "kernel": fused.kernel, "autotuned": fused.tuned}
         del fused, beam, prof
         torch.cuda.empty_cache()
-    r = res["f32p64"]
+
+    def err(key):
+        return {"sigma_dt": abs(coords[key][0] / coords["f64"][0] - 1),
+                "sigma_dE": abs(coords[key][1] / coords["f64"][1] - 1)}
+    r = res["q32p64"]
     return {
         "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": 1,
         "steps": K, "warmup": W, "ms_per_step": r["ms_per_step"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32p64", "data": "synthetic",
+        "dtype": "q32p64", "data": "synthetic",
         "config": {"workload": C5_WORKLOAD, "particles": n, "slices": 65536,
                    "n_fft": n_fft, "l2": "inputs larger than L2"},
         "roofline": {"bound": "hbm", "achieved": r["achieved_gbs"], "peak": peak,
                      "unit": "GB/s", "frac": r["frac"], "traffic": None,
-                     "kernel": f"particle_kernel{'_tma' if r['kernel'] == 'tma' else ''} "
-                               "(global-memory histogram)",
+                     "kernel": {"tma": "particle_kernel_tma", "stab": "particle_kernel_stab",
+                                "packed": "particle_kernel_stab<TAB_GLOBAL>"}
+                               .get(r["kernel"], "particle_kernel"),
                      "kernel_ms": r["kernel_ms"], "head_kernel_ms": r["head_kernel_ms"],
-                     "bytes_per_particle": BYTES_PER_PARTICLE["f32p64"],
+                     "bytes_per_particle": BYTES_PER_PARTICLE["q32p64"],
                      "autotuned": r["autotuned"]},
-        "f64": {k: res["f64"][k] for k in ("value", "ms_per_step", "kernel_ms",
-                                            "head_kernel_ms", "achieved_gbs", "frac")},
-        "f32p64_rel_err_after_turns": {
-            "turns": W + K, "statistic": "in-window rms of dt and dE, F32P64 vs FP64",
-            "sigma_dt": abs(coords["f32p64"][0] / coords["f64"][0] - 1),
-            "sigma_dE": abs(coords["f32p64"][1] / coords["f64"][1] - 1)},
+        **{p: {k: res[p][k] for k in ("value", "ms_per_step", "kernel_ms", "head_kernel_ms",
+                                      "achieved_gbs", "frac", "kernel")}
+           for p in ("f32p64", "f64")},
+        "rel_err_after_turns": {
+            "turns": W + K, "statistic": "in-window rms of dt and dE vs FP64",
+            "q32p64": err("q32p64"), "f32p64": err("f32p64"),
+            "control_fp64_dE_plus_0.01eV": err("control_fp64_dE_plus_0.01eV")},
         "gpu_launches": 2 * K,
         "clocks": r["clocks"],
     }

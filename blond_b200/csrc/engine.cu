@@ -86,7 +86,8 @@ struct blond_engine {
     int blocks_per_sm = 2;
     int turns_per_graph = 50;
     int variant = 0;  // 0: TMA-pipelined particle pass, 1: plain loads,
-                      // 2: plain loads with the table in shared memory
+                      // 2: plain loads with the table in shared memory,
+                      // 3: plain loads, packed histogram, global table
     int hist_mode = -1;  // -1 automatic, else HIST_AGG/I32/PACKED/GLOBAL
     int ring = 0;        // plain pass: prefetch ring stages (0 = direct loads)
     int cluster = 1;     // plain pass: blocks whose histograms merge on chip
@@ -264,15 +265,38 @@ static int stab_smem(const blond_engine* e, int ring) {
     return bytes <= limit ? (int)bytes : -1;
 }
 
+// Dynamic shared memory of the packed plain pass over the global table
+// (variant 3: packed histogram + ring), or -1 when it does not fit or the
+// turn deposits no integer counts.
+template <int PREC>
+static int packed_smem(const blond_engine* e, int ring) {
+    if (e->smooth) return -1;
+    const size_t bytes = pad16((size_t)((e->S + 1) / 2) * 4) +
+                         (size_t)ring * kEngineThreads * ring_bytes<PREC>();
+    const size_t limit = (size_t)device_info().max_smem_optin - sizeof(TurnConsts) - 1024;
+    return bytes <= limit ? (int)bytes : -1;
+}
+
+template <int PREC, int SOLVER, int TAB, int NST>
+static auto packed_kernel() {
+    return particle_kernel_stab<PREC, SOLVER, NST, TAB>;
+}
+
 template <int PREC, int SOLVER>
 static int launch_stab(blond_engine* e, const ParticleArgs& a, cudaStream_t s, bool launch) {
-    const int ring = e->ring ? 2 : 0;
-    const int smem = stab_smem<PREC>(e, ring);
+    const bool shared = e->variant == 2;
+    const int ring = shared ? (e->ring ? 2 : 0) : (e->ring >= 4 ? 4 : (e->ring ? 2 : 0));
+    const int smem = shared ? stab_smem<PREC>(e, ring) : packed_smem<PREC>(e, ring);
     if (smem < 0) {
-        set_error("engine: the shared-table pass does not apply to this engine");
+        set_error(shared ? "engine: the shared-table pass does not apply to this engine"
+                         : "engine: the packed-histogram pass does not fit this engine");
         return BLOND_ERR_UNSUPPORTED;
     }
-    auto k = ring ? particle_kernel_stab<PREC, SOLVER, 2> : particle_kernel_stab<PREC, SOLVER, 0>;
+    auto k = shared ? (ring ? packed_kernel<PREC, SOLVER, TAB_SHARED, 2>()
+                            : packed_kernel<PREC, SOLVER, TAB_SHARED, 0>())
+                    : (ring == 4 ? packed_kernel<PREC, SOLVER, TAB_GLOBAL, 4>()
+                       : ring ? packed_kernel<PREC, SOLVER, TAB_GLOBAL, 2>()
+                              : packed_kernel<PREC, SOLVER, TAB_GLOBAL, 0>());
     int rc;
     if ((rc = allow_smem_once(k))) return rc;
     if (launch) {
@@ -300,12 +324,15 @@ template <int PREC, int SOLVER, bool LIK, bool KICK>
 static int launch_particles_t(blond_engine* e, const ParticleArgs& a, cudaStream_t s,
                               bool launch) {
     if constexpr (KICK) {
-        if (e->variant == 2) {
+        if (e->variant == 2 || e->variant == 3) {
             if constexpr (LIK) {
                 return launch_stab<PREC, SOLVER>(e, a, s, launch);
             } else {
-                set_error("engine: the shared-table pass does not apply to this engine "
-                          "(no interpolated kick)");
+                set_error(e->variant == 2
+                              ? "engine: the shared-table pass does not apply to this engine "
+                                "(no interpolated kick)"
+                              : "engine: the packed-histogram pass does not apply to this "
+                                "engine (no interpolated kick)");
                 return BLOND_ERR_UNSUPPORTED;
             }
         }
@@ -1032,8 +1059,9 @@ int blond_engine_step(blond_engine* e, int part, void* stream) {
 }
 
 int blond_engine_set_kernel(blond_engine* e, int variant) {
-    BB_CHECK_ARG(e && variant >= 0 && variant <= 2,
-                 "engine_set_kernel: variant 0 (staged), 1 (plain) or 2 (shared table)");
+    BB_CHECK_ARG(e && variant >= 0 && variant <= 3,
+                 "engine_set_kernel: variant 0 (staged), 1 (plain), 2 (shared table) or 3 "
+                 "(plain with a packed histogram)");
     e->variant = variant;
     e->graph_dirty = true;
     return BLOND_OK;
@@ -1180,6 +1208,12 @@ int blond_engine_autotune(blond_engine* e, int reps, void* stream, int* config,
         if (sm >= 0) cands.push_back({2, kEngineThreads, 1, HIST_PACKED, ring, 1, 0});
         if (sm >= 0 && ring) cands.push_back({2, kEngineThreads, 1, HIST_PACKED, ring, 1, 1});
     }
+    // the plain pass with a packed histogram over the global table (long profiles)
+    if (e->has_fft || e->has_ind || e->interp)
+        for (int ring : {0, 2, 4}) {
+            const int sm = f64 ? packed_smem<PREC_F64>(e, ring) : packed_smem<PREC_F32P64>(e, ring);
+            if (sm >= 0) cands.push_back({3, kEngineThreads, 1, HIST_PACKED, ring, 1, 0});
+        }
     const Cand old = {e->variant, e->threads, e->blocks_per_sm, e->hist_mode, e->ring,
                       e->cluster, e->l2_ahead ? 1 : 0};
     cudaEvent_t a = nullptr, b = nullptr;
@@ -1248,6 +1282,7 @@ int blond_engine_autotune(blond_engine* e, int reps, void* stream, int* config,
     e->graph_dirty = true;
     config[0] = use.variant;
     config[1] = use.variant == 1 ? use.threads : (use.variant == 0 ? kTmaThreads : kEngineThreads);
+    // (variants 2 and 3 run 1024 threads x one block per SM)
     config[2] = use.variant == 1 ? use.bps : 1;
     config[3] = use.hist;
     config[4] = use.ring;

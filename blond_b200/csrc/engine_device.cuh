@@ -645,7 +645,10 @@ __host__ __device__ constexpr size_t stab_table_bytes(int S) {
 }
 __host__ __device__ constexpr size_t pad16(size_t x) { return (x + 15) & ~(size_t)15; }
 
-template <int PREC, int SOLVER, int NST>
+// TAB = TAB_GLOBAL gives the same pass over the global table (no copy):
+// the plain pass with a packed histogram, which fits 2^16-slice profiles
+// beside the ring.
+template <int PREC, int SOLVER, int NST, int TAB = TAB_SHARED>
 __global__ void __launch_bounds__(kEngineThreads, 1)
 particle_kernel_stab(const ParticleArgs a) {
     using E = typename Coord<PREC>::E;
@@ -655,7 +658,7 @@ particle_kernel_stab(const ParticleArgs a) {
     pdl_launch_dependents();
     const int S = a.S;
     const int half = (S + 1) / 2;
-    const size_t tbytes = stab_table_bytes<PREC>(S);
+    const size_t tbytes = TAB == TAB_SHARED ? stab_table_bytes<PREC>(S) : 0;
     const size_t tpad = pad16(tbytes), hpad = pad16((size_t)half * 4);
     const void* stab = dsm;
     unsigned* sh = reinterpret_cast<unsigned*>(dsm + tpad);
@@ -675,7 +678,8 @@ particle_kernel_stab(const ParticleArgs a) {
         c.d = a.drift[t_idx + 1];
     }
     // the table (L2-resident): 16-byte asynchronous copies, one group
-    {
+    // (empty for the global-table form)
+    if (TAB == TAB_SHARED) {
         const char* src = reinterpret_cast<const char*>(PREC == PREC_F32P64 ? a.table
                                                                             : (const void*)a.vind);
         const size_t n16 = tbytes / 16;
@@ -683,6 +687,8 @@ particle_kernel_stab(const ParticleArgs a) {
         if (threadIdx.x == 0 && (tbytes & 15))
             *reinterpret_cast<double*>(dsm + 16 * n16) =
                 *reinterpret_cast<const double*>(src + 16 * n16);
+        ring_commit();
+    } else {
         ring_commit();
     }
     double* dt = reinterpret_cast<double*>(a.dt);
@@ -702,8 +708,7 @@ particle_kernel_stab(const ParticleArgs a) {
             if (p < npairs) {
                 double2 tt = stream_load(reinterpret_cast<const double2*>(dt) + p, pol);
                 E2 ee = stream_load(reinterpret_cast<const E2*>(dE) + p, pol);
-                track_pair<PREC, SOLVER, true, TAB_SHARED>(tt.x, tt.y, ee.x, ee.y, c, a, order,
-                                                           stab);
+                track_pair<PREC, SOLVER, true, TAB>(tt.x, tt.y, ee.x, ee.y, c, a, order, stab);
                 stream_store(reinterpret_cast<double2*>(dt) + p, tt, pol);
                 stream_store(reinterpret_cast<E2*>(dE) + p, ee, pol);
                 b0 = engine_bin(tt.x, a.cut_left, a.inv_w, S);
@@ -749,8 +754,7 @@ particle_kernel_stab(const ParticleArgs a) {
             if (p < npairs) {
                 double2 tt = rdt[slot * blockDim.x + threadIdx.x];
                 E2 ee = rdE[slot * blockDim.x + threadIdx.x];
-                track_pair<PREC, SOLVER, true, TAB_SHARED>(tt.x, tt.y, ee.x, ee.y, c, a, order,
-                                                           stab);
+                track_pair<PREC, SOLVER, true, TAB>(tt.x, tt.y, ee.x, ee.y, c, a, order, stab);
                 stream_store(reinterpret_cast<double2*>(dt) + p, tt, pol);
                 stream_store(reinterpret_cast<E2*>(dE) + p, ee, pol);
                 b0 = engine_bin(tt.x, a.cut_left, a.inv_w, S);
@@ -766,8 +770,7 @@ particle_kernel_stab(const ParticleArgs a) {
     if ((a.n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
         double t = dt[a.n - 1];
         E e = dE[a.n - 1];
-        track_one<PREC, SOLVER, true, true, true, false, TAB_SHARED>(t, e, c, a, nullptr, order,
-                                                                      stab);
+        track_one<PREC, SOLVER, true, true, true, false, TAB>(t, e, c, a, nullptr, order, stab);
         dt[a.n - 1] = t;
         dE[a.n - 1] = e;
         deposit_packed(sh, half, a.hist, engine_bin(t, a.cut_left, a.inv_w, S));

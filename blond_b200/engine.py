@@ -193,16 +193,17 @@ class FusedTracker:
         self.eng.call("bind_beam", ct.c_void_p(self.dt.data_ptr()),
                       ct.c_void_p(self.dE.data_ptr()), int(beam.n_macroparticles))
         self.eng.call("tune", int(threads), int(blocks_per_sm), int(turns_per_graph))
-        if kernel not in ("auto", "tma", "plain", "stab"):
-            raise ValueError("kernel must be 'auto', 'tma', 'plain' or 'stab' (the plain "
-                             "pass with the table in shared memory)")
+        if kernel not in ("auto", "tma", "plain", "stab", "packed"):
+            raise ValueError("kernel must be 'auto', 'tma', 'plain', 'stab' (the plain "
+                             "pass with the table in shared memory) or 'packed' (the plain "
+                             "pass with a packed 16-bit histogram)")
         self.kernel_requested = kernel
         if kernel == "auto":
             # measured on the B200 (C2 workload): plain loads win for FP64
             # (87 vs 107 us), the bulk-copy pipeline ties or wins for F32P64
             kernel = "plain" if precision == "f64" else "tma"
         self.kernel = kernel
-        self.eng.call("set_kernel", {"tma": 0, "plain": 1, "stab": 2}[kernel])
+        self.eng.call("set_kernel", {"tma": 0, "plain": 1, "stab": 2, "packed": 3}[kernel])
         # the autotuner picks block size, grid (particles per thread),
         # histogram layout and staged vs plain pass on the first track() or
         # prepare(), unless the caller fixed any of them
@@ -356,7 +357,8 @@ class FusedTracker:
         self.eng.call("autotune", int(reps), _stream(), cfg, ct.byref(ms))
         names = {-1: "auto", 0: "smem-warp-aggregated", 1: "smem-int", 2: "smem-packed16",
                  3: "global"}
-        self.tuned = {"kernel": {0: "tma", 1: "plain", 2: "stab"}[cfg[0]], "threads": cfg[1],
+        self.tuned = {"kernel": {0: "tma", 1: "plain", 2: "stab", 3: "packed"}[cfg[0]],
+                      "threads": cfg[1],
                       "blocks_per_sm": cfg[2], "histogram": names.get(cfg[3], cfg[3]),
                       "prefetch_stages": cfg[4], "cluster": cfg[5],
                       "l2_prefetch": bool(cfg[6]), "candidates": cfg[7],

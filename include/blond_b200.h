@@ -395,7 +395,9 @@ int blond_engine_get_feedback(blond_engine* engine, double* state,
                               void* stream);
 /* Particle-pass implementation: 0 = bulk-copy (TMA) pipelined (default;
  * falls back to 1 when the profile is too long for its shared memory),
- * 1 = plain loads, 2 = plain loads with the interpolation table in shared
+ * 1 = plain loads, 3 = plain loads with a packed 16-bit block histogram
+ * (up to 2^17 slices beside the prefetch ring; needs an interpolated kick),
+ * 2 = plain loads with the interpolation table in shared
  * memory (the induced voltage for F64 / Q32P64, entries formed per particle
  * with the head's rounding) and a packed 16-bit histogram; 2 needs an FFT
  * impedance, a non-interpolated kick, integer slicing, bin centres that are

@@ -127,8 +127,32 @@ def test_shared_table_pass_gives_the_global_table_bits(cuda, precision, ring, l2
         np.testing.assert_array_equal(a, b)
 
 
+@pytest.mark.parametrize("precision", ["f64", "f32p64", "q32p64"])
+@pytest.mark.parametrize("slices,ring", [(16384, 0), (16384, 4), (65536, 0), (65536, 2)])
+def test_packed_histogram_pass_gives_the_plain_pass_bits(cuda, precision, slices, ring):
+    """The plain pass with a packed 16-bit block histogram over the global
+    table (the form that fits 2^16-slice profiles beside its ring), on 2e6
+    particles: the same bits as the plain pass with its int32 histogram."""
+    import bench
+    out = []
+    for kernel in ("plain", "packed"):
+        fused, beam, _ = bench.build_fused(2_000_000, slices, 4, precision, kernel=kernel)
+        fused.eng.call("set_prefetch", ring if kernel == "packed" else 0)
+        fused.eng.call("tune", 1024, 1, 2)
+        fused.track(4)
+        fused.check()
+        out.append((fused.dt.cpu().numpy(), fused.dE.cpu().numpy(),
+                    fused.profile_tensor().cpu().numpy(),
+                    fused.induced_voltage_tensor().cpu().numpy()))
+    for a, b in zip(*out):
+        np.testing.assert_array_equal(a, b)
+
+
 def test_shared_table_pass_is_refused_where_it_does_not_apply(cuda):
     from blond_b200 import BlondB200Error
     g, beam, f = fused_for("track_rf.npz", precision="f64", kernel="stab")
     with pytest.raises(BlondB200Error, match="shared-table"):
+        f.track(1)
+    g, beam, f = fused_for("track_rf.npz", precision="f64", kernel="packed")
+    with pytest.raises(BlondB200Error, match="packed-histogram"):
         f.track(1)

@@ -404,7 +404,7 @@ def test_track_host_matches_device_tracking(cuda, precision, chunks):
 
 
 @pytest.mark.parametrize("turns_per_graph", [1, 4])
-@pytest.mark.parametrize("kernel", ["plain", "tma"])
+@pytest.mark.parametrize("kernel", ["plain", "tma", "packed"])
 def test_fused_interpolated_tracker_matches_reference(cuda, turns_per_graph, kernel):
     """RingAndRFTracker(interpolation=True) through the fused engine: the
     head interpolates RF voltage at the bin centres + induced voltage, the
@@ -429,8 +429,9 @@ def test_fused_interpolated_tracker_matches_reference(cuda, turns_per_graph, ker
     np.testing.assert_array_equal(fused.profile_tensor().cpu().numpy(), g["profiles"][-1])
 
 
-@pytest.mark.parametrize("precision", ["f64", "q32p64"])
-def test_fused_interpolated_tracker_without_impedance(cuda, precision):
+@pytest.mark.parametrize("precision,kernel", [("f64", "auto"), ("q32p64", "auto"),
+                                              ("f64", "packed"), ("q32p64", "packed")])
+def test_fused_interpolated_tracker_without_impedance(cuda, precision, kernel):
     """Interpolated RF kick only (no induced voltage), double RF with an
     acceleration-free programme: the fused engine against the drop-in
     objects (bmath rf_volt_comp + linear_interp_kick, turn by turn)."""
@@ -449,7 +450,8 @@ def test_fused_interpolated_tracker_without_impedance(cuda, precision):
                                         n_slices=S))
         tracker = RingAndRFTracker(rf, beam, interpolation=True, profile=prof)
         if fused_path:
-            f = FusedTracker(tracker, prof, precision=precision, turns_per_graph=4)
+            f = FusedTracker(tracker, prof, precision=precision, turns_per_graph=4,
+                             kernel=kernel)
             f.track(turns)
             f.sync()
         else:
