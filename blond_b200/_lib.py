@@ -105,6 +105,7 @@ _EXTRA = {
     "blond_engine_set_histogram": [c_ptr, c_int],
     "blond_engine_set_prefetch": [c_ptr, c_int],
     "blond_engine_set_l2_prefetch": [c_ptr, c_int],
+    "blond_engine_set_overlap": [c_ptr, c_int],
     "blond_engine_set_cluster": [c_ptr, c_int],
     "blond_engine_track_host": [c_ptr, c_ptr, c_ptr, c_i64, c_int, c_ptr],
     "blond_engine_autotune": [c_ptr, c_int, c_ptr, ct.POINTER(c_int), ct.POINTER(c_dbl)],

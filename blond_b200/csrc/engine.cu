@@ -1115,6 +1115,13 @@ int blond_engine_set_l2_prefetch(blond_engine* e, int on) {
     return BLOND_OK;
 }
 
+int blond_engine_set_overlap(blond_engine* e, int on) {
+    BB_CHECK_ARG(e, "engine_set_overlap: null engine");
+    e->pdl = on != 0;
+    e->graph_dirty = true;
+    return BLOND_OK;
+}
+
 int blond_engine_set_prefetch(blond_engine* e, int stages) {
     BB_CHECK_ARG(e && (stages == 0 || stages == 2 || stages == 4),
                  "engine_set_prefetch: stages must be 0, 2 or 4");
@@ -1142,6 +1149,114 @@ int blond_engine_set_histogram(blond_engine* e, int mode) {
 // launches each) and the fastest is kept.  The coordinates and the
 // histogram are snapshotted first and restored afterwards, so tuning does
 // not change the state of the run.
+}  // extern "C"
+
+namespace bb {
+
+// Whole turns (head + particle pass, as tracking runs them) replayed from a
+// graph of `turns` turns: one untimed replay, then `reps` timed; returns
+// the milliseconds per turn.  Advances the beam and the turn counter.
+static int time_graph_turns(blond_engine* e, cudaStream_t s, int turns, int reps, double* ms) {
+    int rc;
+    if ((rc = launch_particles(e, true, s, false))) return rc;
+    if (e->has_fft && (rc = prepare_spectral())) return rc;
+    cudaGraph_t g = nullptr;
+    BB_CUDA(cudaStreamBeginCapture(e->cap_stream, cudaStreamCaptureModeThreadLocal));
+    int lrc = BLOND_OK;
+    for (int i = 0; i < turns && lrc == BLOND_OK; ++i) lrc = launch_turn(e, e->cap_stream);
+    cudaError_t ce = cudaStreamEndCapture(e->cap_stream, &g);
+    if (lrc || ce != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        if (lrc) return lrc;
+        set_error("engine_autotune: graph capture failed: %s", cudaGetErrorString(ce));
+        return BLOND_ERR_CUDA;
+    }
+    cudaGraphExec_t x = nullptr;
+    ce = cudaGraphInstantiate(&x, g, 0);
+    cudaGraphDestroy(g);
+    if (ce != cudaSuccess) {
+        set_error("engine_autotune: graph instantiation failed: %s", cudaGetErrorString(ce));
+        return BLOND_ERR_CUDA;
+    }
+    cudaEvent_t a = nullptr, b = nullptr;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaGraphLaunch(x, s);
+    cudaEventRecord(a, s);
+    for (int r = 0; r < reps; ++r) cudaGraphLaunch(x, s);
+    cudaEventRecord(b, s);
+    ce = cudaEventSynchronize(b);
+    float t = 0.f;
+    if (ce == cudaSuccess) cudaEventElapsedTime(&t, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaGraphExecDestroy(x);
+    if (ce != cudaSuccess) {
+        set_error("engine_autotune: %s", cudaGetErrorString(ce));
+        return BLOND_ERR_CUDA;
+    }
+    *ms = (double)t / ((double)turns * reps);
+    return BLOND_OK;
+}
+
+// Programmatic dependent launch on or off, whichever replays whole turns
+// faster with the chosen particle pass (the early launch of the next
+// kernel pays at short profiles and costs at long ones).  Each setting
+// starts from the same snapshot of the turn counter, induced voltage and
+// profile, which are put back afterwards; the caller restores the beam and
+// histogram.  Skipped (overlap left as it is) with a beam-phase loop or
+// smooth slicing, whose turn state is not snapshotted, and when fewer
+// turns than it needs are left in the programme.
+static int tune_overlap(blond_engine* e, cudaStream_t s, const void* sdt, const void* sdE,
+                        const int* shist, int* chosen) {
+    constexpr int kTurns = 4, kReps = 3;
+    *chosen = e->pdl ? 1 : 0;
+    if (e->has_fb || e->smooth || e->host_turn + kTurns * (kReps + 1) > e->n_turns)
+        return BLOND_OK;
+    const size_t S = (size_t)e->S, n = (size_t)e->n, esz = energy_bytes(e->precision);
+    char* snap = nullptr;
+    if (cudaMalloc(&snap, 16 + 16 * S) != cudaSuccess) {
+        cudaGetLastError();
+        return BLOND_OK;  // no room for the snapshot: keep the setting
+    }
+    double* svind = reinterpret_cast<double*>(snap + 16);
+    double* sprof = svind + S;
+    cudaMemcpyAsync(snap, e->d_turn, sizeof(long long), cudaMemcpyDeviceToDevice, s);
+    if (e->d_vind) cudaMemcpyAsync(svind, e->d_vind, 8 * S, cudaMemcpyDeviceToDevice, s);
+    if (e->d_profile) cudaMemcpyAsync(sprof, e->d_profile, 8 * S, cudaMemcpyDeviceToDevice, s);
+    auto restore = [&]() {
+        cudaMemcpyAsync(e->dt, sdt, 8 * n, cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(e->dE, sdE, esz * n, cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(e->d_hist, shist, sizeof(int) * S, cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(e->d_turn, snap, sizeof(long long), cudaMemcpyDeviceToDevice, s);
+        if (e->d_vind) cudaMemcpyAsync(e->d_vind, svind, 8 * S, cudaMemcpyDeviceToDevice, s);
+        if (e->d_profile) cudaMemcpyAsync(e->d_profile, sprof, 8 * S, cudaMemcpyDeviceToDevice, s);
+    };
+    const bool keep = e->pdl;
+    double t[2] = {0.0, 0.0};
+    int rc = BLOND_OK;
+    for (int on = 1; on >= 0 && rc == BLOND_OK; --on) {
+        restore();
+        e->pdl = on != 0;
+        rc = time_graph_turns(e, s, kTurns, kReps, &t[on]);
+    }
+    restore();
+    const cudaError_t ce = cudaStreamSynchronize(s);
+    cudaFree(snap);
+    if (rc == BLOND_OK && ce != cudaSuccess) {
+        set_error("engine_autotune: %s", cudaGetErrorString(ce));
+        rc = BLOND_ERR_CUDA;
+    }
+    // overlap stays on unless it is clearly slower
+    e->pdl = rc == BLOND_OK ? !(t[0] < 0.97 * t[1]) : keep;
+    *chosen = e->pdl ? 1 : 0;
+    return rc;
+}
+
+}  // namespace bb
+
+extern "C" {
+
 int blond_engine_autotune(blond_engine* e, int reps, void* stream, int* config,
                           double* best_ms) {
     BB_CHECK_ARG(e && config && best_ms && reps >= 1 && reps <= 10,
@@ -1258,6 +1373,18 @@ int blond_engine_autotune(blond_engine* e, int reps, void* stream, int* config,
     }
     cudaEventDestroy(a);
     cudaEventDestroy(b);
+    // whole turns with the winner: overlap on or off
+    int overlap = e->pdl ? 1 : 0;
+    if (rc == BLOND_OK && best < 1e30) {
+        e->variant = win.variant;
+        e->threads = win.threads;
+        e->blocks_per_sm = win.bps;
+        e->hist_mode = win.hist;
+        e->ring = win.ring;
+        e->cluster = win.cluster;
+        e->l2_ahead = win.l2 != 0;
+        rc = tune_overlap(e, s, sdt, sdE, static_cast<const int*>(shist), &overlap);
+    }
     // restore the state of the run
     cudaMemcpyAsync(e->dt, sdt, 8 * n, cudaMemcpyDeviceToDevice, s);
     cudaMemcpyAsync(e->dE, sdE, esz * n, cudaMemcpyDeviceToDevice, s);
@@ -1289,6 +1416,7 @@ int blond_engine_autotune(blond_engine* e, int reps, void* stream, int* config,
     config[5] = use.cluster;
     config[6] = use.l2;
     config[7] = (int)cands.size();
+    config[8] = overlap;
     *best_ms = best < 1e30 ? best : 0.0;
     return rc;
 }

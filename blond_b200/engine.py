@@ -351,8 +351,10 @@ class FusedTracker:
     def autotune(self, reps: int = 3) -> dict:
         """Run the engine's autotuner now (blond_engine_autotune): times
         every feasible particle-pass configuration on this beam, keeps the
-        fastest and leaves the beam untouched.  Returns the choice."""
-        cfg = (ct.c_int * 8)()
+        fastest, then whole turns with and without the early launch of each
+        turn's next kernel ('overlap'), and leaves the beam and the turn
+        state untouched.  Returns the choice."""
+        cfg = (ct.c_int * 9)()
         ms = ct.c_double()
         self.eng.call("autotune", int(reps), _stream(), cfg, ct.byref(ms))
         names = {-1: "auto", 0: "smem-warp-aggregated", 1: "smem-int", 2: "smem-packed16",
@@ -362,6 +364,7 @@ class FusedTracker:
                       "blocks_per_sm": cfg[2], "histogram": names.get(cfg[3], cfg[3]),
                       "prefetch_stages": cfg[4], "cluster": cfg[5],
                       "l2_prefetch": bool(cfg[6]), "candidates": cfg[7],
+                      "overlap": bool(cfg[8]),
                       "particle_pass_ms": ms.value}
         self.kernel = self.tuned["kernel"]
         return self.tuned

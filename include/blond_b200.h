@@ -453,6 +453,11 @@ int blond_engine_set_prefetch(blond_engine* engine, int stages);
  * slice one iteration beyond the ring into L2 (cp.async.bulk.prefetch);
  * on = 0/1. */
 int blond_engine_set_l2_prefetch(blond_engine* engine, int on);
+/* Programmatic dependent launch between a turn's kernels (default on):
+ * each kernel lets the next one launch and run its prologue before the
+ * previous one's results are visible; on = 0 launches them in plain stream
+ * order.  The results are the same either way. */
+int blond_engine_set_overlap(blond_engine* engine, int on);
 /* Plain pass: blocks (1, 2, 4, 8) of a thread-block cluster whose shared
  * histograms are summed through distributed shared memory before one
  * global flush per cluster. */
@@ -460,12 +465,16 @@ int blond_engine_set_cluster(blond_engine* engine, int blocks);
 /* Autotuner: times every feasible particle-pass configuration (plain pass:
  * 256/512/1024 threads x 1/2/4 blocks per SM x histogram layouts x prefetch
  * ring 0/2/4 x clusters of 1/2; staged pass: histogram layouts; shared-table
- * pass: ring 0/2) on the bound beam, `reps` (1..10) launches each after one
- * warm-up, keeps the fastest and restores the coordinates and the
- * histogram.  config[8] receives {variant (0 staged, 1 plain, 2 shared
- * table), threads, blocks per SM, histogram
+ * pass: ring 0/2; packed-histogram pass: ring 0/2/4) on the bound beam,
+ * `reps` (1..10) launches each after one warm-up, and keeps the fastest;
+ * then replays a few whole turns with and without programmatic dependent
+ * launch (blond_engine_set_overlap) and keeps the faster (not with a
+ * beam-phase loop or smooth slicing).  Restores the coordinates, the
+ * histogram, the turn counter, the induced voltage and the profile.
+ * config[9] receives {variant (0 staged, 1 plain, 2 shared table,
+ * 3 packed histogram), threads, blocks per SM, histogram
  * layout, ring stages, cluster blocks, L2 prefetch (0/1), candidates
- * timed}; best_ms the
+ * timed, overlap (0/1)}; best_ms the
  * particle-pass time of the winner.  Not inside stream capture; allocates
  * a snapshot of the coordinates for the duration of the call. */
 int blond_engine_autotune(blond_engine* engine, int reps, void* stream, int* config,

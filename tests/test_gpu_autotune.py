@@ -148,6 +148,55 @@ def test_packed_histogram_pass_gives_the_plain_pass_bits(cuda, precision, slices
         np.testing.assert_array_equal(a, b)
 
 
+@pytest.mark.parametrize("slices", [16384, 65536])
+def test_overlap_tuning_restores_the_turn_state(cuda, slices):
+    """The autotuner's whole-turn replays (overlap on and off) start from
+    and return to the run's state: coordinates, profile, induced voltage
+    and turn counter; tracking afterwards gives the untuned run's bits."""
+    import bench
+    runs = []
+    for tune in ("auto", "fixed"):
+        fused, beam, _ = bench.build_fused(1_000_000, slices, 40, "f64")
+        if tune == "fixed":
+            fused.eng.call("tune", 1024, 1, 5)
+            fused.tune_mode = "fixed"
+        fused.track(2)
+        fused.sync()
+        before = (fused.dt.cpu().numpy().copy(), fused.profile_tensor().cpu().numpy(),
+                  fused.induced_voltage_tensor().cpu().numpy())
+        if tune == "auto":
+            cfg = fused.autotune(reps=1)
+            assert "overlap" in cfg
+            fused.sync()
+            after = (fused.dt.cpu().numpy(), fused.profile_tensor().cpu().numpy(),
+                     fused.induced_voltage_tensor().cpu().numpy())
+            for x, y in zip(before, after):
+                np.testing.assert_array_equal(x, y)
+        fused.track(10)
+        fused.check()
+        runs.append((fused.dt.cpu().numpy(), fused.dE.cpu().numpy(),
+                     fused.profile_tensor().cpu().numpy(),
+                     fused.induced_voltage_tensor().cpu().numpy()))
+    for x, y in zip(*runs):
+        np.testing.assert_array_equal(x, y)
+
+
+def test_overlap_off_gives_the_same_bits(cuda):
+    import bench
+    out = []
+    for on in (1, 0):
+        fused, beam, _ = bench.build_fused(1_000_000, 16384, 8, "f64", kernel="stab")
+        fused.eng.call("set_overlap", on)
+        fused.eng.call("tune", 1024, 1, 3)
+        fused.track(8)
+        fused.check()
+        out.append((fused.dt.cpu().numpy(), fused.dE.cpu().numpy(),
+                    fused.profile_tensor().cpu().numpy(),
+                    fused.induced_voltage_tensor().cpu().numpy()))
+    for x, y in zip(*out):
+        np.testing.assert_array_equal(x, y)
+
+
 def test_shared_table_pass_is_refused_where_it_does_not_apply(cuda):
     from blond_b200 import BlondB200Error
     g, beam, f = fused_for("track_rf.npz", precision="f64", kernel="stab")
