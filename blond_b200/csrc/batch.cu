@@ -78,8 +78,7 @@ particle_kernel_batch(const BatchArgs a) {
             for (int j = threadIdx.x; j < a.n_rf; j += blockDim.x) {
                 c.V[j] = a.V[(rb + t) * a.n_rf + j];
                 c.Vf[j] = (float)c.V[j];
-                c.om[j] = a.om[(rb + t) * a.n_rf + j];
-                c.ph[j] = a.ph[(rb + t) * a.n_rf + j];
+                c.op[j] = make_double2(a.om[(rb + t) * a.n_rf + j], a.ph[(rb + t) * a.n_rf + j]);
             }
             if (threadIdx.x == 0) {
                 c.acc = a.acc[(long long)b * a.n_turns + t];

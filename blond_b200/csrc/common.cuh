@@ -104,12 +104,21 @@ template <> struct Vec2<int> { using type = int2; };
 // and k P2 are exact for |k| < 2^23 -- to r in [-pi/2, pi/2], then the
 // Taylor series of sin through r^21 (the next term is below 1.2e-18 on that
 // interval) by Horner's rule in r^2, and sin(x) = (-1)^k sin(r).  No
-// branch on the quadrant, so a warp's particles stay converged.  Beyond
-// |x| = 1e7 (and for NaN / inf) CUDA's sin is used.  Within a few units in
+// branch on the quadrant, so a warp's particles stay converged; k is
+// rounded with the 1.5 * 2^52 shifter rather than a rounding and a
+// conversion instruction.  Beyond |x| = 1e7 (and for NaN / inf) CUDA's sin
+// is used.  Within a few units in
 // the last place of the correctly rounded sine (tested against numpy).
 __device__ __forceinline__ double rf_sin(double x) {
-    if (!(fabs(x) < 1e7)) return sin(x);
-    const double k = rint(x * 0.3183098861837907);  // 1 / pi
+    if (!(fabs(x) < 1e7)) return sin(x);  // the rare long way (also NaN / inf)
+    // k = rint(x / pi): adding and subtracting 1.5 * 2^52 rounds the
+    // (rounded) quotient to the nearest integer, ties to even, exactly as
+    // rint does for |x / pi| < 2^51, and leaves k's parity in the low bit
+    // of the shifted sum
+    const double shifter = 6755399441055744.0;  // 1.5 * 2^52
+    const double y = __dmul_rn(x, 0.3183098861837907);  // 1 / pi
+    const double ks = __dadd_rn(y, shifter);
+    const double k = __dsub_rn(ks, shifter);
     double r = fma(-k, 3.1415926553308964, x);       // P1
     r = fma(-k, -1.7411031384001463e-09, r);          // P2
     r = fma(-k, -7.00686879617986e-19, r);            // P3
@@ -125,8 +134,8 @@ __device__ __forceinline__ double rf_sin(double x) {
     p = fma(p, r2, -0.0001984126984126984);
     p = fma(p, r2, 0.008333333333333333);
     p = fma(p, r2, -0.16666666666666666);
-    const double s = fma(r * r2, p, r);
-    return (static_cast<long long>(k) & 1) ? -s : s;
+    double s = fma(r * r2, p, r);
+    return (__double2loint(ks) & 1) ? -s : s;
 }
 
 __device__ __forceinline__ double dev_sin(double x) { return rf_sin(x); }

@@ -135,8 +135,9 @@ __device__ __forceinline__ typename TableEntry<PREC>::T table_at(const ParticleA
     }
 }
 
-struct TurnConsts {
-    double V[kMaxRfEngine], om[kMaxRfEngine], ph[kMaxRfEngine];
+struct __align__(16) TurnConsts {
+    double2 op[kMaxRfEngine];  // {omega_rf, phi_rf}: one 16-byte load per harmonic
+    double V[kMaxRfEngine];
     float Vf[kMaxRfEngine];
     double acc;
     DriftTurn d;
@@ -169,7 +170,7 @@ __device__ __forceinline__ void track_one(double& t,
                 }
             }
             double s = 0.0;
-            for (int j = 0; j < a.n_rf; ++j) s += c.V[j] * rf_sin(c.om[j] * t + c.ph[j]);
+            for (int j = 0; j < a.n_rf; ++j) s += c.V[j] * rf_sin(c.op[j].x * t + c.op[j].y);
             e = q32_add(e, inc + (a.charge * s + c.acc), a);
         } else {
             if (LIK) {
@@ -187,12 +188,12 @@ __device__ __forceinline__ void track_one(double& t,
             }
             if (PREC == PREC_F64) {
                 double s = 0.0;
-                for (int j = 0; j < a.n_rf; ++j) s += c.V[j] * rf_sin(c.om[j] * t + c.ph[j]);
+                for (int j = 0; j < a.n_rf; ++j) s += c.V[j] * rf_sin(c.op[j].x * t + c.op[j].y);
                 e += a.charge * s + c.acc;
             } else {
                 float s = 0.0f;
                 for (int j = 0; j < a.n_rf; ++j)
-                    s += c.Vf[j] * sinf((float)reduce_2pi(fma(c.om[j], t, c.ph[j])));
+                    s += c.Vf[j] * sinf((float)reduce_2pi(fma(c.op[j].x, t, c.op[j].y)));
                 e += (float)a.charge * s + (float)c.acc;
             }
         }
@@ -225,11 +226,13 @@ __device__ __forceinline__ void track_pair(double& t0, double& t1,
     TB tb0, tb1;
     float x0f = 0.0f, x1f = 0.0f;  // F32P64: offsets from the slice centre
     if (LIK) {
-        const double f0 = floor((t0 - a.bc0) * a.lik_inv_w);
-        const double f1 = floor((t1 - a.bc0) * a.lik_inv_w);
-        in0 = f0 >= 0.0 && f0 < (double)(a.S - 1);
-        in1 = f1 >= 0.0 && f1 < (double)(a.S - 1);
-        const int k0 = in0 ? (int)f0 : 0, k1 = in1 ? (int)f1 : 0;
+        // y in [0, S - 1) exactly when floor(y) is; there the round-down
+        // conversion is floor(y)
+        const double y0 = (t0 - a.bc0) * a.lik_inv_w;
+        const double y1 = (t1 - a.bc0) * a.lik_inv_w;
+        in0 = y0 >= 0.0 && y0 < (double)(a.S - 1);
+        in1 = y1 >= 0.0 && y1 < (double)(a.S - 1);
+        const int k0 = in0 ? __double2int_rd(y0) : 0, k1 = in1 ? __double2int_rd(y1) : 0;
         tb0 = table_at<PREC, TAB>(a, stab, k0);
         tb1 = table_at<PREC, TAB>(a, stab, k1);
         if (PREC == PREC_F32P64) {
@@ -242,8 +245,8 @@ __device__ __forceinline__ void track_pair(double& t0, double& t1,
         // the turn's whole energy change in float64, rounded once per particle
         double x0 = 0.0, x1 = 0.0;
         for (int j = 0; j < a.n_rf; ++j) {
-            x0 += c.V[j] * rf_sin(c.om[j] * t0 + c.ph[j]);
-            x1 += c.V[j] * rf_sin(c.om[j] * t1 + c.ph[j]);
+            x0 += c.V[j] * rf_sin(c.op[j].x * t0 + c.op[j].y);
+            x1 += c.V[j] * rf_sin(c.op[j].x * t1 + c.op[j].y);
         }
         const double i0 = (LIK && in0) ? __fma_rn(t0, tb0.x, tb0.y) : 0.0;
         const double i1 = (LIK && in1) ? __fma_rn(t1, tb1.x, tb1.y) : 0.0;
@@ -254,16 +257,16 @@ __device__ __forceinline__ void track_pair(double& t0, double& t1,
         if (PREC == PREC_F64) {
             double x0 = 0.0, x1 = 0.0;
             for (int j = 0; j < a.n_rf; ++j) {
-                x0 += c.V[j] * rf_sin(c.om[j] * t0 + c.ph[j]);
-                x1 += c.V[j] * rf_sin(c.om[j] * t1 + c.ph[j]);
+                x0 += c.V[j] * rf_sin(c.op[j].x * t0 + c.op[j].y);
+                x1 += c.V[j] * rf_sin(c.op[j].x * t1 + c.op[j].y);
             }
             s0 = (E)x0;
             s1 = (E)x1;
         } else {
             float x0 = 0.0f, x1 = 0.0f;
             for (int j = 0; j < a.n_rf; ++j) {
-                x0 += c.Vf[j] * sinf((float)reduce_2pi(fma(c.om[j], t0, c.ph[j])));
-                x1 += c.Vf[j] * sinf((float)reduce_2pi(fma(c.om[j], t1, c.ph[j])));
+                x0 += c.Vf[j] * sinf((float)reduce_2pi(fma(c.op[j].x, t0, c.op[j].y)));
+                x1 += c.Vf[j] * sinf((float)reduce_2pi(fma(c.op[j].x, t1, c.op[j].y)));
             }
             s0 = (E)x0;
             s1 = (E)x1;
@@ -297,8 +300,8 @@ __device__ __forceinline__ void track_pair(double& t0, double& t1,
 }
 
 __device__ __forceinline__ int engine_bin(double t, double cut_left, double inv_w, int S) {
-    const double f = floor(__dmul_rn(__dsub_rn(t, cut_left), inv_w));
-    return (f >= 0.0 && f < (double)S) ? (int)f : -1;
+    const double y = __dmul_rn(__dsub_rn(t, cut_left), inv_w);
+    return (y >= 0.0 && y < (double)S) ? __double2int_rd(y) : -1;
 }
 
 __device__ __forceinline__ void deposit(int* sh, int b, bool warp_agg, unsigned mask) {
@@ -329,17 +332,18 @@ enum { HIST_AGG = 0, HIST_I32 = 1, HIST_PACKED = 2 };
 // needs no ordering between threads.
 __device__ __forceinline__ void deposit_packed(unsigned* sh, int half, int* gh, int b) {
     if (b < 0) return;
-    if (b < half) {
-        const unsigned old = atomicAdd(&sh[b], 1u);
-        if ((old & 0xffffu) == 0xffffu) {
-            atomicAdd(&gh[b], 65536);
+    // one atomic for either half; the wrap test and its carries are the
+    // rare branch
+    const bool lo = b < half;
+    const int w = lo ? b : b - half;
+    const unsigned old = atomicAdd(&sh[w], lo ? 1u : 0x10000u);
+    if ((lo ? (old & 0xffffu) : (old >> 16)) == 0xffffu) {
+        atomicAdd(&gh[b], 65536);
+        if (lo) {
             if ((old >> 16) == 0xffffu) atomicAdd(&gh[b + half], 65536);
             const unsigned o2 = atomicSub(&sh[b], 0x10000u);
             if ((o2 >> 16) == 0u) atomicAdd(&gh[b + half], -65536);
         }
-    } else {
-        const unsigned old = atomicAdd(&sh[b - half], 0x10000u);
-        if ((old >> 16) == 0xffffu) atomicAdd(&gh[b], 65536);
     }
 }
 
@@ -512,8 +516,7 @@ particle_kernel(const ParticleArgs a) {
         for (int j = threadIdx.x; j < a.n_rf; j += blockDim.x) {
             c.V[j] = a.V[t_idx * a.n_rf + j];
             c.Vf[j] = (float)c.V[j];
-            c.om[j] = a.om[t_idx * a.n_rf + j];
-            c.ph[j] = a.ph[t_idx * a.n_rf + j];
+            c.op[j] = make_double2(a.om[t_idx * a.n_rf + j], a.ph[t_idx * a.n_rf + j]);
         }
         if (threadIdx.x == 0) {
             c.acc = a.interp ? 0.0 : a.acc[t_idx];
@@ -670,8 +673,7 @@ particle_kernel_stab(const ParticleArgs a) {
     for (int j = threadIdx.x; j < a.n_rf; j += blockDim.x) {
         c.V[j] = a.V[t_idx * a.n_rf + j];
         c.Vf[j] = (float)c.V[j];
-        c.om[j] = a.om[t_idx * a.n_rf + j];
-        c.ph[j] = a.ph[t_idx * a.n_rf + j];
+        c.op[j] = make_double2(a.om[t_idx * a.n_rf + j], a.ph[t_idx * a.n_rf + j]);
     }
     if (threadIdx.x == 0) {
         c.acc = a.interp ? 0.0 : a.acc[t_idx];
@@ -859,8 +861,7 @@ particle_kernel_tma(const ParticleArgs a, int* err) {
     for (int j = threadIdx.x; j < a.n_rf; j += blockDim.x) {
         c.V[j] = a.V[t_idx * a.n_rf + j];
         c.Vf[j] = (float)c.V[j];
-        c.om[j] = a.om[t_idx * a.n_rf + j];
-        c.ph[j] = a.ph[t_idx * a.n_rf + j];
+        c.op[j] = make_double2(a.om[t_idx * a.n_rf + j], a.ph[t_idx * a.n_rf + j]);
     }
     if (threadIdx.x == 0) {
         c.acc = a.interp ? 0.0 : a.acc[t_idx];
