@@ -411,6 +411,10 @@ def run_ours(args, world, rank, local):
                                 "packed": "particle_kernel_stab<TAB_GLOBAL>"}
                                .get(fused.kernel, "particle_kernel") + " (lik+kick+drift+deposit)",
                      "kernel_ms": part_avg, "head_kernel_ms": head_avg,
+                     # the head's share of a graph-replayed turn: the turn
+                     # minus the particle pass's own event-timed launch
+                     "head_exposed_ms": max(0.0, ms_max / K - part_avg),
+                     "turn_frac": alg_bytes / (ms_max / K * 1e-3) / 1e9 / peak,
                      "bytes_per_particle": BYTES_PER_PARTICLE[args.precision],
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst copy)"
                      if peaks.get("hbm_gbs") else "fallback 6650 GB/s"},

@@ -104,13 +104,14 @@ template <> struct Vec2<int> { using type = int2; };
 // and k P2 are exact for |k| < 2^23 -- to r in [-pi/2, pi/2], then the
 // Taylor series of sin through r^21 (the next term is below 1.2e-18 on that
 // interval) by Horner's rule in r^2, and sin(x) = (-1)^k sin(r).  No
-// branch on the quadrant, so a warp's particles stay converged; k is
-// rounded with the 1.5 * 2^52 shifter rather than a rounding and a
-// conversion instruction.  Beyond |x| = 1e7 (and for NaN / inf) CUDA's sin
-// is used.  Within a few units in
-// the last place of the correctly rounded sine (tested against numpy).
+// branch at all, so a warp's particles stay converged; k is rounded with
+// the 1.5 * 2^52 shifter rather than a rounding and a conversion
+// instruction.  Within a few units in the last place of the correctly
+// rounded sine for |x| < 1e9 (tested against numpy); beyond, the reduction
+// is done with fused multiply-adds, each rounding once, so the error grows
+// like |x| * 1e-25 (about 1e-13 at 1e12).  Valid for |x| < 2^51 pi (7e15
+// rad, hours of beam time at any RF frequency); NaN and inf give NaN.
 __device__ __forceinline__ double rf_sin(double x) {
-    if (!(fabs(x) < 1e7)) return sin(x);  // the rare long way (also NaN / inf)
     // k = rint(x / pi): adding and subtracting 1.5 * 2^52 rounds the
     // (rounded) quotient to the nearest integer, ties to even, exactly as
     // rint does for |x / pi| < 2^51, and leaves k's parity in the low bit

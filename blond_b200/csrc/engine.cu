@@ -719,6 +719,10 @@ static int launch_spectral_head(blond_engine* e, cudaStream_t s, bool loop) {
     P.twg = e->d_tw;
     // the interpolated tracker's table (RF + induced voltage) follows the head
     if (e->interp) P.table = nullptr;
+    // the shared-table pass forms FP64 / Q32P64 entries from the voltage
+    // itself: no table to write (the beam-phase loop's SPS_RL average reads
+    // it, so it stays with a loop)
+    if (e->variant == 2 && e->precision != BLOND_PREC_F32P64 && !e->has_fb) P.table = nullptr;
     int rc;
     if (loop) {
         SpecLoop L;

@@ -13,6 +13,7 @@
 #include <cstddef>
 #include <mutex>
 #include <set>
+#include <type_traits>
 #include <utility>
 #include <vector>
 
@@ -121,6 +122,13 @@ __device__ __forceinline__ double bin_centre(const ParticleArgs& a, int k) {
     return __dmul_rn(__dadd_rn(e0, e1), 0.5);
 }
 
+// The same for k + 1 < S (every table entry: k <= S - 2).
+__device__ __forceinline__ double bin_centre_inner(const ParticleArgs& a, int k) {
+    const double e0 = __dadd_rn(__dmul_rn((double)k, a.bc_step), a.cut_left);
+    const double e1 = __dadd_rn(__dmul_rn((double)(k + 1), a.bc_step), a.cut_left);
+    return __dmul_rn(__dadd_rn(e0, e1), 0.5);
+}
+
 template <int PREC, int TAB>
 __device__ __forceinline__ typename TableEntry<PREC>::T table_at(const ParticleArgs& a,
                                                                  const void* stab, int k) {
@@ -131,7 +139,7 @@ __device__ __forceinline__ typename TableEntry<PREC>::T table_at(const ParticleA
         return reinterpret_cast<const float2*>(stab)[k];
     } else {
         const double* V = reinterpret_cast<const double*>(stab);
-        return lik_entry(V[k], V[k + 1], bin_centre(a, k), a.charge, a.lik_inv_w, 0.0);
+        return lik_entry(V[k], V[k + 1], bin_centre_inner(a, k), a.charge, a.lik_inv_w, 0.0);
     }
 }
 
@@ -345,6 +353,15 @@ __device__ __forceinline__ void deposit_packed(unsigned* sh, int half, int* gh, 
             if ((o2 >> 16) == 0u) atomicAdd(&gh[b + half], -65536);
         }
     }
+}
+
+// Packed deposit while no counter can wrap (the block has deposited at
+// most 65535 particles since its counters were zero): no returned value,
+// no test.
+__device__ __forceinline__ void deposit_packed_nowrap(unsigned* sh, int half, int b) {
+    if (b < 0) return;
+    const bool lo = b < half;
+    atomicAdd(&sh[lo ? b : b - half], lo ? 1u : 0x10000u);
 }
 
 template <int HIST>
@@ -701,10 +718,25 @@ particle_kernel_stab(const ParticleArgs a) {
     const int lane = threadIdx.x & 31;
     int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31);
     const uint64_t pol = evict_first_policy();
+    // The block deposits at most 2 x blockDim particles an iteration, so for
+    // its first `safe` iterations (<= 65535 deposits) no counter can wrap
+    // and the deposits skip the wrap test; a barrier separates them from
+    // the tested ones (warps are not in step inside the loop).  Ring
+    // variants only.
+    const int safe = 65535 / (2 * (int)blockDim.x);
+    auto deposit2 = [&](int b0, int b1, auto tested) {
+        if constexpr (decltype(tested)::value) {
+            deposit_packed(sh, half, a.hist, b0);
+            deposit_packed(sh, half, a.hist, b1);
+        } else {
+            deposit_packed_nowrap(sh, half, b0);
+            deposit_packed_nowrap(sh, half, b1);
+        }
+    };
     if (NST == 0) {
         ring_wait<0>();
         __syncthreads();  // every thread's part of the table has landed
-        for (; base < npairs; base += stride) {
+        auto step = [&](auto tested) {
             const int64_t p = base + lane;
             int b0 = -1, b1 = -1;
             if (p < npairs) {
@@ -716,9 +748,10 @@ particle_kernel_stab(const ParticleArgs a) {
                 b0 = engine_bin(tt.x, a.cut_left, a.inv_w, S);
                 b1 = engine_bin(tt.y, a.cut_left, a.inv_w, S);
             }
-            deposit_packed(sh, half, a.hist, b0);
-            deposit_packed(sh, half, a.hist, b1);
-        }
+            deposit2(b0, b1, tested);
+        };
+        // (without the ring the split loop measured slower at 2^16 slices)
+        for (; base < npairs; base += stride) step(std::true_type{});
     } else {
         double2* rdt = reinterpret_cast<double2*>(dsm + tpad + hpad);
         E2* rdE = reinterpret_cast<E2*>(rdt + (size_t)NST * blockDim.x);
@@ -738,7 +771,7 @@ particle_kernel_stab(const ParticleArgs a) {
         ring_wait<NST - 1>();
         __syncthreads();
         int slot = 0;
-        for (; base < npairs; base += stride) {
+        auto step = [&](auto tested) {
             fill(slot == 0 ? NST - 1 : slot - 1, base + (NST - 1) * stride + lane);
             if (a.l2_ahead && threadIdx.x == 0) {
                 const int64_t pb = base + (int64_t)NST * stride;
@@ -762,10 +795,13 @@ particle_kernel_stab(const ParticleArgs a) {
                 b0 = engine_bin(tt.x, a.cut_left, a.inv_w, S);
                 b1 = engine_bin(tt.y, a.cut_left, a.inv_w, S);
             }
-            deposit_packed(sh, half, a.hist, b0);
-            deposit_packed(sh, half, a.hist, b1);
+            deposit2(b0, b1, tested);
             slot = slot + 1 == NST ? 0 : slot + 1;
-        }
+        };
+        int it = 0;
+        for (; base < npairs && it < safe; base += stride, ++it) step(std::false_type{});
+        __syncthreads();
+        for (; base < npairs; base += stride) step(std::true_type{});
         ring_wait<0>();
     }
     // odd tail particle

@@ -49,17 +49,24 @@ def test_kick_sine_against_numpy(cuda):
     """The FP64 kick's sine (Cody-Waite reduction by pi, Taylor series on
     [-pi/2, pi/2]): a kick with V = 1, omega = 1, phi = 0, charge 1 from
     dE = 0 leaves exactly sin(dt) in dE.  Against numpy's sine over the RF
-    phase's range and far beyond (to 1e7 rad, where CUDA's sin takes over):
-    within 4e-16 absolute (two units in the last place of 1)."""
+    phase's range and far beyond (to 3e8 rad): within 4e-16 absolute (two
+    units in the last place of 1); to 1e12 rad within 2e-13 (the reduction's
+    roundings grow with |x|); NaN and inf give NaN."""
     rng = np.random.default_rng(11)
     x = np.concatenate([rng.uniform(-4, 4, 100000), rng.uniform(-1e3, 1e3, 100000),
                         rng.uniform(-1e6, 1e6, 20000), rng.uniform(9e6, 2e7, 1000),
+                        rng.uniform(-3e8, 3e8, 1000),
                         [0.0, -0.0, np.pi, -np.pi / 2, 1e-300, 5e-324, 1e7, 3e8]])
-    dt = _dev(x)
+    far = np.concatenate([rng.uniform(1e9, 1e12, 1000), -rng.uniform(1e9, 1e12, 1000)])
+    special = np.array([np.nan, np.inf, -np.inf])
+    dt = _dev(np.concatenate([x, far, special]))
     dE = torch.zeros_like(dt)
     bm.kick(dt, dE, [1.0], [1.0], [0.0], 1.0, 1, 0.0)
     got = dE.cpu().numpy()
-    assert np.max(np.abs(got - np.sin(x))) <= 4e-16
+    n, m = len(x), len(far)
+    assert np.max(np.abs(got[:n] - np.sin(x))) <= 4e-16
+    assert np.max(np.abs(got[n:n + m] - np.sin(far))) <= 2e-13
+    assert np.all(np.isnan(got[n + m:]))
 
 
 @pytest.mark.parametrize("dtype", [np.float64, np.float32])
