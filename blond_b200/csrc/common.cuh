@@ -199,6 +199,17 @@ __device__ __forceinline__ double2 lik_entry(double v0, double v1, double bc, do
     return make_double2(slope, offset);
 }
 
+// The same with no acceleration kick in the offset (the fused turn applies
+// it with the RF kick): the "+ 0" is left out, which changes nothing but
+// the sign of a zero offset.  The head's table and the shared-table pass
+// both use this form, so they agree bit for bit.
+__device__ __forceinline__ double2 lik_entry0(double v0, double v1, double bc, double charge,
+                                              double inv_w) {
+    const double slope = __dmul_rn(__dmul_rn(charge, __dsub_rn(v1, v0)), inv_w);
+    const double offset = __dsub_rn(__dmul_rn(charge, v0), __dmul_rn(bc, slope));
+    return make_double2(slope, offset);
+}
+
 // ------------------------------------------------------ smooth deposit weights
 // histogram.cpp:75-132.  Weights of a particle at f = (dt-cut_left)*inv_w,
 // k = (int)f, d = f-k: bin k gets 0.5-d; bin k+1 (d > 0.5) or k-1 (else)

@@ -139,7 +139,7 @@ __device__ __forceinline__ typename TableEntry<PREC>::T table_at(const ParticleA
         return reinterpret_cast<const float2*>(stab)[k];
     } else {
         const double* V = reinterpret_cast<const double*>(stab);
-        return lik_entry(V[k], V[k + 1], bin_centre_inner(a, k), a.charge, a.lik_inv_w, 0.0);
+        return lik_entry0(V[k], V[k + 1], bin_centre_inner(a, k), a.charge, a.lik_inv_w);
     }
 }
 
@@ -234,13 +234,16 @@ __device__ __forceinline__ void track_pair(double& t0, double& t1,
     TB tb0, tb1;
     float x0f = 0.0f, x1f = 0.0f;  // F32P64: offsets from the slice centre
     if (LIK) {
-        // y in [0, S - 1) exactly when floor(y) is; there the round-down
-        // conversion is floor(y)
+        // floor(y) in [0, S - 2] exactly when y is in [0, S - 1); the
+        // round-down conversion saturates outside the int range, so one
+        // unsigned compare tests it.  (A NaN y converts to 0 and takes
+        // entry 0; its particle's energy is NaN from the RF kick anyway.)
         const double y0 = (t0 - a.bc0) * a.lik_inv_w;
         const double y1 = (t1 - a.bc0) * a.lik_inv_w;
-        in0 = y0 >= 0.0 && y0 < (double)(a.S - 1);
-        in1 = y1 >= 0.0 && y1 < (double)(a.S - 1);
-        const int k0 = in0 ? __double2int_rd(y0) : 0, k1 = in1 ? __double2int_rd(y1) : 0;
+        const int r0 = __double2int_rd(y0), r1 = __double2int_rd(y1);
+        in0 = (unsigned)r0 < (unsigned)(a.S - 1);
+        in1 = (unsigned)r1 < (unsigned)(a.S - 1);
+        const int k0 = in0 ? r0 : 0, k1 = in1 ? r1 : 0;
         tb0 = table_at<PREC, TAB>(a, stab, k0);
         tb1 = table_at<PREC, TAB>(a, stab, k1);
         if (PREC == PREC_F32P64) {
@@ -308,8 +311,12 @@ __device__ __forceinline__ void track_pair(double& t0, double& t1,
 }
 
 __device__ __forceinline__ int engine_bin(double t, double cut_left, double inv_w, int S) {
+    // floor(y) in [0, S) exactly when y is in [0, S); the round-down
+    // conversion saturates outside the int range and gives 0 for NaN,
+    // which the y == y test excludes
     const double y = __dmul_rn(__dsub_rn(t, cut_left), inv_w);
-    return (y >= 0.0 && y < (double)S) ? __double2int_rd(y) : -1;
+    const int k = __double2int_rd(y);
+    return ((unsigned)k < (unsigned)S && y == y) ? k : -1;
 }
 
 __device__ __forceinline__ void deposit(int* sh, int b, bool warp_agg, unsigned mask) {

@@ -767,7 +767,7 @@ spectral_kernel(const SpecParams P, const typename SpecLoopArg<FB>::type LP) {
                 if (!P.table_f32) {
                     // linear_interp_kick.cpp:44-47 with acc = 0
                     reinterpret_cast<double2*>(g_table)[n] =
-                        lik_entry(a0, a1, bcn, P.charge, inv_w, 0.0);
+                        lik_entry0(a0, a1, bcn, P.charge, inv_w);
                 } else {
                     reinterpret_cast<float2*>(g_table)[n] =
                         make_float2((float)(P.charge * a0),
