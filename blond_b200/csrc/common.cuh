@@ -101,9 +101,9 @@ template <> struct Vec2<int> { using type = int2; };
 // see (|x| up to ~1e3 rad): Cody-Waite reduction by pi (W. J. Cody and
 // W. Waite, "Software Manual for the Elementary Functions", 1980) with pi
 // split in three parts -- the first two with 30 significant bits, so k P1
-// and k P2 are exact for |k| < 2^23 -- to r in [-pi/2, pi/2], then the
-// Taylor series of sin through r^21 (the next term is below 1.2e-18 on that
-// interval) by Horner's rule in r^2, and sin(x) = (-1)^k sin(r).  No
+// and k P2 are exact for |k| < 2^23 -- to r in [-pi/2, pi/2], then an odd
+// polynomial through r^17 (a Chebyshev approximation, coefficients from
+// gen_sin_coeffs.py) by Horner's rule in r^2, and sin(x) = (-1)^k sin(r).  No
 // branch at all, so a warp's particles stay converged; k is rounded with
 // the 1.5 * 2^52 shifter rather than a rounding and a conversion
 // instruction.  Within a few units in the last place of the correctly
@@ -124,16 +124,15 @@ __device__ __forceinline__ double rf_sin(double x) {
     r = fma(-k, -1.7411031384001463e-09, r);          // P2
     r = fma(-k, -7.00686879617986e-19, r);            // P3
     const double r2 = r * r;
-    // (-1)^n / (2n + 1)!, n = 10 .. 1
-    double p = 1.9572941063391263e-20;
-    p = fma(p, r2, -8.22063524662433e-18);
-    p = fma(p, r2, 2.8114572543455206e-15);
-    p = fma(p, r2, -7.647163731819816e-13);
-    p = fma(p, r2, 1.6059043836821613e-10);
-    p = fma(p, r2, -2.505210838544172e-08);
-    p = fma(p, r2, 2.7557319223985893e-06);
-    p = fma(p, r2, -0.0001984126984126984);
-    p = fma(p, r2, 0.008333333333333333);
+    // sin r = r + r^3 P(r^2), P the degree-7 Chebyshev approximation on
+    // [0, (pi/2)^2] (gen_sin_coeffs.py; error below 1.3e-18)
+    double p = 2.7314447669863995e-15;
+    p = fma(p, r2, -7.643970296798572e-13);
+    p = fma(p, r2, 1.6058977312464087e-10);
+    p = fma(p, r2, -2.5052107616996182e-08);
+    p = fma(p, r2, 2.7557319219163234e-06);
+    p = fma(p, r2, -0.00019841269841254974);
+    p = fma(p, r2, 0.008333333333333316);
     p = fma(p, r2, -0.16666666666666666);
     double s = fma(r * r2, p, r);
     return (__double2loint(ks) & 1) ? -s : s;

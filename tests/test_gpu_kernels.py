@@ -46,7 +46,7 @@ def test_kick(cuda, dtype, n):
 
 
 def test_kick_sine_against_numpy(cuda):
-    """The FP64 kick's sine (Cody-Waite reduction by pi, Taylor series on
+    """The FP64 kick's sine (Cody-Waite reduction by pi, odd polynomial on
     [-pi/2, pi/2]): a kick with V = 1, omega = 1, phi = 0, charge 1 from
     dE = 0 leaves exactly sin(dt) in dE.  Against numpy's sine over the RF
     phase's range and far beyond (to 3e8 rad): within 4e-16 absolute (two
