@@ -20,6 +20,9 @@ namespace bb {
 
 constexpr int kBatchChunkDefault = 32768;
 constexpr int kBatchMaxThreads = 1024;
+// Largest histogram + table copy per block (four 256-thread blocks per SM
+// stay resident).
+constexpr size_t kBatchTableSmem = 48 * 1024;
 
 struct BatchArgs {
     void* dt;
@@ -55,12 +58,16 @@ struct BatchArgs {
 // The launch bound (1024 threads, one block) caps registers at 64 a thread,
 // so every shape with at most 1024 resident threads per SM runs the same
 // code.
-template <int PREC, int SOLVER, bool LIK, bool KICK, int PPT>
+// TSM: the beam's interpolation table is copied into shared memory (after
+// the histogram) at the start of every chunk, for short profiles.
+template <int PREC, int SOLVER, bool LIK, bool KICK, int PPT, bool TSM = false>
 __global__ void __launch_bounds__(kBatchMaxThreads, 1)
 particle_kernel_batch(const BatchArgs a) {
     using E = typename Coord<PREC>::E;
+    using TB = typename TableEntry<PREC>::T;
     static_assert(PPT == 2 || PPT == 4 || PPT == 8, "particles per thread");
-    extern __shared__ int sh[];
+    extern __shared__ __align__(16) int sh[];
+    TB* stab = reinterpret_cast<TB*>(reinterpret_cast<char*>(sh) + pad16((size_t)a.S * 4));
     __shared__ TurnConsts c;
     long long t = a.turn ? (*a.turn - 1) : 0;
     if (t < 0) t = 0;
@@ -85,7 +92,18 @@ particle_kernel_batch(const BatchArgs a) {
                 c.d = a.drift[rb + t + 1];
             }
         }
+        if constexpr (TSM && LIK) {
+            // the beam's S - 1 entries (L2-resident), asynchronously, one
+            // entry-sized copy each (entries are 16- or 8-byte aligned)
+            const TB* src = reinterpret_cast<const TB*>(a.table) + (long long)b * S;
+            for (int k = threadIdx.x; k < S - 1; k += blockDim.x) {
+                if constexpr (sizeof(TB) == 16) copy16_async(&stab[k], &src[k]);
+                else copy8_async(&stab[k], &src[k]);
+            }
+            ring_commit();
+        }
         for (int k = threadIdx.x; k < S; k += blockDim.x) sh[k] = 0;
+        if constexpr (TSM && LIK) ring_wait<0>();
         __syncthreads();
         ParticleArgs pa = {};
         pa.n_rf = a.n_rf;
@@ -133,8 +151,8 @@ particle_kernel_batch(const BatchArgs a) {
             if (KICK) {
 #pragma unroll
                 for (int q = 0; q < PPT; q += 2)
-                    track_pair<PREC, SOLVER, LIK>(tq[q], tq[q + 1], e[q], e[q + 1], c, pa,
-                                                  a.order);
+                    track_pair<PREC, SOLVER, LIK, (TSM && LIK) ? TAB_ENTRIES : TAB_GLOBAL>(
+                        tq[q], tq[q + 1], e[q], e[q + 1], c, pa, a.order, stab);
 #pragma unroll
                 for (int q = 0; q < PPT; ++q) {
                     if (in[q]) {
@@ -244,14 +262,26 @@ static BatchArgs batch_args(blond_batch* q) {
     return a;
 }
 
+// Shared memory of the batched pass: the histogram, and with the table
+// copy (short profiles) the table after it; 0 when the copy does not fit.
+template <int PREC>
+static int batch_table_smem(const blond_batch* q) {
+    const size_t bytes = pad16((size_t)q->S * 4) +
+                         pad16((size_t)(q->S - 1) * sizeof(typename TableEntry<PREC>::T));
+    return bytes <= kBatchTableSmem ? (int)bytes : 0;
+}
+
 template <int PREC, int SOLVER, bool LIK, bool KICK, int PPT>
 static int launch_batch_k(blond_batch* q, cudaStream_t s, bool launch) {
     static bool done[64] = {false};
-    auto k = particle_kernel_batch<PREC, SOLVER, LIK, KICK, PPT>;
+    static bool done_t[64] = {false};
+    const int tsm = (LIK && KICK) ? batch_table_smem<PREC>(q) : 0;
+    auto k = tsm ? particle_kernel_batch<PREC, SOLVER, LIK, KICK, PPT, true>
+                 : particle_kernel_batch<PREC, SOLVER, LIK, KICK, PPT, false>;
     int rc;
-    if ((rc = allow_max_smem(k, done))) return rc;
+    if ((rc = allow_max_smem(k, tsm ? done_t : done))) return rc;
     if (!launch) return BLOND_OK;
-    const int smem = (int)sizeof(int) * q->S;
+    const int smem = tsm ? tsm : (int)sizeof(int) * q->S;
     const int grid = std::max(1, std::min(q->n_chunks, device_info().sm_count * q->blocks_per_sm));
     k<<<grid, q->threads, smem, s>>>(batch_args(q));
     BB_LAUNCH_CHECK();

@@ -112,7 +112,9 @@ __device__ __forceinline__ int q32_add(int q, double inc, const ParticleArgs& a)
 // Table sources of the induced kick: the global table the head wrote, or a
 // copy in shared memory (F64 / Q32P64: the induced voltage only, entries
 // formed per particle with lik_entry; F32P64: the float2 table itself).
-enum { TAB_GLOBAL = 0, TAB_SHARED = 1 };
+// TAB_ENTRIES: the table's own entries in shared memory (the batched pass
+// copies its beam's short table per chunk).
+enum { TAB_GLOBAL = 0, TAB_SHARED = 1, TAB_ENTRIES = 2 };
 
 // numpy.linspace midpoint k (linspace_centre) with the step precomputed.
 __device__ __forceinline__ double bin_centre(const ParticleArgs& a, int k) {
@@ -135,8 +137,8 @@ __device__ __forceinline__ typename TableEntry<PREC>::T table_at(const ParticleA
     using TB = typename TableEntry<PREC>::T;
     if constexpr (TAB == TAB_GLOBAL) {
         return __ldg(reinterpret_cast<const TB*>(a.table) + k);
-    } else if constexpr (PREC == PREC_F32P64) {
-        return reinterpret_cast<const float2*>(stab)[k];
+    } else if constexpr (TAB == TAB_ENTRIES || PREC == PREC_F32P64) {
+        return reinterpret_cast<const TB*>(stab)[k];
     } else {
         const double* V = reinterpret_cast<const double*>(stab);
         return lik_entry0(V[k], V[k + 1], bin_centre_inner(a, k), a.charge, a.lik_inv_w);
@@ -662,6 +664,10 @@ particle_kernel(const ParticleArgs a) {
 // prefetch ring; the block copies the table after the head has completed.
 __device__ __forceinline__ void copy16_async(void* smem, const void* gmem) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                     (uint32_t)__cvta_generic_to_shared(smem)), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void copy8_async(void* smem, const void* gmem) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(
                      (uint32_t)__cvta_generic_to_shared(smem)), "l"(gmem) : "memory");
 }
 
