@@ -31,7 +31,7 @@ S = 512
 COUNTS = [3000, 1, 32768 * 2 + 5, 777, 40001]
 
 
-def make_beam(k, n, turns):
+def make_beam(k, n, turns, S=S):
     """Beam k of a double-RF scan (h, 4h, V2/V1 = 0.1, phi2 = pi)."""
     rng = np.random.default_rng(100 + k)
     V1 = 2e6 + 5e6 * rng.random()
@@ -50,9 +50,12 @@ def make_beam(k, n, turns):
     return ring, rf, beam, prof, tiv, iv, (dt, dE)
 
 
-def test_batch_matches_oracle_and_single_beam_engine(cuda):
+@pytest.mark.parametrize("S", [512, 4096])
+def test_batch_matches_oracle_and_single_beam_engine(cuda, S):
+    """512 slices: each chunk copies its beam's table into shared memory;
+    4096: the table is gathered from global memory."""
     turns = 5
-    built = [make_beam(k, n, turns) for k, n in enumerate(COUNTS)]
+    built = [make_beam(k, n, turns, S) for k, n in enumerate(COUNTS)]
     batch = BatchTracker([(RingAndRFTracker(rf, beam), prof, tiv)
                           for _, rf, beam, prof, tiv, _, _ in built],
                          precision="f64", turns_per_graph=2)
@@ -71,7 +74,7 @@ def test_batch_matches_oracle_and_single_beam_engine(cuda):
         assert normwise(vind[b], ovind[-1]) < 1e-10
     # the same beams one by one through the single-beam engine
     for b, n in enumerate(COUNTS):
-        ring, rf, beam, p, tiv, iv, _ = make_beam(b, n, turns)
+        ring, rf, beam, p, tiv, iv, _ = make_beam(b, n, turns, S)
         f = FusedTracker(RingAndRFTracker(rf, beam), p, tiv, precision="f64",
                          turns_per_graph=2)
         f.track(turns)
