@@ -341,8 +341,11 @@ __device__ __forceinline__ void warp_fft(double2* a, int B, const double2* __res
 }
 
 // B transforms of length L, interleaved, starting in a[]; returns the buffer
-// (a or b) that holds the result.  Ends with __syncthreads().
-__device__ double2* batch_fft(double2* a, double2* b, int L, int B, const int* radices,
+// (a or b) that holds the result.  Ends with __syncthreads().  Not inlined:
+// the head calls it six times, and six inlined copies made the kernel's code
+// about 700 KB, whose instruction fetches were the head's top stall.
+__device__ __noinline__ double2* batch_fft(double2* a, double2* b, int L, int B,
+                                           const int* radices,
                               int npass, const double2* tw, bool inverse) {
     switch (L) {
         case 32: warp_fft<1>(a, B, tw, inverse, 5); return a;
@@ -570,8 +573,9 @@ spectral_kernel(const SpecParams P, const typename SpecLoopArg<FB>::type LP) {
         // ---- column transforms (length M1 over n1, Bc of them)
         double2* r1 = batch_fft(buf[0], buf[1], M1, Bc, p.r1, p.n1, tw1, false);
         double2* f1 = r1 == buf[0] ? buf[1] : buf[0];
-        cluster.sync();  // (A) every CTA's columns done
         BB_PHASE(4);
+        cluster.sync();  // (A) every CTA's columns done
+        BB_PHASE(5);
         // ---- transpose into rows with the four-step twiddle W_M^(n2 k1),
         // written to a buffer nobody reads remotely
         for (int e = tid; e < Br * M2; e += nth) {
@@ -588,16 +592,18 @@ spectral_kernel(const SpecParams P, const typename SpecLoopArg<FB>::type LP) {
         // CTAs may still read it
         if (three) {
             __syncthreads();
+            BB_PHASE(6);
             rows = batch_fft(f1, buf[2], M2, Br, p.r2, p.n2, tw2, false);
             spare = rows == f1 ? buf[2] : f1;
             spare2 = r1;
+            BB_PHASE(7);
         } else {
             cluster.sync();
             rows = batch_fft(f1, r1, M2, Br, p.r2, p.n2, tw2, false);
             spare = rows == f1 ? r1 : f1;
         }
         cluster.sync();  // (C) Z complete everywhere
-        BB_PHASE(5);
+        BB_PHASE(8);
     } else {
         wait_twiddles();
         __syncthreads();  // twiddle tables
@@ -606,7 +612,7 @@ spectral_kernel(const SpecParams P, const typename SpecLoopArg<FB>::type LP) {
     }
 
     if (p.prefetch) asm volatile("cp.async.wait_group 0;" ::: "memory");
-    BB_PHASE(6);
+    BB_PHASE(9);
 
     double2* ubuf = nullptr;
     if (P.mode & (SPEC_OUT_SPECTRUM | SPEC_MULTIPLY | SPEC_IN_SPECTRUM)) {
@@ -668,6 +674,7 @@ spectral_kernel(const SpecParams P, const typename SpecLoopArg<FB>::type LP) {
             }
         }
     }
+    BB_PHASE(10);
     if (!inverse) {
         cluster.sync();  // partners' reads of `rows` done before this CTA exits
         return;
@@ -683,13 +690,14 @@ spectral_kernel(const SpecParams P, const typename SpecLoopArg<FB>::type LP) {
         __syncthreads();
         rres = batch_fft(ubuf, other, M2, Br, p.r2, p.n2, tw2, true);
         rfree = rres == ubuf ? other : ubuf;
+        BB_PHASE(11);
     } else {
         cluster.sync();
         rres = batch_fft(ubuf, rows, M2, Br, p.r2, p.n2, tw2, true);
         rfree = rres == ubuf ? rows : ubuf;
     }
     cluster.sync();  // (E) every CTA's rows done
-    BB_PHASE(7);
+    BB_PHASE(12);
     // ---- transpose into columns with the conjugate four-step twiddle
     double2* cdst = (three && rows) ? rows : rfree;  // rows is free after (E)
     for (int e = tid; e < Bc * M1; e += nth) {
@@ -711,7 +719,7 @@ spectral_kernel(const SpecParams P, const typename SpecLoopArg<FB>::type LP) {
         cres = batch_fft(cdst, rres, M1, Bc, p.r1, p.n1, tw1, true);
     }
 
-    BB_PHASE(8);
+    BB_PHASE(13);
     // ---- real output y[2m], y[2m+1] with m = c Bc + b + M2 m1
     const int64_t S = P.n_in;
     auto value = [&](int64_t n, double y) {
@@ -747,7 +755,7 @@ spectral_kernel(const SpecParams P, const typename SpecLoopArg<FB>::type LP) {
     // (G) the neighbour values have landed, and every CTA has finished
     // reading the others' `rres` -- no CTA may exit before that
     cluster.sync();
-    BB_PHASE(9);
+    BB_PHASE(14);
     if (!g_table && !P.bump_turn) return;
     if (g_table) {
         const int64_t nt = P.n_out - 1;
@@ -813,7 +821,7 @@ spectral_kernel(const SpecParams P, const typename SpecLoopArg<FB>::type LP) {
         }
     }
     if (P.bump_turn && beam == 0 && c == 0 && tid == 0) *P.turn = turn + 1;
-    BB_PHASE(10);
+    BB_PHASE(15);
 }
 
 #endif  // BB_SPECTRAL_KERNELS
