@@ -124,6 +124,14 @@ _EXTRA = {
                                     c_int, c_dbl, c_dbl, c_ptr, c_ptr, c_ptr],
     "blond_adjoint_spectral": [c_int, c_ptr, c_int, c_ptr, c_i64, c_dbl, c_ptr, c_ptr,
                                c_ptr, c_ptr],
+    "blond_adjoint_forward_run": [c_int, c_ptr, c_ptr, c_i64, c_int, c_i64, c_ptr, c_ptr,
+                                  c_ptr, c_ptr, c_ptr, c_dbl, c_ptr, c_i64, c_dbl, c_ptr,
+                                  c_ptr, c_ptr, c_int, c_dbl, c_dbl, c_int, c_ptr, c_ptr,
+                                  c_ptr],
+    "blond_adjoint_backward_run": [c_int, c_i64, c_int, c_i64, c_ptr, c_ptr, c_ptr, c_ptr,
+                                   c_ptr, c_dbl, c_ptr, c_i64, c_dbl, c_ptr, c_ptr, c_int,
+                                   c_dbl, c_dbl, c_int, c_ptr, c_ptr, c_ptr, c_ptr, c_ptr,
+                                   c_ptr, c_ptr, c_ptr, c_ptr, c_ptr, c_ptr, c_ptr],
     "blond_engine_set_feedback": [c_ptr, c_int, c_int, c_dbl, c_dbl, c_dbl, c_int, c_dbl,
                                   c_dbl, c_dbl, c_int, c_ptr, c_ptr, c_int, c_ptr],
     "blond_engine_get_feedback": [c_ptr, c_ptr, c_ptr, c_ptr, c_ptr, c_ptr],

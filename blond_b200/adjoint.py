@@ -115,6 +115,9 @@ class AdjointTracker:
                         * np.asarray(rf.eta_0, float)[nx]
                         / (np.asarray(rf.beta, float)[nx] ** 2
                            * np.asarray(rf.energy, float)[nx])).tolist()
+        # host copies for the C turn loops
+        self._acc_h = (ct.c_double * self.T)(*self.acc)
+        self._drift_h = (ct.c_double * self.T)(*self.drift_c)
         _lib.load()
 
     # ------------------------------------------------------------ helpers
@@ -177,17 +180,20 @@ class _AdjointMap(torch.autograd.Function):
         vind = torch.empty(tr.T, tr.S, dtype=torch.float64, device=dev) if has_z else None
         spec = torch.empty(tr.T, M1, dtype=torch.complex128, device=dev) if has_z else None
         prof = torch.zeros(tr.T + 1, tr.S, dtype=torch.float64, device=dev)
-        _lib.call("blond_adjoint_deposit", _p(dt), tr.n, tr.S, tr.bc0, tr.inv_w,
-                  _p(prof[0]), _stream())
-        ckpt = []
+        nseg = (tr.T + tr.K - 1) // tr.K
+        ckpt_dt = torch.empty(nseg, tr.n, dtype=torch.float64, device=dev)
+        ckpt_dE = torch.empty(nseg, tr.n, dtype=edt, device=dev)
         Zr = _real_view(Zd) if has_z else None
-        for t in range(tr.T):
-            if t % tr.K == 0:
-                ckpt.append((dt.clone(), dE.clone()))
-            if has_z:
-                tr._spectral(0, prof[t], Zr, vind[t], _real_view(spec[t]))
-            tr._forward_turn(t, dt, dE, dt, dE, V, P, vind[t] if has_z else None,
-                             prof[t + 1])
+        # the turn loop runs in C (blond_adjoint_forward_run): the turn-0
+        # profile, then per turn checkpoints, induced voltage and spectrum,
+        # forward turn and profile
+        _lib.call("blond_adjoint_forward_run", PREC[tr.precision], _p(dt), _p(dE), tr.n,
+                  tr.n_rf, tr.T, _p(V), _p(tr.omega), _p(P),
+                  ct.cast(tr._acc_h, ct.c_void_p), ct.cast(tr._drift_h, ct.c_void_p),
+                  tr.charge, _p(Zr), tr.n_fft, tr.scale, _p(vind),
+                  _p(_real_view(spec) if has_z else None), _p(prof), tr.S, tr.bc0, tr.inv_w,
+                  tr.K, _p(ckpt_dt), _p(ckpt_dE), _stream())
+        ckpt = (ckpt_dt, ckpt_dE)
         ctx.tr = tr
         ctx.saved = (V, P, Zd, vind, spec, ckpt)
         ctx.edt = (dt0.dtype, dE0.dtype)
@@ -214,33 +220,19 @@ class _AdjointMap(torch.autograd.Function):
         lam_v = torch.zeros(T, S, dtype=torch.float64, device=dev) if has_z else None
         lam_pt = torch.empty(T, S, dtype=torch.float64, device=dev) if has_z else None
         states = torch.empty(K + 1, n, dtype=torch.float64, device=dev)
-        nseg = len(ckpt)
-        stream = _stream()
-        for seg in reversed(range(nseg)):
-            a, b = seg * K, min(T, (seg + 1) * K)
-            dt_a, dE_a = ckpt[seg]
-            states[0].copy_(dt_a)
-            dE = dE_a.clone()
-            for t in range(a, b):
-                tr._forward_turn(t, states[t - a], dE, states[t - a + 1], dE, V, P,
-                                 vind[t] if has_z else None, None)
-            for t in range(b - 1, a - 1, -1):
-                _lib.call("blond_adjoint_backward_turn", _p(states[t - a]),
-                          _p(states[t - a + 1]), n, _p(lam_dt), _p(lam_dE), _p(lam_p), 1,
-                          tr.n_rf, _p(V[t]), _p(tr.omega[t]), _p(P[t]), tr.charge,
-                          tr.drift_c[t], _p(vind[t] if has_z else None), S, tr.bc0,
-                          tr.inv_w, _p(lam_v[t] if has_z else None), _p(grad_rf[t]), stream)
-                if has_z:
-                    tr._spectral(1, lam_v[t], Zc, lam_pt[t], _real_view(spec[t]),
-                                 _real_view(G))
-                    lam_p = lam_pt[t]
-                else:
-                    lam_p = None
-        if lam_p is not None:
-            # the turn-0 profile is a deposit of the initial dt
-            _lib.call("blond_adjoint_backward_turn", None, _p(ckpt[0][0]), n, _p(lam_dt),
-                      _p(lam_dE), _p(lam_p), 0, tr.n_rf, None, None, None, tr.charge, 0.0,
-                      None, S, tr.bc0, tr.inv_w, None, None, stream)
+        ckpt_dt, ckpt_dE = ckpt
+        dE_work = torch.empty_like(ckpt_dE[0])
+        # the backward sweep runs in C (blond_adjoint_backward_run): per
+        # segment the recomputed turn-start coordinates, then the backward
+        # turns and the transposed induced-voltage transform, last the
+        # deposit adjoint of the turn-0 profile
+        _lib.call("blond_adjoint_backward_run", PREC[tr.precision], n, tr.n_rf, T, _p(V),
+                  _p(tr.omega), _p(P), ct.cast(tr._acc_h, ct.c_void_p),
+                  ct.cast(tr._drift_h, ct.c_void_p), tr.charge, _p(Zc), tr.n_fft, tr.scale,
+                  _p(vind), _p(_real_view(spec) if has_z else None), S, tr.bc0, tr.inv_w, K,
+                  _p(ckpt_dt), _p(ckpt_dE), _p(states), _p(dE_work), _p(lam_dt), _p(lam_dE),
+                  _p(lam_p), _p(lam_v), _p(lam_pt), _p(grad_rf),
+                  _p(_real_view(G) if has_z else None), _stream())
         grad_V = grad_rf[:, :tr.n_rf].contiguous()
         grad_phi = grad_rf[:, tr.n_rf:].contiguous()
         grad_Z = None

@@ -469,3 +469,183 @@ int blond_adjoint_spectral(int mode, const double* x, int n_slices, const double
 }
 
 }  // extern "C"
+
+namespace bb {
+
+// The induced-voltage transform of the turn loops below: one plan and one
+// twiddle table for the whole run (the per-turn entry point builds the plan
+// on the host and the twiddles in the kernel at every call).
+struct AdjSpectral {
+    SpecPlan plan = {};
+    double2* tw = nullptr;
+    ~AdjSpectral() {
+        if (tw) cudaFree(tw);
+    }
+    int init(int64_t n_fft) {
+        if (!make_spec_plan(n_fft, plan)) {
+            set_error("adjoint run: n_fft=%lld is not an even 5-smooth length <= %lld",
+                      (long long)n_fft, (long long)kMaxClusterFFT);
+            return BLOND_ERR_UNSUPPORTED;
+        }
+        int rc;
+        if ((rc = prepare_spectral())) return rc;
+        return make_spec_twiddles(plan, &tw);
+    }
+    // the same transform as blond_adjoint_spectral(mode, ...)
+    int run(int mode, const double* x, int S, const double* H, double scale, double* y,
+            double* spectrum, double* accum, cudaStream_t s) const {
+        SpecParams P = {};
+        P.p = plan;
+        P.twg = tw;
+        P.mode = SPEC_FORWARD | SPEC_MULTIPLY | SPEC_INVERSE;
+        P.in_f64 = x;
+        P.n_in = S;
+        P.H = reinterpret_cast<const double2*>(H);
+        P.out = y;
+        P.n_out = S < plan.N ? S : plan.N;
+        P.out_scale = -scale / (double)plan.M;
+        if (mode == 0 && spectrum) {
+            P.mode |= SPEC_OUT_SPECTRUM;
+            P.spec_out = reinterpret_cast<double2*>(spectrum);
+        }
+        if (mode == 1) {
+            P.mode |= SPEC_ACCUM;
+            P.acc_a = reinterpret_cast<const double2*>(spectrum);
+            P.acc_g = reinterpret_cast<double2*>(accum);
+        }
+        return launch_spectral(P, s);
+    }
+};
+
+}  // namespace bb
+
+extern "C" {
+
+int blond_adjoint_forward_run(int precision, double* dt, void* dE, int64_t n, int n_rf,
+                              int64_t n_turns, const double* voltage, const double* omega_rf,
+                              const double* phi_rf, const double* acc_kick,
+                              const double* drift_coeff, double charge,
+                              const double* impedance, int64_t n_fft, double scale,
+                              double* induced_voltage, double* spectrum, double* profile,
+                              int n_slices, double bin_center0, double inv_bin_width,
+                              int checkpoint_every, double* ckpt_dt, void* ckpt_dE,
+                              void* stream) {
+    BB_CHECK_ARG(precision == BLOND_PREC_F64 || precision == BLOND_PREC_F32P64,
+                 "adjoint_forward_run: precision must be F64 or F32P64");
+    BB_CHECK_ARG(n >= 1 && n_turns >= 1 && n_slices >= 2 && checkpoint_every >= 1,
+                 "adjoint_forward_run: bad size");
+    BB_CHECK_ARG(dt && dE && voltage && omega_rf && phi_rf && acc_kick && drift_coeff &&
+                     profile && ckpt_dt && ckpt_dE,
+                 "adjoint_forward_run: null pointer");
+    BB_CHECK_ARG(!impedance || (induced_voltage && spectrum),
+                 "adjoint_forward_run: an impedance needs the induced-voltage and spectrum "
+                 "arrays");
+    cudaStream_t s = as_stream(stream);
+    const size_t esz = precision == BLOND_PREC_F64 ? sizeof(double) : sizeof(float);
+    const int64_t M1 = n_fft / 2 + 1;
+    AdjSpectral sp;
+    int rc;
+    if (impedance && (rc = sp.init(n_fft))) return rc;
+    if ((rc = blond_adjoint_deposit(dt, n, n_slices, bin_center0, inv_bin_width, profile,
+                                    stream)))
+        return rc;
+    for (int64_t t = 0; t < n_turns; ++t) {
+        if (t % checkpoint_every == 0) {
+            const int64_t seg = t / checkpoint_every;
+            BB_CUDA(cudaMemcpyAsync(ckpt_dt + seg * n, dt, sizeof(double) * n,
+                                    cudaMemcpyDeviceToDevice, s));
+            BB_CUDA(cudaMemcpyAsync(static_cast<char*>(ckpt_dE) + (size_t)seg * n * esz, dE,
+                                    esz * n, cudaMemcpyDeviceToDevice, s));
+        }
+        double* vind = impedance ? induced_voltage + t * n_slices : nullptr;
+        if (impedance &&
+            (rc = sp.run(0, profile + t * n_slices, n_slices, impedance, scale, vind,
+                         spectrum + t * M1 * 2, nullptr, s)))
+            return rc;
+        if ((rc = blond_adjoint_forward_turn(
+                 precision, dt, dE, dt, dE, n, n_rf, voltage + t * n_rf, omega_rf + t * n_rf,
+                 phi_rf + t * n_rf, acc_kick[t], charge, drift_coeff[t], vind, n_slices,
+                 bin_center0, inv_bin_width, profile + (t + 1) * n_slices, stream)))
+            return rc;
+    }
+    return BLOND_OK;
+}
+
+int blond_adjoint_backward_run(int precision, int64_t n, int n_rf, int64_t n_turns,
+                               const double* voltage, const double* omega_rf,
+                               const double* phi_rf, const double* acc_kick,
+                               const double* drift_coeff, double charge,
+                               const double* impedance_conj, int64_t n_fft, double scale,
+                               const double* induced_voltage, const double* spectrum,
+                               int n_slices, double bin_center0, double inv_bin_width,
+                               int checkpoint_every, const double* ckpt_dt,
+                               const void* ckpt_dE, double* states, void* dE_work,
+                               double* lam_dt, double* lam_dE, const double* lam_p_final,
+                               double* lam_v, double* lam_pt, double* grad_rf,
+                               double* spectrum_accum, void* stream) {
+    BB_CHECK_ARG(precision == BLOND_PREC_F64 || precision == BLOND_PREC_F32P64,
+                 "adjoint_backward_run: precision must be F64 or F32P64");
+    BB_CHECK_ARG(n >= 1 && n_turns >= 1 && n_slices >= 2 && checkpoint_every >= 1,
+                 "adjoint_backward_run: bad size");
+    BB_CHECK_ARG(voltage && omega_rf && phi_rf && acc_kick && drift_coeff && ckpt_dt &&
+                     ckpt_dE && states && dE_work && lam_dt && lam_dE && grad_rf,
+                 "adjoint_backward_run: null pointer");
+    BB_CHECK_ARG(!impedance_conj || (induced_voltage && spectrum && lam_v && lam_pt &&
+                                     spectrum_accum),
+                 "adjoint_backward_run: an impedance needs the stored induced voltages and "
+                 "spectra and the adjoint arrays");
+    cudaStream_t s = as_stream(stream);
+    const size_t esz = precision == BLOND_PREC_F64 ? sizeof(double) : sizeof(float);
+    const int64_t M1 = n_fft / 2 + 1;
+    const int64_t K = checkpoint_every;
+    const int64_t nseg = (n_turns + K - 1) / K;
+    const bool has_z = impedance_conj != nullptr;
+    AdjSpectral sp;
+    int rc;
+    if (has_z && (rc = sp.init(n_fft))) return rc;
+    const double* lam_p = lam_p_final;
+    for (int64_t seg = nseg - 1; seg >= 0; --seg) {
+        const int64_t a = seg * K, b = std::min(n_turns, (seg + 1) * K);
+        // the segment's turn-start coordinates, recomputed from its checkpoint
+        BB_CUDA(cudaMemcpyAsync(states, ckpt_dt + seg * n, sizeof(double) * n,
+                                cudaMemcpyDeviceToDevice, s));
+        BB_CUDA(cudaMemcpyAsync(dE_work, static_cast<const char*>(ckpt_dE) + (size_t)seg * n * esz,
+                                esz * n, cudaMemcpyDeviceToDevice, s));
+        for (int64_t t = a; t < b; ++t) {
+            if ((rc = blond_adjoint_forward_turn(
+                     precision, states + (t - a) * n, dE_work, states + (t - a + 1) * n,
+                     dE_work, n, n_rf, voltage + t * n_rf, omega_rf + t * n_rf,
+                     phi_rf + t * n_rf, acc_kick[t], charge, drift_coeff[t],
+                     has_z ? induced_voltage + t * n_slices : nullptr, n_slices, bin_center0,
+                     inv_bin_width, nullptr, stream)))
+                return rc;
+        }
+        for (int64_t t = b - 1; t >= a; --t) {
+            if ((rc = blond_adjoint_backward_turn(
+                     states + (t - a) * n, states + (t - a + 1) * n, n, lam_dt, lam_dE, lam_p, 1,
+                     n_rf, voltage + t * n_rf, omega_rf + t * n_rf, phi_rf + t * n_rf, charge,
+                     drift_coeff[t], has_z ? induced_voltage + t * n_slices : nullptr,
+                     n_slices, bin_center0, inv_bin_width,
+                     has_z ? lam_v + t * n_slices : nullptr, grad_rf + t * 2 * n_rf, stream)))
+                return rc;
+            if (has_z) {
+                if ((rc = sp.run(1, lam_v + t * n_slices, n_slices, impedance_conj, scale,
+                                 lam_pt + t * n_slices, const_cast<double*>(spectrum) + t * M1 * 2,
+                                 spectrum_accum, s)))
+                    return rc;
+                lam_p = lam_pt + t * n_slices;
+            } else {
+                lam_p = nullptr;
+            }
+        }
+    }
+    // the turn-0 profile is a deposit of the initial dt
+    if (lam_p)
+        return blond_adjoint_backward_turn(nullptr, ckpt_dt, n, lam_dt, lam_dE, lam_p, 0, n_rf,
+                                           nullptr, nullptr, nullptr, charge, 0.0, nullptr,
+                                           n_slices, bin_center0, inv_bin_width, nullptr,
+                                           nullptr, stream);
+    return BLOND_OK;
+}
+
+}  // extern "C"

@@ -340,19 +340,27 @@ __device__ __forceinline__ void warp_fft(double2* a, int B, const double2* __res
     __syncthreads();
 }
 
-// B transforms of length L, interleaved, starting in a[]; returns the buffer
-// (a or b) that holds the result.  Ends with __syncthreads().  Not inlined:
-// the head calls it six times, and six inlined copies made the kernel's code
-// about 700 KB, whose instruction fetches were the head's top stall.
-__device__ __noinline__ double2* batch_fft(double2* a, double2* b, int L, int B,
-                                           const int* radices,
-                              int npass, const double2* tw, bool inverse) {
+// The register transforms of lengths 32 .. 256 in place.  Not inlined: the
+// head calls the transform batch six times, and six inlined copies of these
+// made the kernel's code about 700 KB, whose instruction fetches were the
+// head's top stall.
+__device__ __noinline__ void warp_fft_any(double2* a, int L, int B, const double2* tw,
+                                          bool inverse) {
     switch (L) {
-        case 32: warp_fft<1>(a, B, tw, inverse, 5); return a;
-        case 64: warp_fft<2>(a, B, tw, inverse, 6); return a;
-        case 128: warp_fft<4>(a, B, tw, inverse, 7); return a;
-        case 256: warp_fft<8>(a, B, tw, inverse, 8); return a;
-        default: break;
+        case 32: warp_fft<1>(a, B, tw, inverse, 5); return;
+        case 64: warp_fft<2>(a, B, tw, inverse, 6); return;
+        case 128: warp_fft<4>(a, B, tw, inverse, 7); return;
+        default: warp_fft<8>(a, B, tw, inverse, 8); return;
+    }
+}
+
+// B transforms of length L, interleaved, starting in a[]; returns the buffer
+// (a or b) that holds the result.  Ends with __syncthreads().
+__device__ double2* batch_fft(double2* a, double2* b, int L, int B, const int* radices,
+                              int npass, const double2* tw, bool inverse) {
+    if (L == 32 || L == 64 || L == 128 || L == 256) {
+        warp_fft_any(a, L, B, tw, inverse);
+        return a;
     }
     const double s = inverse ? 1.0 : -1.0;
     const int lgB = (B & (B - 1)) == 0 ? __ffs(B) - 1 : -1;

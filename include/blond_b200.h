@@ -631,6 +631,42 @@ int blond_adjoint_backward_turn(const double* dt, const double* dt_next, int64_t
 int blond_adjoint_spectral(int mode, const double* x, int n_slices, const double* impedance,
                            int64_t n_fft, double scale, double* y, double* spectrum,
                            double* accum, void* stream);
+/* The forward map's turn loop in one call: profile[0] = deposit of dt, then
+ * for t < n_turns: every checkpoint_every turns a copy of (dt, dE) into row
+ * t / checkpoint_every of ckpt_dt / ckpt_dE; with an impedance (n_fft/2+1
+ * complex, or NULL) induced_voltage[t] and spectrum[t] from profile[t]
+ * (mode 0 above); one forward turn into profile[t + 1].  voltage, omega_rf,
+ * phi_rf: device [n_turns][n_rf]; acc_kick, drift_coeff: HOST [n_turns];
+ * profile: device [n_turns + 1][n_slices], zeros on entry. */
+int blond_adjoint_forward_run(int precision, double* dt, void* dE, int64_t n, int n_rf,
+                              int64_t n_turns, const double* voltage, const double* omega_rf,
+                              const double* phi_rf, const double* acc_kick,
+                              const double* drift_coeff, double charge,
+                              const double* impedance, int64_t n_fft, double scale,
+                              double* induced_voltage, double* spectrum, double* profile,
+                              int n_slices, double bin_center0, double inv_bin_width,
+                              int checkpoint_every, double* ckpt_dt, void* ckpt_dE,
+                              void* stream);
+/* The backward sweep in one call: segment by segment from the last, the
+ * segment's turn-start dt recomputed from its checkpoint into states
+ * ([checkpoint_every + 1][n]; dE_work [n] holds the energies), then the
+ * backward turns (with an impedance, conj(Z) as impedance_conj: lam_v[t]
+ * through mode 1 above into lam_pt[t], accumulating spectrum_accum), and
+ * last the deposit adjoint of the turn-0 profile.  lam_p_final: dL/d(final
+ * profile) or NULL.  On exit lam_dt / lam_dE hold dL/d(initial dt, dE),
+ * grad_rf[t] = {dL/dV_j, dL/dphi_j}. */
+int blond_adjoint_backward_run(int precision, int64_t n, int n_rf, int64_t n_turns,
+                               const double* voltage, const double* omega_rf,
+                               const double* phi_rf, const double* acc_kick,
+                               const double* drift_coeff, double charge,
+                               const double* impedance_conj, int64_t n_fft, double scale,
+                               const double* induced_voltage, const double* spectrum,
+                               int n_slices, double bin_center0, double inv_bin_width,
+                               int checkpoint_every, const double* ckpt_dt,
+                               const void* ckpt_dE, double* states, void* dE_work,
+                               double* lam_dt, double* lam_dE, const double* lam_p_final,
+                               double* lam_v, double* lam_pt, double* grad_rf,
+                               double* spectrum_accum, void* stream);
 
 #ifdef __cplusplus
 }
