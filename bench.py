@@ -74,6 +74,9 @@ def parse():
     ap.add_argument("--threads", type=int, default=1024)
     ap.add_argument("--blocks-per-sm", type=int, default=1)
     ap.add_argument("--prefetch", type=int, default=2, choices=[0, 2, 4])
+    ap.add_argument("--c5-forms", default="q32p64,f32p64,f64,control",
+                    help="c5: the forms to run (comma list of q32p64, f32p64, f64, control); "
+                         "q32p64 gives the line's value")
     return ap.parse_args()
 
 
@@ -797,7 +800,7 @@ C5_WORKLOAD = ("1e8 protons 26 GeV/c, double RF h=4620/18480 4.5/0.45 MV (phi 0/
                "Q 100/1000/3000/30000) + inductive Im(Z)/n 0.1 Ohm, intensity 1e11")
 
 
-def build_c5(n, n_turns, precision, seed=0):
+def build_c5(n, n_turns, precision, seed=0, shape=None, kernel="auto"):
     """The C5 pipeline: a long profile (2^16 slices, histogram deposited
     straight into global memory) and a sum of five impedance sources."""
     import torch
@@ -821,8 +824,16 @@ def build_c5(n, n_turns, precision, seed=0):
                                                     [100.0, 1000.0, 3000.0, 30000.0])])
     ind = InductiveImpedance(beam, prof, [0.1] * (n_turns + 1), rf)
     tiv = TotalInducedVoltage(beam, prof, [iv, ind])
-    fused = FusedTracker(RingAndRFTracker(rf, beam), prof, tiv, precision=precision,
-                         turns_per_graph=50)
+    if shape is None:
+        fused = FusedTracker(RingAndRFTracker(rf, beam), prof, tiv, precision=precision,
+                             turns_per_graph=50)
+    else:
+        threads, bps, ring_stages = shape
+        fused = FusedTracker(RingAndRFTracker(rf, beam), prof, tiv, precision=precision,
+                             turns_per_graph=50, kernel="packed" if kernel == "auto" else kernel,
+                             threads=threads, blocks_per_sm=bps, tune="fixed")
+        fused.eng.call("set_prefetch", ring_stages)
+        fused.eng.call("set_overlap", 0)  # what the autotuner picks at 2^16 slices
     return fused, beam, prof, iv.n_fft
 
 
@@ -836,9 +847,15 @@ def run_c5(args):
     n = int(args.particles) if args.particles != 1e7 else int(1e8)
     res, coords = {}, {}
     peak = _peaks().get("hbm_gbs") or 6650.0
+    shape = ((args.threads, args.blocks_per_sm, args.prefetch) if args.tune == "fixed"
+             else None)
+    forms = args.c5_forms.split(",")
     for prec, shift in (("q32p64", 0.0), ("f32p64", 0.0), ("f64", 0.0), ("f64", 0.01)):
         key = prec if not shift else "control_fp64_dE_plus_0.01eV"
-        fused, beam, prof, n_fft = build_c5(n, W + K + kt + 4, prec)
+        if (key if not shift else "control") not in forms:
+            continue
+        fused, beam, prof, n_fft = build_c5(n, W + K + kt + 4, prec, shape=shape,
+                                            kernel=args.kernel)
         if shift:
             fused.dE.add_(shift)
             fused.eng.call("slice", ct_stream())
@@ -862,6 +879,8 @@ def run_c5(args):
         torch.cuda.empty_cache()
 
     def err(key):
+        if key not in coords or "f64" not in coords:
+            return None
         return {"sigma_dt": abs(coords[key][0] / coords["f64"][0] - 1),
                 "sigma_dE": abs(coords[key][1] / coords["f64"][1] - 1)}
     r = res["q32p64"]
@@ -882,7 +901,7 @@ def run_c5(args):
                      "autotuned": r["autotuned"]},
         **{p: {k: res[p][k] for k in ("value", "ms_per_step", "kernel_ms", "head_kernel_ms",
                                       "achieved_gbs", "frac", "kernel")}
-           for p in ("f32p64", "f64")},
+           for p in ("f32p64", "f64") if p in res},
         "rel_err_after_turns": {
             "turns": W + K, "statistic": "in-window rms of dt and dE vs FP64",
             "q32p64": err("q32p64"), "f32p64": err("f32p64"),
