@@ -500,7 +500,8 @@ def _peaks():
 def _traffic(precision, n, kernel="plain"):
     """DRAM bytes per launch of the particle kernel from the committed ncu
     summary of that kernel (scaled to n particles), or None."""
-    name = {"stab": "particle_kernel_stab_c2.txt", "plain": "particle_kernel_c2.txt"}.get(kernel)
+    name = {"stab": "particle_kernel_stab_c2.txt", "plain": "particle_kernel_c2.txt",
+            "packed": "particle_kernel_packed_c5_q32.txt"}.get(kernel)
     if precision == "q32p64" and kernel == "plain":
         name = "particle_kernel_q32_c2.txt"
     if name is None:
@@ -892,7 +893,8 @@ def run_c5(args):
         "config": {"workload": C5_WORKLOAD, "particles": n, "slices": 65536,
                    "n_fft": n_fft, "l2": "inputs larger than L2"},
         "roofline": {"bound": "hbm", "achieved": r["achieved_gbs"], "peak": peak,
-                     "unit": "GB/s", "frac": r["frac"], "traffic": None,
+                     "unit": "GB/s", "frac": r["frac"],
+                     "traffic": _traffic("q32p64", n, r["kernel"]),
                      "kernel": {"tma": "particle_kernel_tma", "stab": "particle_kernel_stab",
                                 "packed": "particle_kernel_stab<TAB_GLOBAL>"}
                                .get(r["kernel"], "particle_kernel"),
