@@ -480,6 +480,22 @@ spectral_kernel(const SpecParams P, const typename SpecLoopArg<FB>::type LP) {
     double* nbr = reinterpret_cast<double*>(sraw + lay.nbr);
     const bool three = p.nbuf == 3;
     const bool inverse = (P.mode & SPEC_INVERSE) != 0;
+    // Index arithmetic without runtime integer division where the factors
+    // are powers of two (every plan of a power-of-two n_fft): quotient and
+    // remainder by shift and mask.  L always is one.
+    const bool pw = (M1 & (M1 - 1)) == 0 && (M2 & (M2 - 1)) == 0 && (Bc & (Bc - 1)) == 0 &&
+                    (Br & (Br - 1)) == 0;
+    const int lgM1 = 31 - __clz(M1), lgM2 = 31 - __clz(M2);
+    const int lgBc = 31 - __clz(Bc), lgBr = 31 - __clz(Br), lgL = 31 - __clz(L);
+    auto qr = [&](int x, int d, int lg, int& q, int& r) {
+        if (pw) {
+            q = x >> lg;
+            r = x & (d - 1);
+        } else {
+            q = x / d;
+            r = x - q * d;
+        }
+    };
 
     BB_PHASE(0);
     // ---- twiddle tables precomputed by the engine: copied asynchronously
@@ -494,14 +510,18 @@ spectral_kernel(const SpecParams P, const typename SpecLoopArg<FB>::type LP) {
     if (p.prefetch) {
         if (P.mode & SPEC_MULTIPLY) {
             for (int e = tid; e < per; e += nth) {
-                const int k = c * Br + e % Br + M1 * (e / Br);
+                int q, r;
+                qr(e, Br, lgBr, q, r);
+                const int k = c * Br + r + M1 * q;
                 cp_async16(&hk[e], &g_H[k]);
                 cp_async16(&hp[e], &g_H[k == 0 ? M : M - k]);
             }
         }
         if (inverse && g_table) {
             for (int e = tid; e < per; e += nth) {
-                const int64_t m = (int64_t)c * Bc + e % Bc + (int64_t)M2 * (e / Bc);
+                int q, r;
+                qr(e, Bc, lgBc, q, r);
+                const int64_t m = (int64_t)c * Bc + r + (int64_t)M2 * q;
                 if (2 * m < P.n_out - 1) cp_async8(&bcs[2 * e], &g_bc[2 * m]);
                 if (2 * m + 1 < P.n_out - 1) cp_async8(&bcs[2 * e + 1], &g_bc[2 * m + 1]);
             }
@@ -532,8 +552,9 @@ spectral_kernel(const SpecParams P, const typename SpecLoopArg<FB>::type LP) {
         }
     };
     // W_M^j and W_N^j (N = 2M) for 0 <= j < M from the two-level tables
-    auto twm = [&](long long j) { return cmul(tam[j / L], tbm[j % L]); };
-    auto twn = [&](long long j) { return cmul(tan_[j / L], tbn[j % L]); };
+    // (0 <= j < M: int arithmetic, L a power of two)
+    auto twm = [&](int j) { return cmul(tam[j >> lgL], tbm[j & (L - 1)]); };
+    auto twn = [&](int j) { return cmul(tan_[j >> lgL], tbn[j & (L - 1)]); };
 
     double2* rows = nullptr;   // row-phase buffer holding Z
     double2* spare = nullptr;  // buffers that no other CTA reads right now
@@ -544,7 +565,8 @@ spectral_kernel(const SpecParams P, const typename SpecLoopArg<FB>::type LP) {
         // ---- load: z[m] = x[2m] + i x[2m+1], m = c Bc + b + M2 n1
         const int64_t nlim = P.n_in < (int64_t)p.N ? P.n_in : (int64_t)p.N;
         for (int e = tid; e < per; e += nth) {
-            const int b = e % Bc, n1 = e / Bc;
+            int n1, b;
+            qr(e, Bc, lgBc, n1, b);
             const int64_t m = (int64_t)c * Bc + b + (int64_t)M2 * n1;
             double x0 = 0.0, x1 = 0.0;
             const int64_t i0 = 2 * m, i1 = 2 * m + 1;
@@ -587,12 +609,14 @@ spectral_kernel(const SpecParams P, const typename SpecLoopArg<FB>::type LP) {
         // ---- transpose into rows with the four-step twiddle W_M^(n2 k1),
         // written to a buffer nobody reads remotely
         for (int e = tid; e < Br * M2; e += nth) {
-            const int n2 = e % M2, br = e / M2;
+            int br, n2;
+            qr(e, M2, lgM2, br, n2);
             const int k1 = c * Br + br;
-            const int owner = n2 / Bc;
+            int owner, nl;
+            qr(n2, Bc, lgBc, owner, nl);
             const double2* remote = cluster.map_shared_rank(r1, owner);
-            double2 v = remote[k1 * Bc + (n2 - owner * Bc)];
-            const long long ex = ((long long)n2 * k1) % M;
+            double2 v = remote[k1 * Bc + nl];
+            const int ex = n2 * k1;  // < M1 M2 = M
             if (ex) v = cmul(v, twm(ex));
             f1[n2 * Br + br] = v;
         }
@@ -627,20 +651,23 @@ spectral_kernel(const SpecParams P, const typename SpecLoopArg<FB>::type LP) {
         // ---- spectral step on own k = k1 + M1 k2 with partner M - k
         ubuf = spare;
         for (int e = tid; e < per; e += nth) {
-            const int br = e % Br, k2 = e / Br;
+            int k2, br;
+            qr(e, Br, lgBr, k2, br);
             const int k1 = c * Br + br;
             const int k = k1 + M1 * k2;
-            const int pk = (M - k) % M;
+            const int pk = k == 0 ? 0 : M - k;
             double2 Yk, Yp;  // Y[k], Y[M-k] (Y[M] when k == 0)
             if (P.mode & SPEC_IN_SPECTRUM) {
                 const int64_t kk = k, kp = (k == 0) ? M : (M - k);
                 Yk = kk < P.n_spec_in ? P.spec_in[kk] : make_double2(0, 0);
                 Yp = kp < P.n_spec_in ? P.spec_in[kp] : make_double2(0, 0);
             } else {
-                const int p1 = pk % M1, p2 = pk / M1, owner = p1 / Br;
+                int p2, p1, owner, pl;
+                qr(pk, M1, lgM1, p2, p1);
+                qr(p1, Br, lgBr, owner, pl);
                 const double2* remote = cluster.map_shared_rank(rows, owner);
                 const double2 Zk = rows[k2 * Br + br];
-                const double2 Zp = remote[p2 * Br + (p1 - owner * Br)];
+                const double2 Zp = remote[p2 * Br + pl];
                 if (k == 0) {
                     Yk = make_double2(Zk.x + Zk.y, 0.0);  // X[0]
                     Yp = make_double2(Zk.x - Zk.y, 0.0);  // X[M]
@@ -709,12 +736,14 @@ spectral_kernel(const SpecParams P, const typename SpecLoopArg<FB>::type LP) {
     // ---- transpose into columns with the conjugate four-step twiddle
     double2* cdst = (three && rows) ? rows : rfree;  // rows is free after (E)
     for (int e = tid; e < Bc * M1; e += nth) {
-        const int k1 = e % M1, bcol = e / M1;
+        int bcol, k1;
+        qr(e, M1, lgM1, bcol, k1);
         const int m2 = c * Bc + bcol;
-        const int owner = k1 / Br;
+        int owner, kl;
+        qr(k1, Br, lgBr, owner, kl);
         const double2* remote = cluster.map_shared_rank(rres, owner);
-        double2 v = remote[m2 * Br + (k1 - owner * Br)];
-        const long long ex = ((long long)k1 * m2) % M;
+        double2 v = remote[m2 * Br + kl];
+        const int ex = k1 * m2;  // < M
         if (ex) v = cmul(v, cconj(twm(ex)));
         cdst[k1 * Bc + bcol] = v;
     }
@@ -744,7 +773,8 @@ spectral_kernel(const SpecParams P, const typename SpecLoopArg<FB>::type LP) {
         return v;
     };
     for (int e = tid; e < per; e += nth) {
-        const int b = e % Bc, m1 = e / Bc;
+        int m1, b;
+        qr(e, Bc, lgBc, m1, b);
         const int64_t m = (int64_t)c * Bc + b + (int64_t)M2 * m1;
         const double2 u = cres[m1 * Bc + b];
         const double v0 = value(2 * m, u.x), v1 = value(2 * m + 1, u.y);
@@ -768,7 +798,8 @@ spectral_kernel(const SpecParams P, const typename SpecLoopArg<FB>::type LP) {
     if (g_table) {
         const int64_t nt = P.n_out - 1;
         for (int e = tid; e < per; e += nth) {
-            const int b = e % Bc, m1 = e / Bc;
+            int m1, b;
+        qr(e, Bc, lgBc, m1, b);
             const int64_t m = (int64_t)c * Bc + b + (int64_t)M2 * m1;
             const double2 u = cres[m1 * Bc + b];
             const double v0 = vloc[e];
