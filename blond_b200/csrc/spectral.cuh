@@ -340,6 +340,39 @@ __device__ __forceinline__ void warp_fft(double2* a, int B, const double2* __res
     __syncthreads();
 }
 
+// B transforms of length G = 2, 4, 8 or 16 (interleaved as in warp_fft):
+// a group of G lanes per transform, one element per lane, 32 / G
+// transforms per warp; the butterflies of every span by shuffles inside the
+// group, radix-2 decimation in frequency, results to the bit-reversed
+// index.  Replaces the Stockham passes (a block barrier each) for the short
+// factors of small plans (512- and 1024-point transforms).  Ends with
+// __syncthreads().
+template <int G>
+__device__ __forceinline__ void subwarp_fft(double2* a, int B, const double2* __restrict__ tw,
+                                            bool inverse, int lgG) {
+    const int lane = threadIdx.x & 31, gl = lane & (G - 1), grp = lane / G;
+    const int tpw = 32 / G, nw = blockDim.x >> 5;
+    const double sg = inverse ? -1.0 : 1.0;
+    // b0 is the same for the whole warp, so every lane reaches the shuffles
+    for (int b0 = (threadIdx.x >> 5) * tpw; b0 < B; b0 += nw * tpw) {
+        const int b = b0 + grp;
+        const bool act = b < B;
+        double2 v = act ? a[gl * B + b] : make_double2(0.0, 0.0);
+#pragma unroll
+        for (int h = G / 2; h >= 1; h >>= 1) {
+            const bool upper = (gl & h) != 0;
+            double2 w = upper ? tw[(gl & (h - 1)) * (G / (2 * h))] : make_double2(1.0, 0.0);
+            w.y *= sg;
+            double2 q;
+            q.x = __shfl_xor_sync(0xffffffffu, v.x, h);
+            q.y = __shfl_xor_sync(0xffffffffu, v.y, h);
+            v = upper ? cmul(csub(q, v), w) : cadd(v, q);
+        }
+        if (act) a[(int)(__brev((unsigned)gl) >> (32 - lgG)) * B + b] = v;
+    }
+    __syncthreads();
+}
+
 // The register transforms of lengths 32 .. 256 in place.  Not inlined: the
 // head calls the transform batch six times, and six inlined copies of these
 // made the kernel's code about 700 KB, whose instruction fetches were the
@@ -347,6 +380,10 @@ __device__ __forceinline__ void warp_fft(double2* a, int B, const double2* __res
 __device__ __noinline__ void warp_fft_any(double2* a, int L, int B, const double2* tw,
                                           bool inverse) {
     switch (L) {
+        case 2: subwarp_fft<2>(a, B, tw, inverse, 1); return;
+        case 4: subwarp_fft<4>(a, B, tw, inverse, 2); return;
+        case 8: subwarp_fft<8>(a, B, tw, inverse, 3); return;
+        case 16: subwarp_fft<16>(a, B, tw, inverse, 4); return;
         case 32: warp_fft<1>(a, B, tw, inverse, 5); return;
         case 64: warp_fft<2>(a, B, tw, inverse, 6); return;
         case 128: warp_fft<4>(a, B, tw, inverse, 7); return;
@@ -358,7 +395,7 @@ __device__ __noinline__ void warp_fft_any(double2* a, int L, int B, const double
 // (a or b) that holds the result.  Ends with __syncthreads().
 __device__ double2* batch_fft(double2* a, double2* b, int L, int B, const int* radices,
                               int npass, const double2* tw, bool inverse) {
-    if (L == 32 || L == 64 || L == 128 || L == 256) {
+    if (L >= 2 && L <= 256 && (L & (L - 1)) == 0) {
         warp_fft_any(a, L, B, tw, inverse);
         return a;
     }
