@@ -563,6 +563,13 @@ int blond_batch_set_impedance(blond_batch* q, int64_t n_fft, const double* Z,
                   (long long)n_fft, (long long)kMaxClusterFFT);
         return BLOND_ERR_UNSUPPORTED;
     }
+    // With at least one beam per two SMs, one CTA per beam when the whole
+    // transform fits in its shared memory: no cluster barriers, and the
+    // beams themselves fill the GPU
+    SpecPlan one;
+    if (q->B * 2 >= device_info().sm_count && make_spec_plan(n_fft, one, 1) &&
+        one.smem <= device_info().max_smem_optin)
+        plan = one;
     BB_CHECK_SIZE(n_fft >= q->S && plan.smem <= device_info().max_smem_optin,
                   "batch_set_impedance: n_fft=%lld unsupported for %d slices",
                   (long long)n_fft, q->S);

@@ -26,7 +26,7 @@ static bool smooth5(int64_t x) {
     return x == 1;
 }
 
-bool make_spec_plan(int64_t N, SpecPlan& plan) {
+bool make_spec_plan(int64_t N, SpecPlan& plan, int max_cluster) {
     if (N < 2 || (N & 1) || N > kMaxClusterFFT) return false;
     const int M = (int)(N / 2);
     if (!smooth5(M)) return false;
@@ -39,7 +39,7 @@ bool make_spec_plan(int64_t N, SpecPlan& plan) {
         if (M % m1) continue;
         const int m2 = M / m1;
         int cc = 1;
-        while (cc * 2 <= kMaxCluster && m1 % (cc * 2) == 0 && m2 % (cc * 2) == 0 &&
+        while (cc * 2 <= max_cluster && m1 % (cc * 2) == 0 && m2 % (cc * 2) == 0 &&
                M / (cc * 2) >= 64)
             cc *= 2;
         const double score = cc * 1e6 + (double)m1 / (double)m2;

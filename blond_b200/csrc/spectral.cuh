@@ -904,7 +904,7 @@ spectral_kernel(const SpecParams P, const typename SpecLoopArg<FB>::type LP) {
 
 // Host: choose the factorisation and cluster size for a real length N.
 // Returns false when N is odd, too large, or has a prime factor above 5.
-bool make_spec_plan(int64_t N, SpecPlan& plan);
+bool make_spec_plan(int64_t N, SpecPlan& plan, int max_cluster = kMaxCluster);
 // Launch one cluster of spectral_kernel with the plan in P.
 int launch_spectral(const SpecParams& P, cudaStream_t stream);
 // The same with the engine's beam-phase loop inside (single profile).
