@@ -74,6 +74,13 @@ def parse():
     ap.add_argument("--threads", type=int, default=1024)
     ap.add_argument("--blocks-per-sm", type=int, default=1)
     ap.add_argument("--prefetch", type=int, default=2, choices=[0, 2, 4])
+    ap.add_argument("--c3-forms", default="q32p64,f32p64,f64",
+                    help="c3: the precision forms to run (q32p64 gives the line's value; "
+                         "f64 also runs the beams one by one and the FP64 controls)")
+    ap.add_argument("--particles-per-thread", type=int, default=4, choices=[2, 4, 8],
+                    help="c3 with --tune fixed: particles per thread of the batched pass")
+    ap.add_argument("--chunk", type=int, default=16384,
+                    help="c3 with --tune fixed: particles per chunk of the batched pass")
     ap.add_argument("--c5-forms", default="q32p64,f32p64,f64,control",
                     help="c5: the forms to run (comma list of q32p64, f32p64, f64, control); "
                          "q32p64 gives the line's value")
@@ -724,7 +731,7 @@ def _err_summary(errs):
 
 
 def c3_measure(n_beams, W, K, T_err, precisions=("q32p64", "f32p64", "f64"),
-               controls=("ulp", "shift"), unbatched=False):
+               controls=("ulp", "shift"), unbatched=False, shape=None):
     """C3: every precision batched (autotuned launch shape, graph-replayed
     turns), timed over K turns after W, then tracked on (untimed) to turn
     T_err, where each form's per-beam rms errors against FP64 are taken.
@@ -732,7 +739,9 @@ def c3_measure(n_beams, W, K, T_err, precisions=("q32p64", "f32p64", "f64"),
     FP64 again from initial times moved by one ulp (no bin changes);
     "shift", FP64 from initial energies moved by 0.01 eV (1e-10 of the
     spread, ten times below the Q32P64 grid).  unbatched: every beam
-    through its own FP64 engine, one after the other."""
+    through its own FP64 engine, one after the other.  shape: a fixed
+    launch shape (threads, blocks per SM, particles per thread, chunk)
+    instead of the autotuner's."""
     import torch
     from blond_b200.batch import BatchTracker
     from blond_b200.engine import FusedTracker
@@ -743,14 +752,20 @@ def c3_measure(n_beams, W, K, T_err, precisions=("q32p64", "f32p64", "f64"),
     for prec in precisions:
         bt = BatchTracker([(RingAndRFTracker(rf, b), p, t) for rf, b, p, t in beams],
                           precision=prec)
-        shape = bt.autotune()
+        if shape is None:
+            picked = bt.autotune()
+        else:
+            bt.set_shape(*shape)
+            picked = {"threads": shape[0], "blocks_per_sm": shape[1],
+                      "particles_per_thread": shape[2], "chunk": shape[3],
+                      "particle_pass_ms": None}
         bt.track(W)
         bt.prepare()
         ms = time_turns(bt, K)
         bt.track(T_err - W - K)  # untimed, to the comparison turn
         bt.check()
         res[prec] = {"value": n_total * K / (ms * 1e-3), "ms_per_step": ms / K,
-                     "autotuned": shape}
+                     "autotuned": picked}
         trackers[prec] = bt
         for rf, _, _, _ in beams:
             rf.counter[0] = 0
@@ -1171,7 +1186,13 @@ def main():
         return
     if args.workload == "c3" and args.impl == "ours":
         W, K = max(3, args.warmup), args.steps
-        m = c3_measure(args.beams, W, K, max(1000, W + K), unbatched=True)
+        forms = tuple(args.c3_forms.split(","))
+        shape = ((args.threads, args.blocks_per_sm, args.particles_per_thread, args.chunk)
+                 if args.tune == "fixed" else None)
+        T_err = max(args.batched_error_turns, W + K) if args.batched_error_turns > 0 else W + K
+        m = c3_measure(args.beams, W, K, T_err, precisions=forms,
+                       controls=("ulp", "shift") if args.batched_error_turns > 0 else (),
+                       unbatched="f64" in forms, shape=shape)
         q = m["runs"]["q32p64"]
         peak = _peaks().get("hbm_gbs") or 6650.0
         print(json.dumps({
@@ -1181,21 +1202,21 @@ def main():
             "dtype": "q32p64", "data": "synthetic",
             "config": {"workload": C3_WORKLOAD, "beams": args.beams,
                        "particles_total": m["n_total"], "slices": 512, "n_fft": 512},
-            "runs": {k: {**v, "particle_pass_gbs": 24 * m["n_total"] /
-                         (v["autotuned"]["particle_pass_ms"] * 1e-3) / 1e9
-                         if k != "f64" else 32 * m["n_total"] /
-                         (v["autotuned"]["particle_pass_ms"] * 1e-3) / 1e9}
+            "runs": {k: {**v, "particle_pass_gbs": (24 if k != "f64" else 32) * m["n_total"]
+                         / (v["autotuned"]["particle_pass_ms"] * 1e-3) / 1e9
+                         if v["autotuned"].get("particle_pass_ms") else None}
                      for k, v in m["runs"].items()},
             "hbm_peak_gbs": peak,
-            "unbatched_plain_f64": m["unbatched_f64"],
+            "unbatched_plain_f64": m.get("unbatched_f64"),
             "speedup_q32p64_batched_vs_unbatched_f64":
-                q["value"] / m["unbatched_f64"]["value"],
+                q["value"] / m["unbatched_f64"]["value"] if "unbatched_f64" in m else None,
             "rel_err_after_turns": {
                 "turns": m["turns"],
                 "statistic": "in-window rms of dt and dE, per beam, vs the FP64 batch",
-                **{k: _err_summary(v) for k, v in m["errors"].items()},
-                "control_fp64_one_ulp": _err_summary(m["controls"]["ulp"]),
-                "control_fp64_dE_plus_0.01eV": _err_summary(m["controls"]["shift"])},
+                **{k: _err_summary(v) for k, v in m.get("errors", {}).items()},
+                **({"control_fp64_one_ulp": _err_summary(m["controls"]["ulp"]),
+                    "control_fp64_dE_plus_0.01eV": _err_summary(m["controls"]["shift"])}
+                   if m.get("controls") else {})},
             "gpu_launches": 2 * K,
         }), flush=True)
         return
