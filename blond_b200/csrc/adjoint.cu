@@ -252,8 +252,10 @@ adj_backward_kernel(const AdjTurn T, int kick, const double* __restrict__ dt,
 #pragma unroll
             for (int j = 0; j < kAdjMaxRf; ++j) {
                 if (j < T.n_rf) {
+                    // sin and cos at the forward's phase, to rounding (the
+                    // forward map itself keeps CUDA's sin)
                     double s, c;
-                    sincos(adj_reduce_2pi(fma(sOm[j], t, sPh[j])), &s, &c);
+                    rf_sincos(fma(sOm[j], t, sPh[j]), &s, &c);
                     dg += sV[j] * sOm[j] * c;
                     gv[j] += lE * s;
                     gp[j] += lE * sV[j] * c;

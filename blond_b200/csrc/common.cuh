@@ -138,6 +138,43 @@ __device__ __forceinline__ double rf_sin(double x) {
     return (__double2loint(ks) & 1) ? -s : s;
 }
 
+// sin(x) and cos(x) with rf_sin's reduction: cos(x) = (-1)^k cos(r), cos r
+// = 1 + r^2 Q(r^2) with Q the degree-8 Chebyshev approximation on
+// [0, (pi/2)^2] (gen_sin_coeffs.py; within 1.6e-16 absolute).  Same range
+// as rf_sin; no branch.
+__device__ __forceinline__ void rf_sincos(double x, double* sp, double* cp) {
+    const double shifter = 6755399441055744.0;  // 1.5 * 2^52
+    const double y = __dmul_rn(x, 0.3183098861837907);
+    const double ks = __dadd_rn(y, shifter);
+    const double k = __dsub_rn(ks, shifter);
+    double r = fma(-k, 3.1415926553308964, x);
+    r = fma(-k, -1.7411031384001463e-09, r);
+    r = fma(-k, -7.00686879617986e-19, r);
+    const double r2 = r * r;
+    double p = 2.7314447669863995e-15;
+    p = fma(p, r2, -7.643970296798572e-13);
+    p = fma(p, r2, 1.6058977312464087e-10);
+    p = fma(p, r2, -2.5052107616996182e-08);
+    p = fma(p, r2, 2.7557319219163234e-06);
+    p = fma(p, r2, -0.00019841269841254974);
+    p = fma(p, r2, 0.008333333333333316);
+    p = fma(p, r2, -0.16666666666666666);
+    const double s = fma(r * r2, p, r);
+    double q = -1.5169166967261124e-16;
+    q = fma(q, r2, 4.777404889695354e-14);
+    q = fma(q, r2, -1.147069401087498e-11);
+    q = fma(q, r2, 2.0876756238770223e-09);
+    q = fma(q, r2, -2.7557319217593045e-07);
+    q = fma(q, r2, 2.4801587301556646e-05);
+    q = fma(q, r2, -0.0013888888888888816);
+    q = fma(q, r2, 0.041666666666666664);
+    q = fma(q, r2, -0.5);
+    const double c = fma(r2, q, 1.0);
+    const bool odd = (__double2loint(ks) & 1) != 0;
+    *sp = odd ? -s : s;
+    *cp = odd ? -c : c;
+}
+
 __device__ __forceinline__ double dev_sin(double x) { return rf_sin(x); }
 __device__ __forceinline__ float dev_sin(float x) { return sinf(x); }
 __device__ __forceinline__ double dev_floor(double x) { return floor(x); }

@@ -1,4 +1,5 @@
-"""Coefficients of the FP64 RF sine's polynomial (rf_sin in common.cuh).
+"""Coefficients of the FP64 RF sine's and cosine's polynomials (rf_sin and
+rf_sincos in common.cuh).
 
 sin(r) on [-pi/2, pi/2] is written r + r^3 P(r^2).  P is the degree-7
 Chebyshev approximation (mpmath.chebyfit: interpolation at Chebyshev
@@ -9,8 +10,10 @@ double.  Its approximation error in sin is below 1.3e-18; evaluated in
 double by Horner's rule with fused multiply-adds, the result is within 2
 units in the last place of sin(r) (checked here with exact fma
 emulation), as the Taylor polynomial through r^21 it replaces was, with two
-fewer terms.  Run with mpmath installed; prints the coefficients, highest
-degree first.
+fewer terms.  The cosine (for the adjoint's derivatives) is 1 + r^2 Q(r^2),
+Q the degree-8 Chebyshev approximation of (cos(sqrt u) - 1) / u (error
+below 3e-20; 1.6e-16 absolute in double).  Run with mpmath installed;
+prints the coefficients, highest degree first.
 """
 import math
 import random
@@ -44,6 +47,28 @@ def evaluate(r: float, co) -> float:
     return _fma(float(Fraction(r) * Fraction(r2)), p, r)
 
 
+def cos_coefficients(degree: int = 7):
+    """cos(r) = 1 + r^2 Q(r^2) on [-pi/2, pi/2]: Q the degree-`degree`
+    Chebyshev approximation of (cos(sqrt u) - 1) / u on [0, (pi/2)^2]."""
+    mp.mp.dps = 60
+
+    def h(u):
+        if u == 0:
+            return mp.mpf(-1) / 2
+        return (mp.cos(mp.sqrt(u)) - 1) / u
+
+    poly, err = mp.chebyfit(h, [0, (mp.pi / 2) ** 2], degree + 1, error=True)
+    return [float(c) for c in poly], float(err * (mp.pi / 2) ** 2)
+
+
+def evaluate_cos(r: float, co) -> float:
+    r2 = float(Fraction(r) * Fraction(r))
+    p = co[0]
+    for c in co[1:]:
+        p = _fma(p, r2, c)
+    return _fma(r2, p, 1.0)
+
+
 if __name__ == "__main__":
     co, bound = coefficients()
     print("approximation error bound:", bound)
@@ -54,3 +79,9 @@ if __name__ == "__main__":
     worst = max(abs(evaluate(r, co) - float(mp.sin(r))) / math.ulp(float(mp.sin(r)))
                 for r in pts if r != 0.0)
     print("max error over 20000 points (ulps):", worst)
+    cco, cbound = cos_coefficients(8)
+    print("cosine: approximation error bound:", cbound)
+    for c in cco:
+        print(repr(c))
+    worst = max(abs(evaluate_cos(r, cco) - float(mp.cos(r))) for r in pts)
+    print("max absolute error over 20000 points:", worst)
