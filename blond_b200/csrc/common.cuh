@@ -175,6 +175,26 @@ __device__ __forceinline__ void rf_sincos(double x, double* sp, double* cp) {
     *cp = odd ? -c : c;
 }
 
+// sin(x) as a float for the F32P64 kick: k = rint(x / pi) by the shifter
+// and r = x - k pi with one fused multiply-add in double (exact enough for
+// float: |k| (pi - fl(pi)) < 4e-10 below 1e7 rad), then r + r^3 P(r^2) in
+// float, P the degree-4 Chebyshev approximation on [0, (pi/2)^2]
+// (gen_sin_coeffs.py; within 2 float ulps).  No branch.
+__device__ __forceinline__ float rf_sinf(double x) {
+    const double shifter = 6755399441055744.0;  // 1.5 * 2^52
+    const double ks = __dadd_rn(__dmul_rn(x, 0.3183098861837907), shifter);
+    const double k = __dsub_rn(ks, shifter);
+    const float r = (float)fma(-k, 3.141592653589793, x);
+    const float r2 = r * r;
+    float p = -2.408019028621311e-08f;
+    p = fmaf(p, r2, 2.75364641311171e-06f);
+    p = fmaf(p, r2, -0.00019841086759697646f);
+    p = fmaf(p, r2, 0.00833333283662796f);
+    p = fmaf(p, r2, -0.1666666716337204f);
+    const float s = fmaf(r * r2, p, r);
+    return (__double2loint(ks) & 1) ? -s : s;
+}
+
 __device__ __forceinline__ double dev_sin(double x) { return rf_sin(x); }
 __device__ __forceinline__ float dev_sin(float x) { return sinf(x); }
 __device__ __forceinline__ double dev_floor(double x) { return floor(x); }

@@ -153,12 +153,6 @@ struct __align__(16) TurnConsts {
     DriftTurn d;
 };
 
-// 2 pi split for the FP64 range reduction of the RF phase.
-__device__ __forceinline__ double reduce_2pi(double x) {
-    const double inv2pi = 0.15915494309189533577;
-    const double twopi = 6.28318530717958647692;
-    return fma(-rint(x * inv2pi), twopi, x);
-}
 
 template <int PREC, int SOLVER, bool LIK, bool KICK, bool HIST, bool WARP_AGG,
           int TAB = TAB_GLOBAL>
@@ -203,7 +197,7 @@ __device__ __forceinline__ void track_one(double& t,
             } else {
                 float s = 0.0f;
                 for (int j = 0; j < a.n_rf; ++j)
-                    s += c.Vf[j] * sinf((float)reduce_2pi(fma(c.op[j].x, t, c.op[j].y)));
+                    s += c.Vf[j] * rf_sinf(fma(c.op[j].x, t, c.op[j].y));
                 e += (float)a.charge * s + (float)c.acc;
             }
         }
@@ -278,8 +272,8 @@ __device__ __forceinline__ void track_pair(double& t0, double& t1,
         } else {
             float x0 = 0.0f, x1 = 0.0f;
             for (int j = 0; j < a.n_rf; ++j) {
-                x0 += c.Vf[j] * sinf((float)reduce_2pi(fma(c.op[j].x, t0, c.op[j].y)));
-                x1 += c.Vf[j] * sinf((float)reduce_2pi(fma(c.op[j].x, t1, c.op[j].y)));
+                x0 += c.Vf[j] * rf_sinf(fma(c.op[j].x, t0, c.op[j].y));
+                x1 += c.Vf[j] * rf_sinf(fma(c.op[j].x, t1, c.op[j].y));
             }
             s0 = (E)x0;
             s1 = (E)x1;

@@ -79,6 +79,10 @@ if __name__ == "__main__":
     worst = max(abs(evaluate(r, co) - float(mp.sin(r))) / math.ulp(float(mp.sin(r)))
                 for r in pts if r != 0.0)
     print("max error over 20000 points (ulps):", worst)
+    fco, fbound = coefficients(4)
+    print("float sine (degree 4 in r^2): approximation error bound:", fbound)
+    for c in fco:
+        print(repr(float(__import__("numpy").float32(c))))
     cco, cbound = cos_coefficients(8)
     print("cosine: approximation error bound:", cbound)
     for c in cco:
