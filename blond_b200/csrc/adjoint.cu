@@ -61,6 +61,8 @@ struct AdjTurn {
     double bc0, inv_w;   // bin centres bc0 + k / inv_w
     int smem_hist;       // 1: block-private histograms in shared memory
     int fix_bits;        // fixed-point units per particle: 2^fix_bits
+    double fix_scale;    // 2^fix_bits
+    int vind_smem;       // 1: a copy of vind in shared memory for the gathers
 };
 
 template <int PREC> struct AdjE;
@@ -87,13 +89,14 @@ inline int fixed_bits(int64_t n) {
     return std::min(52, 62 - lg);
 }
 
+// (scale = 2^b: the product is exact, as ldexp's would be; floor(f) is the
+// round-down conversion for the f > -1 that get here)
 __device__ __forceinline__ void cic_deposit(u64* h, int S, double t, double bc0,
-                                            double inv_w, int bits) {
+                                            double inv_w, int bits, double scale) {
     const double f = (t - bc0) * inv_w;
     if (!(f > -1.0 && f < (double)S)) return;  // also drops NaN
-    const double fl = floor(f);
-    const int j = (int)fl;
-    const u64 w1 = (u64)llrint(ldexp(f - fl, bits));
+    const int j = __double2int_rd(f);
+    const u64 w1 = (u64)__double2ll_rn((f - (double)j) * scale);
     const u64 w0 = (1ull << bits) - w1;
     if (j >= 0 && w0) atomicAdd(&h[j], w0);
     if (j + 1 < S && w1) atomicAdd(&h[j + 1], w1);
@@ -131,19 +134,34 @@ adj_deposit_kernel(const double* __restrict__ dt, int64_t n, int S, double bc0, 
     __syncthreads();
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x)
-        cic_deposit(h, S, dt[i], bc0, inv_w, bits);
+        cic_deposit(h, S, dt[i], bc0, inv_w, bits, ldexp(1.0, bits));
     __syncthreads();
     if (smem_hist) flush_shared(sh, prof, S);
 }
 
+// Converts the fixed-point profile to counts in the block that finishes
+// last (a counter in global memory, reset by that block), so a turn needs
+// no separate conversion launch.  Every block calls it after its own
+// deposits; no block waits on another.
+__device__ void convert_when_last(u64* prof, int S, int bits, unsigned* done) {
+    __shared__ int last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(done, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    for (int k = threadIdx.x; k < S; k += blockDim.x)
+        reinterpret_cast<double*>(prof)[k] = ldexp((double)__ldcg(prof + k), -bits);
+    if (threadIdx.x == 0) *done = 0u;
+}
+
 template <int PREC>
 __global__ void __launch_bounds__(kAdjThreads)
-adj_forward_kernel(const AdjTurn T, const double* __restrict__ dt_in,
-                   const void* __restrict__ dE_in, double* __restrict__ dt_out,
-                   void* __restrict__ dE_out, u64* __restrict__ prof_out) {
+adj_forward_kernel(const AdjTurn T, const double* dt_in, const void* dE_in, double* dt_out,
+                   void* dE_out, u64* prof_out, unsigned* done) {
     using E = typename AdjE<PREC>::E;
     extern __shared__ u64 shf[];
-    u64* sh = shf;
     __shared__ double sV[kAdjMaxRf], sOm[kAdjMaxRf], sPh[kAdjMaxRf];
     if (threadIdx.x < T.n_rf) {
         sV[threadIdx.x] = T.V[threadIdx.x];
@@ -151,8 +169,15 @@ adj_forward_kernel(const AdjTurn T, const double* __restrict__ dt_in,
         sPh[threadIdx.x] = T.ph[threadIdx.x];
     }
     const bool dep = prof_out != nullptr;
-    u64* h = T.smem_hist ? sh : prof_out;
-    if (dep && T.smem_hist) zero_shared(sh, T.S);
+    const bool hsm = dep && T.smem_hist;
+    u64* h = hsm ? shf : prof_out;
+    if (hsm) zero_shared(shf, T.S);
+    const double* vind = T.vind;
+    if (vind && T.vind_smem) {
+        double* sv = reinterpret_cast<double*>(shf + (hsm ? T.S : 0));
+        for (int k = threadIdx.x; k < T.S; k += blockDim.x) sv[k] = T.vind[k];
+        vind = sv;
+    }
     __syncthreads();
     const E* dEi = static_cast<const E*>(dE_in);
     E* dEo = static_cast<E*>(dE_out);
@@ -161,13 +186,12 @@ adj_forward_kernel(const AdjTurn T, const double* __restrict__ dt_in,
          i += (int64_t)gridDim.x * blockDim.x) {
         double t = dt_in[i];
         E e = dEi[i];
-        if (T.vind) {
+        if (vind) {
             const double f = (t - T.bc0) * T.inv_w;
             if (f >= 0.0 && f < (double)(T.S - 1)) {
-                const double fl = floor(f);
-                const int k = (int)fl;
-                const double u = f - fl;
-                e += (E)(q * (T.vind[k] * (1.0 - u) + T.vind[k + 1] * u));
+                const int k = __double2int_rd(f);
+                const double w = f - (double)k;
+                e += (E)(q * (vind[k] * (1.0 - w) + vind[k + 1] * w));
             }
         }
         if (PREC == BLOND_PREC_F64) {
@@ -177,22 +201,23 @@ adj_forward_kernel(const AdjTurn T, const double* __restrict__ dt_in,
                 if (j < T.n_rf) s += sV[j] * sin(fma(sOm[j], t, sPh[j]));
             e += (E)(q * s + T.acc);
         } else {
+            // the engine's F32P64 sine: reduction in double, polynomial in float
             float s = 0.0f;
 #pragma unroll
             for (int j = 0; j < kAdjMaxRf; ++j)
-                if (j < T.n_rf)
-                    s += (float)sV[j] * sinf((float)adj_reduce_2pi(fma(sOm[j], t, sPh[j])));
+                if (j < T.n_rf) s += (float)sV[j] * rf_sinf(fma(sOm[j], t, sPh[j]));
             e += (E)q * s + (E)T.acc;
         }
         t = t + T.drift_c * (double)e;
         dt_out[i] = t;
         dEo[i] = e;
-        if (dep) cic_deposit(h, T.S, t, T.bc0, T.inv_w, T.fix_bits);
+        if (dep) cic_deposit(h, T.S, t, T.bc0, T.inv_w, T.fix_bits, T.fix_scale);
     }
-    if (dep && T.smem_hist) {
+    if (hsm) {
         __syncthreads();
-        flush_shared(sh, prof_out, T.S);
+        flush_shared(shf, prof_out, T.S);
     }
+    if (dep && done) convert_when_last(prof_out, T.S, T.fix_bits, done);
 }
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -203,7 +228,8 @@ __device__ __forceinline__ double warp_sum(double v) {
 
 // One backward turn (kick = 1), or only the deposit adjoint of a profile
 // at dt_next (kick = 0).  Shared memory: lambda_p_next copy, then the
-// block's lambda_V accumulator (S doubles each, when smem_hist).
+// block's lambda_V accumulator (S doubles each, when smem_hist), then a
+// copy of the turn's induced voltage (when vind_smem).
 __global__ void __launch_bounds__(kAdjThreads)
 adj_backward_kernel(const AdjTurn T, int kick, const double* __restrict__ dt,
                     const double* __restrict__ dt_next, const double* __restrict__ lam_p_next,
@@ -216,6 +242,7 @@ adj_backward_kernel(const AdjTurn T, int kick, const double* __restrict__ dt,
     const bool sm = T.smem_hist != 0;
     double* lp = sm ? sh : const_cast<double*>(lam_p_next);
     double* lv = sm ? sh + S : lam_v;
+    const double* vind = T.vind;
     if (kick && threadIdx.x < T.n_rf) {
         sV[threadIdx.x] = T.V[threadIdx.x];
         sOm[threadIdx.x] = T.om[threadIdx.x];
@@ -226,6 +253,11 @@ adj_backward_kernel(const AdjTurn T, int kick, const double* __restrict__ dt,
             sh[k] = lam_p_next ? lam_p_next[k] : 0.0;
             sh[S + k] = 0.0;
         }
+    }
+    if (vind && T.vind_smem) {
+        double* sv = sh + 2 * S;
+        for (int k = threadIdx.x; k < S; k += blockDim.x) sv[k] = T.vind[k];
+        vind = sv;
     }
     __syncthreads();
     const double q = T.charge;
@@ -239,7 +271,7 @@ adj_backward_kernel(const AdjTurn T, int kick, const double* __restrict__ dt,
         if (lam_p_next) {
             const double f = (dt_next[i] - T.bc0) * T.inv_w;
             if (f > -1.0 && f < (double)S) {
-                const int j = (int)floor(f);
+                const int j = __double2int_rd(f);
                 const double a = j >= 0 ? lp[j] : 0.0;
                 const double b = j + 1 < S ? lp[j + 1] : 0.0;
                 ldt += (b - a) * T.inv_w;
@@ -262,15 +294,14 @@ adj_backward_kernel(const AdjTurn T, int kick, const double* __restrict__ dt,
                 }
             }
             dg *= q;
-            if (T.vind) {
+            if (vind) {
                 const double f = (t - T.bc0) * T.inv_w;
                 if (f >= 0.0 && f < (double)(S - 1)) {
-                    const double fl = floor(f);
-                    const int k = (int)fl;
-                    const double u = f - fl;
-                    dg += q * (T.vind[k + 1] - T.vind[k]) * T.inv_w;
-                    atomicAdd(&lv[k], lE * q * (1.0 - u));
-                    atomicAdd(&lv[k + 1], lE * q * u);
+                    const int k = __double2int_rd(f);
+                    const double w = f - (double)k;
+                    dg += q * (vind[k + 1] - vind[k]) * T.inv_w;
+                    atomicAdd(&lv[k], lE * q * (1.0 - w));
+                    atomicAdd(&lv[k + 1], lE * q * w);
                 }
             }
             ldt += lE * dg;
@@ -303,6 +334,10 @@ adj_backward_kernel(const AdjTurn T, int kick, const double* __restrict__ dt,
 
 static int adj_smem_limit() { return (device_info().max_smem_optin - 4096) / 16; }
 
+// Shared memory a block may take for its copy of the induced voltage (with
+// the arrays it holds anyway), so that four blocks still fit on an SM.
+constexpr size_t kAdjVindSmem = 48 * 1024;
+
 template <typename K>
 static int adj_allow_smem(K kernel, bool* done) {
     const DeviceInfo& d = device_info();
@@ -312,6 +347,68 @@ static int adj_allow_smem(K kernel, bool* done) {
         BB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      d.max_smem_optin - (int)fa.sharedSizeBytes));
         done[d.device & 63] = true;
+    }
+    return BLOND_OK;
+}
+
+// One forward turn.  With a counter (`done`, zero between launches) the
+// last block converts the deposited profile to counts; without one a
+// second launch does.
+static int adj_forward_launch(int precision, const double* dt_in, const void* dE_in,
+                              double* dt_out, void* dE_out, int64_t n, int n_rf,
+                              const double* voltage, const double* omega_rf,
+                              const double* phi_rf, double acc_kick, double charge,
+                              double drift_coeff, const double* induced_voltage,
+                              int n_slices, double bin_center0, double inv_bin_width,
+                              double* profile_out, unsigned* done, void* stream) {
+    BB_CHECK_ARG(precision == BLOND_PREC_F64 || precision == BLOND_PREC_F32P64,
+                 "adjoint_forward_turn: unknown precision %d", precision);
+    BB_CHECK_SIZE(n_rf >= 0 && n_rf <= kAdjMaxRf, "adjoint_forward_turn: n_rf=%d not in "
+                  "[0, %d]", n_rf, kAdjMaxRf);
+    BB_CHECK_ARG(n >= 0 && n_slices >= 2, "adjoint_forward_turn: bad size");
+    BB_CHECK_ARG((n == 0 || (dt_in && dE_in && dt_out && dE_out)) &&
+                     (n_rf == 0 || (voltage && omega_rf && phi_rf)),
+                 "adjoint_forward_turn: null pointer");
+    if (n == 0) return BLOND_OK;
+    AdjTurn T = {};
+    T.n = n;
+    T.n_rf = n_rf;
+    T.V = voltage;
+    T.om = omega_rf;
+    T.ph = phi_rf;
+    T.acc = acc_kick;
+    T.charge = charge;
+    T.drift_c = drift_coeff;
+    T.vind = induced_voltage;
+    T.S = n_slices;
+    T.bc0 = bin_center0;
+    T.inv_w = inv_bin_width;
+    T.smem_hist = n_slices <= adj_smem_limit() ? 1 : 0;
+    T.fix_bits = fixed_bits(n);
+    T.fix_scale = ldexp(1.0, T.fix_bits);
+    const size_t hist = profile_out && T.smem_hist ? sizeof(u64) * n_slices : 0;
+    T.vind_smem = induced_voltage && hist + sizeof(double) * n_slices <= kAdjVindSmem;
+    const size_t smem = hist + (T.vind_smem ? sizeof(double) * n_slices : 0);
+    const int grid = particle_grid(n, kAdjThreads, 4);
+    cudaStream_t s = as_stream(stream);
+    u64* prof = reinterpret_cast<u64*>(profile_out);
+    int rc;
+    if (precision == BLOND_PREC_F64) {
+        static bool attr[64] = {false};
+        if ((rc = adj_allow_smem(adj_forward_kernel<BLOND_PREC_F64>, attr))) return rc;
+        adj_forward_kernel<BLOND_PREC_F64><<<grid, kAdjThreads, smem, s>>>(
+            T, dt_in, dE_in, dt_out, dE_out, prof, done);
+    } else {
+        static bool attr[64] = {false};
+        if ((rc = adj_allow_smem(adj_forward_kernel<BLOND_PREC_F32P64>, attr))) return rc;
+        adj_forward_kernel<BLOND_PREC_F32P64><<<grid, kAdjThreads, smem, s>>>(
+            T, dt_in, dE_in, dt_out, dE_out, prof, done);
+    }
+    BB_LAUNCH_CHECK();
+    if (profile_out && !done) {
+        fixed_to_counts_kernel<<<(n_slices + 255) / 256, 256, 0, s>>>(profile_out, n_slices,
+                                                                      T.fix_bits);
+        BB_LAUNCH_CHECK();
     }
     return BLOND_OK;
 }
@@ -350,52 +447,10 @@ int blond_adjoint_forward_turn(int precision, const double* dt_in, const void* d
                                double drift_coeff, const double* induced_voltage,
                                int n_slices, double bin_center0, double inv_bin_width,
                                double* profile_out, void* stream) {
-    BB_CHECK_ARG(precision == BLOND_PREC_F64 || precision == BLOND_PREC_F32P64,
-                 "adjoint_forward_turn: unknown precision %d", precision);
-    BB_CHECK_SIZE(n_rf >= 0 && n_rf <= kAdjMaxRf, "adjoint_forward_turn: n_rf=%d not in "
-                  "[0, %d]", n_rf, kAdjMaxRf);
-    BB_CHECK_ARG(n >= 0 && n_slices >= 2, "adjoint_forward_turn: bad size");
-    BB_CHECK_ARG((n == 0 || (dt_in && dE_in && dt_out && dE_out)) &&
-                     (n_rf == 0 || (voltage && omega_rf && phi_rf)),
-                 "adjoint_forward_turn: null pointer");
-    if (n == 0) return BLOND_OK;
-    AdjTurn T = {};
-    T.n = n;
-    T.n_rf = n_rf;
-    T.V = voltage;
-    T.om = omega_rf;
-    T.ph = phi_rf;
-    T.acc = acc_kick;
-    T.charge = charge;
-    T.drift_c = drift_coeff;
-    T.vind = induced_voltage;
-    T.S = n_slices;
-    T.bc0 = bin_center0;
-    T.inv_w = inv_bin_width;
-    T.smem_hist = n_slices <= adj_smem_limit() ? 1 : 0;
-    T.fix_bits = fixed_bits(n);
-    const size_t smem = profile_out && T.smem_hist ? sizeof(u64) * n_slices : 0;
-    const int grid = particle_grid(n, kAdjThreads, 4);
-    cudaStream_t s = as_stream(stream);
-    int rc;
-    if (precision == BLOND_PREC_F64) {
-        static bool done[64] = {false};
-        if ((rc = adj_allow_smem(adj_forward_kernel<BLOND_PREC_F64>, done))) return rc;
-        adj_forward_kernel<BLOND_PREC_F64><<<grid, kAdjThreads, smem, s>>>(
-            T, dt_in, dE_in, dt_out, dE_out, reinterpret_cast<u64*>(profile_out));
-    } else {
-        static bool done[64] = {false};
-        if ((rc = adj_allow_smem(adj_forward_kernel<BLOND_PREC_F32P64>, done))) return rc;
-        adj_forward_kernel<BLOND_PREC_F32P64><<<grid, kAdjThreads, smem, s>>>(
-            T, dt_in, dE_in, dt_out, dE_out, reinterpret_cast<u64*>(profile_out));
-    }
-    BB_LAUNCH_CHECK();
-    if (profile_out) {
-        fixed_to_counts_kernel<<<(n_slices + 255) / 256, 256, 0, s>>>(profile_out, n_slices,
-                                                                      T.fix_bits);
-        BB_LAUNCH_CHECK();
-    }
-    return BLOND_OK;
+    return adj_forward_launch(precision, dt_in, dE_in, dt_out, dE_out, n, n_rf, voltage,
+                              omega_rf, phi_rf, acc_kick, charge, drift_coeff,
+                              induced_voltage, n_slices, bin_center0, inv_bin_width,
+                              profile_out, nullptr, stream);
 }
 
 int blond_adjoint_backward_turn(const double* dt, const double* dt_next, int64_t n,
@@ -427,10 +482,11 @@ int blond_adjoint_backward_turn(const double* dt, const double* dt_next, int64_t
     T.bc0 = bin_center0;
     T.inv_w = inv_bin_width;
     T.smem_hist = n_slices <= adj_smem_limit() ? 1 : 0;
+    T.vind_smem = T.vind && T.smem_hist && 3 * sizeof(double) * n_slices <= kAdjVindSmem;
     static bool done[64] = {false};
     int rc;
     if ((rc = adj_allow_smem(adj_backward_kernel, done))) return rc;
-    const size_t smem = T.smem_hist ? 2 * sizeof(double) * n_slices : 0;
+    const size_t smem = T.smem_hist ? (T.vind_smem ? 3 : 2) * sizeof(double) * n_slices : 0;
     const int grid = particle_grid(n, kAdjThreads, 4);
     adj_backward_kernel<<<grid, kAdjThreads, smem, as_stream(stream)>>>(
         T, kick, dt, dt_next, lam_p_next, lam_dt, lam_dE, lam_v, grad_rf);
@@ -519,6 +575,20 @@ struct AdjSpectral {
     }
 };
 
+// A zeroed device counter for the forward kernel's last-block conversion,
+// owned by one run.
+struct AdjCounter {
+    unsigned* p = nullptr;
+    ~AdjCounter() {
+        if (p) cudaFree(p);
+    }
+    int init(cudaStream_t s) {
+        BB_CUDA(cudaMalloc(&p, sizeof(unsigned)));
+        BB_CUDA(cudaMemsetAsync(p, 0, sizeof(unsigned), s));
+        return BLOND_OK;
+    }
+};
+
 }  // namespace bb
 
 extern "C" {
@@ -546,8 +616,10 @@ int blond_adjoint_forward_run(int precision, double* dt, void* dE, int64_t n, in
     const size_t esz = precision == BLOND_PREC_F64 ? sizeof(double) : sizeof(float);
     const int64_t M1 = n_fft / 2 + 1;
     AdjSpectral sp;
+    AdjCounter done;
     int rc;
     if (impedance && (rc = sp.init(n_fft))) return rc;
+    if ((rc = done.init(s))) return rc;
     if ((rc = blond_adjoint_deposit(dt, n, n_slices, bin_center0, inv_bin_width, profile,
                                     stream)))
         return rc;
@@ -564,10 +636,10 @@ int blond_adjoint_forward_run(int precision, double* dt, void* dE, int64_t n, in
             (rc = sp.run(0, profile + t * n_slices, n_slices, impedance, scale, vind,
                          spectrum + t * M1 * 2, nullptr, s)))
             return rc;
-        if ((rc = blond_adjoint_forward_turn(
+        if ((rc = adj_forward_launch(
                  precision, dt, dE, dt, dE, n, n_rf, voltage + t * n_rf, omega_rf + t * n_rf,
                  phi_rf + t * n_rf, acc_kick[t], charge, drift_coeff[t], vind, n_slices,
-                 bin_center0, inv_bin_width, profile + (t + 1) * n_slices, stream)))
+                 bin_center0, inv_bin_width, profile + (t + 1) * n_slices, done.p, stream)))
             return rc;
     }
     return BLOND_OK;
