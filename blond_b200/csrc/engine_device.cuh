@@ -271,6 +271,8 @@ __device__ __forceinline__ void track_pair(double& t0, double& t1,
             s1 = (E)x1;
         } else {
             float x0 = 0.0f, x1 = 0.0f;
+            // unrolled by two: C2 F32P64 (one harmonic) pass 47.3 -> 46.8 us
+#pragma unroll 2
             for (int j = 0; j < a.n_rf; ++j) {
                 x0 += c.Vf[j] * rf_sinf(fma(c.op[j].x, t0, c.op[j].y));
                 x1 += c.Vf[j] * rf_sinf(fma(c.op[j].x, t1, c.op[j].y));
