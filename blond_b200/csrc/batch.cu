@@ -53,7 +53,20 @@ struct BatchArgs {
     const double* lsb;          // Q32P64: [2B] energy unit per beam, then its inverse
     int* err;                   // sticky error word (ERR_ENERGY_RANGE)
     int agg;                    // warp-aggregated shared-memory deposits
+    unsigned* next_chunk;       // chunks claimed beyond the first wave (zero between launches)
 };
+
+// Block b starts on chunk b; afterwards each block claims the next unclaimed
+// chunk (chunks are sorted by size, largest first, so the launch ends on
+// small ones and the blocks finish together).  There are n_chunks claims
+// per launch (every chunk past the first wave once, plus one failed claim
+// per block); the block making the last one resets the counter for the
+// next launch, when no block of this launch touches it any more.
+__device__ __forceinline__ int claim_chunk(unsigned* counter, int n_chunks) {
+    const unsigned v = atomicAdd(counter, 1u);
+    if (v == (unsigned)n_chunks - 1u) *counter = 0u;
+    return (int)gridDim.x + (int)v;
+}
 
 // The launch bound (1024 threads, one block) caps registers at 64 a thread,
 // so every shape with at most 1024 resident threads per SM runs the same
@@ -76,7 +89,8 @@ particle_kernel_batch(const BatchArgs a) {
     E* dE = reinterpret_cast<E*>(a.dE);
     const int S = a.S;
     const uint64_t pol = evict_first_policy();
-    for (int ch = blockIdx.x; ch < a.n_chunks; ch += gridDim.x) {
+    __shared__ int next;
+    for (int ch = blockIdx.x; ch < a.n_chunks; ch = next) {
         const int b = a.chunk_beam[ch];
         const long long start = a.chunk_start[ch];
         const int count = a.chunk_count[ch];
@@ -173,6 +187,7 @@ particle_kernel_batch(const BatchArgs a) {
             const int v = sh[k];
             if (v) atomicAdd(&a.hist[(long long)b * S + k], v);
         }
+        if (threadIdx.x == 0) next = claim_chunk(a.next_chunk, a.n_chunks);
         __syncthreads();  // shared histogram and constants are reused
     }
 }
@@ -217,6 +232,7 @@ struct blond_batch {
     double* d_lsb = nullptr;       // Q32P64: [2B] energy units, then inverses
     bool lsb_set = false;
     int* d_err = nullptr;          // sticky error word of the particle pass
+    unsigned* d_next_chunk = nullptr;  // the particle pass's chunk claims
     bool rf_set = false, drift_set = false, slicing_set = false;
     // launch shape of the particle pass
     int threads = 512, blocks_per_sm = 2, ppt = 4, chunk = bb::kBatchChunkDefault, agg = 0;
@@ -259,6 +275,7 @@ static BatchArgs batch_args(blond_batch* q) {
     a.lsb = q->d_lsb;
     a.err = q->d_err;
     a.agg = q->agg;
+    a.next_chunk = q->d_next_chunk;
     return a;
 }
 
@@ -324,16 +341,23 @@ static int launch_batch(blond_batch* q, bool kick, cudaStream_t s, bool launch =
 }
 
 // Cut every beam into chunks of at most q->chunk particles (one block's
-// piece of work) and upload the chunk table.
+// piece of work), largest first (the blocks claim them in this order), and
+// upload the chunk table.
 static int batch_rechunk(blond_batch* q) {
+    struct Chunk { long long start; int beam, count; };
+    std::vector<Chunk> all;
+    for (int b = 0; b < q->B; ++b) {
+        for (int64_t s0 = q->offsets[b]; s0 < q->offsets[b + 1]; s0 += q->chunk)
+            all.push_back({s0, b, (int)std::min<int64_t>(q->chunk, q->offsets[b + 1] - s0)});
+    }
+    std::stable_sort(all.begin(), all.end(),
+                     [](const Chunk& x, const Chunk& y) { return x.count > y.count; });
     std::vector<long long> cs;
     std::vector<int> cb, cc;
-    for (int b = 0; b < q->B; ++b) {
-        for (int64_t s0 = q->offsets[b]; s0 < q->offsets[b + 1]; s0 += q->chunk) {
-            cs.push_back(s0);
-            cb.push_back(b);
-            cc.push_back((int)std::min<int64_t>(q->chunk, q->offsets[b + 1] - s0));
-        }
+    for (const Chunk& c : all) {
+        cs.push_back(c.start);
+        cb.push_back(c.beam);
+        cc.push_back(c.count);
     }
     int rc;
     q->n_chunks = (int)cs.size();
@@ -429,6 +453,7 @@ int blond_batch_create(blond_batch** out, int precision, int n_beams, int n_rf, 
     int rc = BLOND_OK;
     if (cudaMalloc(&q->d_turn, sizeof(long long)) != cudaSuccess ||
         cudaMalloc(&q->d_err, sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&q->d_next_chunk, sizeof(unsigned)) != cudaSuccess ||
         cudaMalloc(&q->d_hist, sizeof(int) * bs) != cudaSuccess ||
         cudaMalloc(&q->d_profile, sizeof(double) * bs) != cudaSuccess ||
         cudaMalloc(&q->d_vind, sizeof(double) * bs) != cudaSuccess ||
@@ -439,6 +464,7 @@ int blond_batch_create(blond_batch** out, int precision, int n_beams, int n_rf, 
     } else {
         cudaMemset(q->d_turn, 0, sizeof(long long));
         cudaMemset(q->d_err, 0, sizeof(int));
+        cudaMemset(q->d_next_chunk, 0, sizeof(unsigned));
         cudaMemset(q->d_hist, 0, sizeof(int) * bs);
         cudaMemset(q->d_profile, 0, sizeof(double) * bs);
         cudaMemset(q->d_vind, 0, sizeof(double) * bs);
@@ -467,7 +493,7 @@ int blond_batch_destroy(blond_batch* q) {
                     (void*)q->d_bc0, (void*)q->d_lik_inv_w, (void*)q->d_bw, (void*)q->d_bc,
                     (void*)q->d_H, (void*)q->d_scale, (void*)q->d_tw, (void*)q->d_hist,
                     (void*)q->d_profile, (void*)q->d_vind, q->d_table, (void*)q->d_turn,
-                    (void*)q->d_lsb, (void*)q->d_err})
+                    (void*)q->d_lsb, (void*)q->d_err, (void*)q->d_next_chunk})
         free_ptr(p);
     delete q;
     return BLOND_OK;

@@ -38,7 +38,8 @@ def test_autotune_leaves_the_beam_untouched(cuda, precision):
     dt0 = fa.dt.cpu().numpy().copy()
     cfg = fa.autotune(reps=2)
     assert cfg["candidates"] > 0 and cfg["particle_pass_ms"] > 0
-    assert cfg["kernel"] in ("tma", "plain")
+    # whichever pass wins on this box: every candidate gives the same bits
+    assert cfg["kernel"] in ("tma", "plain", "stab", "packed")
     np.testing.assert_array_equal(fa.dt.cpu().numpy(), dt0)
     fa.track(nt)
     np.testing.assert_array_equal(fa.dt.cpu().numpy(), ref[0])
