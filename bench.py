@@ -478,9 +478,10 @@ def run_ours(args, world, rank, local):
             "beams_within_1e-5": int(np.sum(eq.max(axis=1) <= 1e-5)),
             "max_rel_err": float(eq.max()),
             "autotuned": q["autotuned"],
+            "clocks": q["clocks"],
             "f32p64": {"value": f32["value"], "ms_per_step": f32["ms_per_step"],
                        "beams_within_1e-5": int(np.sum(ef.max(axis=1) <= 1e-5)),
-                       "max_rel_err": float(ef.max())},
+                       "max_rel_err": float(ef.max()), "clocks": f32["clocks"]},
             "f64": {"value": f64["value"], "ms_per_step": f64["ms_per_step"]},
             "control_fp64_dE_plus_0.01eV": {
                 "what": "FP64 from energies moved by 0.01 eV vs FP64: the beams' own "
@@ -761,11 +762,13 @@ def c3_measure(n_beams, W, K, T_err, precisions=("q32p64", "f32p64", "f64"),
                       "particle_pass_ms": None}
         bt.track(W)
         bt.prepare()
+        clocks = ClockSampler(torch.cuda.current_device())
         ms = time_turns(bt, K)
+        clk = clocks.stop()
         bt.track(T_err - W - K)  # untimed, to the comparison turn
         bt.check()
         res[prec] = {"value": n_total * K / (ms * 1e-3), "ms_per_step": ms / K,
-                     "autotuned": picked}
+                     "autotuned": picked, "clocks": clk}
         trackers[prec] = bt
         for rf, _, _, _ in beams:
             rf.counter[0] = 0

@@ -140,47 +140,82 @@ particle_kernel_batch(const BatchArgs a) {
         // loads in flight per SM, which capped HBM near 2.4 TB/s).  Whole
         // warps iterate together, so the aggregated deposit's warp vote
         // sees every lane.
+        // PPT particles per thread and iteration as PPT / 2 pairs of
+        // neighbours (one 16-byte dt load, one pair-sized dE load each), all
+        // loads issued before any arithmetic (two particles per thread left
+        // ~16 KB of loads in flight per SM, which capped HBM near 2.4 TB/s).
+        // Pairs start on an even particle index; an odd first particle and
+        // an unpaired last one go through the same arithmetic below.  Whole
+        // warps iterate together, so the aggregated deposit's warp vote sees
+        // every lane.
+        using E2 = typename Vec2<E>::type;
+        constexpr int PP = PPT / 2;
         const int bd = blockDim.x;
         const int lane_base = threadIdx.x & ~31;
-        for (int w = lane_base; w < count; w += PPT * bd) {
-            const int i = w + (threadIdx.x & 31);
+        const int head = (int)(start & 1);
+        const long long p0 = (start + head) >> 1;  // first pair
+        const int npair = (count - head) >> 1;
+        const double2* dt2 = reinterpret_cast<const double2*>(dt);
+        const E2* dE2 = reinterpret_cast<const E2*>(dE);
+        for (int w = lane_base; w < npair; w += PP * bd) {
+            const int j = w + (threadIdx.x & 31);
             // F32P64: thread 0 prefetches the block's next iteration into L2
             // (C3: 2.059 -> 2.040 ms per turn)
-            if (PREC == PREC_F32P64 && threadIdx.x == 0 && w + PPT * bd < count) {
-                const long long lo = start + w + (long long)PPT * bd;
-                const long long hi = start + min((long long)count, (long long)w + 2LL * PPT * bd);
+            if (PREC == PREC_F32P64 && threadIdx.x == 0 && w + PP * bd < npair) {
+                const long long lo = 2 * (p0 + w + (long long)PP * bd);
+                const long long hi = 2 * (p0 + min((long long)npair, (long long)w + 2LL * PP * bd));
                 l2_prefetch_range(dt + lo, dt + hi, pol);
                 l2_prefetch_range(dE + lo, dE + hi, pol);
             }
-            double tq[PPT];
-            E e[PPT];
-            bool in[PPT];
+            double2 tq[PP];
+            E2 e[PP];
+            bool in[PP];
 #pragma unroll
-            for (int q = 0; q < PPT; ++q) {
-                in[q] = i + q * bd < count;
-                const long long g = start + (in[q] ? i + q * bd : 0);
-                tq[q] = stream_load(dt + g, pol);
-                e[q] = stream_load(dE + g, pol);
+            for (int q = 0; q < PP; ++q) {
+                in[q] = j + q * bd < npair;
+                const long long g = p0 + (in[q] ? j + q * bd : 0);
+                tq[q] = stream_load(dt2 + g, pol);
+                e[q] = stream_load(dE2 + g, pol);
             }
             if (KICK) {
 #pragma unroll
-                for (int q = 0; q < PPT; q += 2)
+                for (int q = 0; q < PP; ++q)
                     track_pair<PREC, SOLVER, LIK, (TSM && LIK) ? TAB_ENTRIES : TAB_GLOBAL>(
-                        tq[q], tq[q + 1], e[q], e[q + 1], c, pa, a.order, stab);
+                        tq[q].x, tq[q].y, e[q].x, e[q].y, c, pa, a.order, stab);
 #pragma unroll
-                for (int q = 0; q < PPT; ++q) {
+                for (int q = 0; q < PP; ++q) {
                     if (in[q]) {
-                        stream_store(dt + start + i + q * bd, tq[q], pol);
-                        stream_store(dE + start + i + q * bd, e[q], pol);
+                        stream_store(reinterpret_cast<double2*>(dt) + p0 + j + q * bd, tq[q], pol);
+                        stream_store(reinterpret_cast<E2*>(dE) + p0 + j + q * bd, e[q], pol);
                     }
                 }
             }
 #pragma unroll
-            for (int q = 0; q < PPT; ++q) {
-                const int bq = in[q] ? engine_bin(tq[q], cl, iw, S) : -1;
-                if (a.agg) deposit(sh, bq, true, 0xffffffffu);
-                else if (bq >= 0) atomicAdd(&sh[bq], 1);
+            for (int q = 0; q < PP; ++q) {
+                const int b0 = in[q] ? engine_bin(tq[q].x, cl, iw, S) : -1;
+                const int b1 = in[q] ? engine_bin(tq[q].y, cl, iw, S) : -1;
+                if (a.agg) {
+                    deposit(sh, b0, true, 0xffffffffu);
+                    deposit(sh, b1, true, 0xffffffffu);
+                } else {
+                    if (b0 >= 0) atomicAdd(&sh[b0], 1);
+                    if (b1 >= 0) atomicAdd(&sh[b1], 1);
+                }
             }
+        }
+        // the odd first particle (thread 0) and the unpaired last one (thread 1)
+        if (threadIdx.x < 2 && (threadIdx.x == 0 ? head : (count - head) & 1)) {
+            const long long g = threadIdx.x == 0 ? start : start + count - 1;
+            double t0 = dt[g], t1 = t0;
+            E e0 = dE[g], e1 = e0;
+            if (KICK) {
+                track_pair<PREC, SOLVER, LIK, (TSM && LIK) ? TAB_ENTRIES : TAB_GLOBAL>(
+                    t0, t1, e0, e1, c, pa, a.order, stab);
+                dt[g] = t0;
+                dE[g] = e0;
+            }
+            const int bq = engine_bin(t0, cl, iw, S);
+            if (bq >= 0) atomicAdd(&sh[bq], 1);
         }
         __syncthreads();
         for (int k = threadIdx.x; k < S; k += blockDim.x) {
@@ -617,7 +652,8 @@ int blond_batch_set_impedance(blond_batch* q, int64_t n_fft, const double* Z,
 int blond_batch_bind_beams(blond_batch* q, void* dt, void* dE, const int64_t* offsets) {
     using namespace bb;
     BB_CHECK_ARG(q && dt && dE && offsets, "batch_bind_beams: null pointer");
-    BB_CHECK_ARG(aligned(dt, 8) && aligned(dE, 8), "batch_bind_beams: misaligned arrays");
+    BB_CHECK_ARG(aligned(dt, 16) && aligned(dE, 16),
+                 "batch_bind_beams: dt and dE must be 16-byte aligned");
     BB_CHECK_ARG(offsets[0] == 0, "batch_bind_beams: offsets[0] must be 0");
     for (int b = 0; b < q->B; ++b)
         BB_CHECK_ARG(offsets[b + 1] >= offsets[b], "batch_bind_beams: offsets decrease");

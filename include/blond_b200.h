@@ -490,7 +490,8 @@ int blond_engine_autotune(blond_engine* engine, int reps, void* stream, int* con
  * [B][n_turns+1], cuts [B], bin_centers [B][n_slices], impedance
  * [B][n_fft/2+1] complex, scale [B] (= charge * e * ratio of each beam).
  * dt/dE: device arrays of all beams concatenated, beam b occupying
- * [offsets[b], offsets[b+1]) (host offsets). */
+ * [offsets[b], offsets[b+1]) (host offsets), both 16-byte aligned (the
+ * particle pass loads neighbouring particles in pairs). */
 typedef struct blond_batch blond_batch;
 int blond_batch_create(blond_batch** batch, int precision, int n_beams, int n_rf,
                        int solver, int n_slices);
