@@ -39,6 +39,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <mutex>
+#include <set>
+#include <utility>
 
 #include "../../include/blond_b200.h"
 #include "common.cuh"
@@ -156,7 +159,11 @@ __device__ void convert_when_last(u64* prof, int S, int bits, unsigned* done) {
     if (threadIdx.x == 0) *done = 0u;
 }
 
-template <int PREC>
+// NRF: the number of RF harmonics, a template parameter so that every
+// harmonic's arithmetic is issued only when it exists (a runtime count
+// under an unrolled loop to kAdjMaxRf left the unused harmonics' sines
+// issued under predicates).
+template <int PREC, int NRF>
 __global__ void __launch_bounds__(kAdjThreads)
 adj_forward_kernel(const AdjTurn T, const double* dt_in, const void* dE_in, double* dt_out,
                    void* dE_out, u64* prof_out, unsigned* done) {
@@ -197,15 +204,13 @@ adj_forward_kernel(const AdjTurn T, const double* dt_in, const void* dE_in, doub
         if (PREC == BLOND_PREC_F64) {
             double s = 0.0;
 #pragma unroll
-            for (int j = 0; j < kAdjMaxRf; ++j)
-                if (j < T.n_rf) s += sV[j] * sin(fma(sOm[j], t, sPh[j]));
+            for (int j = 0; j < NRF; ++j) s += sV[j] * sin(fma(sOm[j], t, sPh[j]));
             e += (E)(q * s + T.acc);
         } else {
             // the engine's F32P64 sine: reduction in double, polynomial in float
             float s = 0.0f;
 #pragma unroll
-            for (int j = 0; j < kAdjMaxRf; ++j)
-                if (j < T.n_rf) s += (float)sV[j] * rf_sinf(fma(sOm[j], t, sPh[j]));
+            for (int j = 0; j < NRF; ++j) s += (float)sV[j] * rf_sinf(fma(sOm[j], t, sPh[j]));
             e += (E)q * s + (E)T.acc;
         }
         t = t + T.drift_c * (double)e;
@@ -230,6 +235,7 @@ __device__ __forceinline__ double warp_sum(double v) {
 // at dt_next (kick = 0).  Shared memory: lambda_p_next copy, then the
 // block's lambda_V accumulator (S doubles each, when smem_hist), then a
 // copy of the turn's induced voltage (when vind_smem).
+template <int NRF>
 __global__ void __launch_bounds__(kAdjThreads)
 adj_backward_kernel(const AdjTurn T, int kick, const double* __restrict__ dt,
                     const double* __restrict__ dt_next, const double* __restrict__ lam_p_next,
@@ -282,16 +288,14 @@ adj_backward_kernel(const AdjTurn T, int kick, const double* __restrict__ dt,
             const double lE = ldE + T.drift_c * ldt;
             double dg = 0.0;
 #pragma unroll
-            for (int j = 0; j < kAdjMaxRf; ++j) {
-                if (j < T.n_rf) {
-                    // sin and cos at the forward's phase, to rounding (the
-                    // forward map itself keeps CUDA's sin)
-                    double s, c;
-                    rf_sincos(fma(sOm[j], t, sPh[j]), &s, &c);
-                    dg += sV[j] * sOm[j] * c;
-                    gv[j] += lE * s;
-                    gp[j] += lE * sV[j] * c;
-                }
+            for (int j = 0; j < NRF; ++j) {
+                // sin and cos at the forward's phase, to rounding (the
+                // forward map itself keeps CUDA's sin)
+                double s, c;
+                rf_sincos(fma(sOm[j], t, sPh[j]), &s, &c);
+                dg += sV[j] * sOm[j] * c;
+                gv[j] += lE * s;
+                gp[j] += lE * sV[j] * c;
             }
             dg *= q;
             if (vind) {
@@ -314,7 +318,7 @@ adj_backward_kernel(const AdjTurn T, int kick, const double* __restrict__ dt,
         // programme gradients: warp sums, then one atomic per block and value
         const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
 #pragma unroll
-        for (int j = 0; j < kAdjMaxRf; ++j) {
+        for (int j = 0; j < NRF; ++j) {
             const double a = warp_sum(gv[j]), b = warp_sum(gp[j]);
             if (lane == 0) {
                 red[w][j] = a;
@@ -349,6 +353,45 @@ static int adj_allow_smem(K kernel, bool* done) {
         done[d.device & 63] = true;
     }
     return BLOND_OK;
+}
+
+// The same once per kernel and device, for kernels chosen at run time.
+template <typename K>
+static int adj_allow_smem(K kernel) {
+    static std::mutex m;
+    static std::set<std::pair<const void*, int>> done;
+    const DeviceInfo& d = device_info();
+    std::lock_guard<std::mutex> g(m);
+    const auto key = std::make_pair(reinterpret_cast<const void*>(kernel), d.device);
+    if (done.count(key)) return BLOND_OK;
+    cudaFuncAttributes fa;
+    BB_CUDA(cudaFuncGetAttributes(&fa, kernel));
+    BB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 d.max_smem_optin - (int)fa.sharedSizeBytes));
+    done.insert(key);
+    return BLOND_OK;
+}
+
+// The kernels for the run-time harmonic count n_rf (0..kAdjMaxRf).
+template <int PREC>
+static auto adj_forward_for(int n_rf) {
+    switch (n_rf) {
+        case 0: return adj_forward_kernel<PREC, 0>;
+        case 1: return adj_forward_kernel<PREC, 1>;
+        case 2: return adj_forward_kernel<PREC, 2>;
+        case 3: return adj_forward_kernel<PREC, 3>;
+        default: return adj_forward_kernel<PREC, 4>;
+    }
+}
+
+static auto adj_backward_for(int n_rf) {
+    switch (n_rf) {
+        case 0: return adj_backward_kernel<0>;
+        case 1: return adj_backward_kernel<1>;
+        case 2: return adj_backward_kernel<2>;
+        case 3: return adj_backward_kernel<3>;
+        default: return adj_backward_kernel<4>;
+    }
 }
 
 // One forward turn.  With a counter (`done`, zero between launches) the
@@ -393,17 +436,10 @@ static int adj_forward_launch(int precision, const double* dt_in, const void* dE
     cudaStream_t s = as_stream(stream);
     u64* prof = reinterpret_cast<u64*>(profile_out);
     int rc;
-    if (precision == BLOND_PREC_F64) {
-        static bool attr[64] = {false};
-        if ((rc = adj_allow_smem(adj_forward_kernel<BLOND_PREC_F64>, attr))) return rc;
-        adj_forward_kernel<BLOND_PREC_F64><<<grid, kAdjThreads, smem, s>>>(
-            T, dt_in, dE_in, dt_out, dE_out, prof, done);
-    } else {
-        static bool attr[64] = {false};
-        if ((rc = adj_allow_smem(adj_forward_kernel<BLOND_PREC_F32P64>, attr))) return rc;
-        adj_forward_kernel<BLOND_PREC_F32P64><<<grid, kAdjThreads, smem, s>>>(
-            T, dt_in, dE_in, dt_out, dE_out, prof, done);
-    }
+    const auto k = precision == BLOND_PREC_F64 ? adj_forward_for<BLOND_PREC_F64>(n_rf)
+                                               : adj_forward_for<BLOND_PREC_F32P64>(n_rf);
+    if ((rc = adj_allow_smem(k))) return rc;
+    k<<<grid, kAdjThreads, smem, s>>>(T, dt_in, dE_in, dt_out, dE_out, prof, done);
     BB_LAUNCH_CHECK();
     if (profile_out && !done) {
         fixed_to_counts_kernel<<<(n_slices + 255) / 256, 256, 0, s>>>(profile_out, n_slices,
@@ -483,13 +519,13 @@ int blond_adjoint_backward_turn(const double* dt, const double* dt_next, int64_t
     T.inv_w = inv_bin_width;
     T.smem_hist = n_slices <= adj_smem_limit() ? 1 : 0;
     T.vind_smem = T.vind && T.smem_hist && 3 * sizeof(double) * n_slices <= kAdjVindSmem;
-    static bool done[64] = {false};
     int rc;
-    if ((rc = adj_allow_smem(adj_backward_kernel, done))) return rc;
+    const auto k = adj_backward_for(kick ? n_rf : 0);
+    if ((rc = adj_allow_smem(k))) return rc;
     const size_t smem = T.smem_hist ? (T.vind_smem ? 3 : 2) * sizeof(double) * n_slices : 0;
     const int grid = particle_grid(n, kAdjThreads, 4);
-    adj_backward_kernel<<<grid, kAdjThreads, smem, as_stream(stream)>>>(
-        T, kick, dt, dt_next, lam_p_next, lam_dt, lam_dE, lam_v, grad_rf);
+    k<<<grid, kAdjThreads, smem, as_stream(stream)>>>(T, kick, dt, dt_next, lam_p_next, lam_dt,
+                                                      lam_dE, lam_v, grad_rf);
     BB_LAUNCH_CHECK();
     return BLOND_OK;
 }
