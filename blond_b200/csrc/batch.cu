@@ -180,7 +180,7 @@ particle_kernel_batch(const BatchArgs a) {
             if (KICK) {
 #pragma unroll
                 for (int q = 0; q < PP; ++q)
-                    track_pair<PREC, SOLVER, LIK, (TSM && LIK) ? TAB_ENTRIES : TAB_GLOBAL>(
+                    track_pair<PREC, SOLVER, LIK, (TSM && LIK) ? TAB_ENTRIES : TAB_GLOBAL, true>(
                         tq[q].x, tq[q].y, e[q].x, e[q].y, c, pa, a.order, stab);
 #pragma unroll
                 for (int q = 0; q < PP; ++q) {
@@ -209,7 +209,7 @@ particle_kernel_batch(const BatchArgs a) {
             double t0 = dt[g], t1 = t0;
             E e0 = dE[g], e1 = e0;
             if (KICK) {
-                track_pair<PREC, SOLVER, LIK, (TSM && LIK) ? TAB_ENTRIES : TAB_GLOBAL>(
+                track_pair<PREC, SOLVER, LIK, (TSM && LIK) ? TAB_ENTRIES : TAB_GLOBAL, true>(
                     t0, t1, e0, e1, c, pa, a.order, stab);
                 dt[g] = t0;
                 dE[g] = e0;
