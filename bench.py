@@ -477,17 +477,21 @@ def run_ours(args, world, rank, local):
                                  "vs the FP64 batch",
             "beams_within_1e-5": int(np.sum(eq.max(axis=1) <= 1e-5)),
             "max_rel_err": float(eq.max()),
+            "profile_l2_rel_err": _l2_summary(m["profile_l2"]["q32p64"]),
             "autotuned": q["autotuned"],
             "clocks": q["clocks"],
             "f32p64": {"value": f32["value"], "ms_per_step": f32["ms_per_step"],
                        "beams_within_1e-5": int(np.sum(ef.max(axis=1) <= 1e-5)),
-                       "max_rel_err": float(ef.max()), "clocks": f32["clocks"]},
+                       "max_rel_err": float(ef.max()),
+                       "profile_l2_rel_err": _l2_summary(m["profile_l2"]["f32p64"]),
+                       "clocks": f32["clocks"]},
             "f64": {"value": f64["value"], "ms_per_step": f64["ms_per_step"]},
             "control_fp64_dE_plus_0.01eV": {
                 "what": "FP64 from energies moved by 0.01 eV vs FP64: the beams' own "
                         "sensitivity after the same turns",
                 "beams_within_1e-5": int(np.sum(m["controls"]["shift"].max(axis=1) <= 1e-5)),
-                "max_rel_err": float(m["controls"]["shift"].max())},
+                "max_rel_err": float(m["controls"]["shift"].max()),
+                "profile_l2_rel_err": _l2_summary(m["profile_l2"]["control_shift"])},
         }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, turns, kind, cores, sec = cpu_reference(n, S, None, args.cpu_seconds)
@@ -721,6 +725,18 @@ def _c3_rel_errs(beams, other, ref):
     return np.array(out)
 
 
+def _c3_profile_l2(other, ref):
+    """Per beam: ||p_other - p_ref||_2 / ||p_ref||_2 of the profiles (the
+    turn's slice counts) of two BatchTrackers."""
+    po, pr = other.profiles_tensor(), ref.profiles_tensor()
+    return ((po - pr).norm(dim=1) / pr.norm(dim=1).clamp_min(1e-300)).cpu().numpy()
+
+
+def _l2_summary(v):
+    return {"median": float(np.median(v)), "p90": float(np.percentile(v, 90)),
+            "max": float(v.max())}
+
+
 def _err_summary(errs):
     return {"sigma_dt_median": float(np.median(errs[:, 0])),
             "sigma_dt_p90": float(np.percentile(errs[:, 0], 90)),
@@ -776,6 +792,8 @@ def c3_measure(n_beams, W, K, T_err, precisions=("q32p64", "f32p64", "f64"),
     if "f64" in trackers:
         for prec in precisions:
             if prec != "f64":
+                out.setdefault("profile_l2", {})[prec] = _c3_profile_l2(trackers[prec],
+                                                                       trackers["f64"])
                 out.setdefault("errors", {})[prec] = _c3_rel_errs(
                     beams, trackers[prec], trackers["f64"])
         for ctl in controls:
@@ -790,6 +808,8 @@ def c3_measure(n_beams, W, K, T_err, precisions=("q32p64", "f32p64", "f64"),
             for rf, _, _, _ in beams:
                 rf.counter[0] = 0
             out.setdefault("controls", {})[ctl] = _c3_rel_errs(beams, bp, trackers["f64"])
+            out.setdefault("profile_l2", {})["control_" + ctl] = _c3_profile_l2(
+                bp, trackers["f64"])
             del bp
     del trackers
     torch.cuda.empty_cache()
@@ -864,7 +884,7 @@ def run_c5(args):
     W, K = max(3, args.warmup), args.steps
     kt = min(K, 20)
     n = int(args.particles) if args.particles != 1e7 else int(1e8)
-    res, coords = {}, {}
+    res, coords, profs = {}, {}, {}
     peak = _peaks().get("hbm_gbs") or 6650.0
     shape = ((args.threads, args.blocks_per_sm, args.prefetch) if args.tune == "fixed"
              else None)
@@ -887,6 +907,7 @@ def run_c5(args):
         fused.check()
         w = (fused.dt > prof.cut_left) & (fused.dt < prof.cut_right)
         coords[key] = (fused.dt[w].std().item(), fused.energies()[w].std().item())
+        profs[key] = fused.profile_tensor().double().cpu()
         if not shift:
             head_ms, part_ms = fused.time_kernels(kt)
             ach = BYTES_PER_PARTICLE[prec] * n / (part_ms / kt * 1e-3) / 1e9
@@ -901,7 +922,9 @@ def run_c5(args):
         if key not in coords or "f64" not in coords:
             return None
         return {"sigma_dt": abs(coords[key][0] / coords["f64"][0] - 1),
-                "sigma_dE": abs(coords[key][1] / coords["f64"][1] - 1)}
+                "sigma_dE": abs(coords[key][1] / coords["f64"][1] - 1),
+                "profile_l2": float((profs[key] - profs["f64"]).norm()
+                                    / profs["f64"].norm())}
     r = res["q32p64"]
     return {
         "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": 1,
@@ -923,7 +946,8 @@ def run_c5(args):
                                       "achieved_gbs", "frac", "kernel")}
            for p in ("f32p64", "f64") if p in res},
         "rel_err_after_turns": {
-            "turns": W + K, "statistic": "in-window rms of dt and dE vs FP64",
+            "turns": W + K, "statistic": "in-window rms of dt and dE vs FP64; "
+                                         "profile_l2 = ||p - p_FP64||_2 / ||p_FP64||_2",
             "q32p64": err("q32p64"), "f32p64": err("f32p64"),
             "control_fp64_dE_plus_0.01eV": err("control_fp64_dE_plus_0.01eV")},
         "gpu_launches": 2 * K,
@@ -1220,6 +1244,9 @@ def main():
                 **({"control_fp64_one_ulp": _err_summary(m["controls"]["ulp"]),
                     "control_fp64_dE_plus_0.01eV": _err_summary(m["controls"]["shift"])}
                    if m.get("controls") else {})},
+            "profile_l2_rel_err_after_turns": {
+                "statistic": "||p - p_FP64||_2 / ||p_FP64||_2 of each beam's profile",
+                **{k: _l2_summary(v) for k, v in m.get("profile_l2", {}).items()}},
             "gpu_launches": 2 * K,
         }), flush=True)
         return
