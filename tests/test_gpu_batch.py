@@ -83,6 +83,39 @@ def test_batch_matches_oracle_and_single_beam_engine(cuda, S):
         np.testing.assert_array_equal(dE, beam.dE.cpu().numpy())
 
 
+@pytest.mark.parametrize("precision", ["f64", "q32p64"])
+def test_batch_chunks_claimed_beyond_the_first_wave(cuda, precision):
+    """More chunks than resident blocks (1024-particle chunks, one 256-thread
+    block per SM): blocks claim chunks as they finish, largest first, across
+    turns; every beam, chunk starts at odd offsets included, ends bit for
+    bit where the single-beam engine leaves it."""
+    turns = 4
+    counts = [3000, 1, 200001, 777, 40001]
+    # one energy unit for every beam (the default, from each beam's largest
+    # |dE|, is too fine for the one-particle beam's energy swing)
+    unit = {"energy_unit": 0.5} if precision == "q32p64" else {}
+    built = [make_beam(k, n, turns) for k, n in enumerate(counts)]
+    batch = BatchTracker([(RingAndRFTracker(rf, beam), prof, tiv)
+                          for _, rf, beam, prof, tiv, _, _ in built],
+                         precision=precision, turns_per_graph=2,
+                         energy_units=[0.5] * len(counts) if unit else None)
+    batch.set_shape(256, 1, 4, 1024, False)
+    n_chunks = sum(-(-n // 1024) for n in counts)
+    assert n_chunks > torch.cuda.get_device_properties(0).multi_processor_count
+    batch.track(turns)
+    batch.check()
+    prof = batch.profiles_tensor().cpu().numpy()
+    for b, n in enumerate(counts):
+        ring, rf, beam, p, tiv, iv, _ = make_beam(b, n, turns)
+        f = FusedTracker(RingAndRFTracker(rf, beam), p, tiv, precision=precision,
+                         turns_per_graph=2, **unit)
+        f.track(turns)
+        dt, dE = (x.cpu().numpy() for x in batch.coordinates(b))
+        np.testing.assert_array_equal(dt, f.dt.cpu().numpy())
+        np.testing.assert_array_equal(dE, f.dE.cpu().numpy())
+        np.testing.assert_array_equal(prof[b], f.profile_tensor().cpu().numpy())
+
+
 def test_batch_f32p64_bunch_statistics(cuda):
     turns = 100
     counts = [20000, 50000, 30000]
