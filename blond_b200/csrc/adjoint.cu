@@ -168,6 +168,10 @@ __global__ void __launch_bounds__(kAdjThreads)
 adj_forward_kernel(const AdjTurn T, const double* dt_in, const void* dE_in, double* dt_out,
                    void* dE_out, u64* prof_out, unsigned* done) {
     using E = typename AdjE<PREC>::E;
+    // launched with programmatic stream serialization inside the runs: the
+    // next grid may launch now; the programme and shared memory are set up
+    // before this grid waits for the one before it
+    pdl_launch_dependents();
     extern __shared__ u64 shf[];
     __shared__ double sV[kAdjMaxRf], sOm[kAdjMaxRf], sPh[kAdjMaxRf];
     if (threadIdx.x < T.n_rf) {
@@ -179,6 +183,7 @@ adj_forward_kernel(const AdjTurn T, const double* dt_in, const void* dE_in, doub
     const bool hsm = dep && T.smem_hist;
     u64* h = hsm ? shf : prof_out;
     if (hsm) zero_shared(shf, T.S);
+    pdl_wait();  // coordinates, induced voltage and counter of the grids before
     const double* vind = T.vind;
     if (vind && T.vind_smem) {
         double* sv = reinterpret_cast<double*>(shf + (hsm ? T.S : 0));
@@ -249,11 +254,13 @@ adj_backward_kernel(const AdjTurn T, int kick, const double* __restrict__ dt,
     double* lp = sm ? sh : const_cast<double*>(lam_p_next);
     double* lv = sm ? sh + S : lam_v;
     const double* vind = T.vind;
+    pdl_launch_dependents();  // as in adj_forward_kernel
     if (kick && threadIdx.x < T.n_rf) {
         sV[threadIdx.x] = T.V[threadIdx.x];
         sOm[threadIdx.x] = T.om[threadIdx.x];
         sPh[threadIdx.x] = T.ph[threadIdx.x];
     }
+    pdl_wait();  // the adjoint and coordinates of the grids before
     if (sm) {
         for (int k = threadIdx.x; k < S; k += blockDim.x) {
             sh[k] = lam_p_next ? lam_p_next[k] : 0.0;
@@ -372,6 +379,25 @@ static int adj_allow_smem(K kernel) {
     return BLOND_OK;
 }
 
+// Launch, with programmatic stream serialization when pdl (the turn loops
+// of the runs: each grid launches while the one before it finishes).
+template <typename... KArgs, typename... Args>
+static int adj_launch(void (*k)(KArgs...), int grid, size_t smem, cudaStream_t s, bool pdl,
+                      Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(kAdjThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    BB_CUDA(cudaLaunchKernelEx(&cfg, k, args...));
+    return BLOND_OK;
+}
+
 // The kernels for the run-time harmonic count n_rf (0..kAdjMaxRf).
 template <int PREC>
 static auto adj_forward_for(int n_rf) {
@@ -403,7 +429,8 @@ static int adj_forward_launch(int precision, const double* dt_in, const void* dE
                               const double* phi_rf, double acc_kick, double charge,
                               double drift_coeff, const double* induced_voltage,
                               int n_slices, double bin_center0, double inv_bin_width,
-                              double* profile_out, unsigned* done, void* stream) {
+                              double* profile_out, unsigned* done, void* stream,
+                              bool pdl = false) {
     BB_CHECK_ARG(precision == BLOND_PREC_F64 || precision == BLOND_PREC_F32P64,
                  "adjoint_forward_turn: unknown precision %d", precision);
     BB_CHECK_SIZE(n_rf >= 0 && n_rf <= kAdjMaxRf, "adjoint_forward_turn: n_rf=%d not in "
@@ -439,14 +466,56 @@ static int adj_forward_launch(int precision, const double* dt_in, const void* dE
     const auto k = precision == BLOND_PREC_F64 ? adj_forward_for<BLOND_PREC_F64>(n_rf)
                                                : adj_forward_for<BLOND_PREC_F32P64>(n_rf);
     if ((rc = adj_allow_smem(k))) return rc;
-    k<<<grid, kAdjThreads, smem, s>>>(T, dt_in, dE_in, dt_out, dE_out, prof, done);
-    BB_LAUNCH_CHECK();
+    if ((rc = adj_launch(k, grid, smem, s, pdl, T, dt_in, dE_in, dt_out, dE_out, prof, done)))
+        return rc;
     if (profile_out && !done) {
         fixed_to_counts_kernel<<<(n_slices + 255) / 256, 256, 0, s>>>(profile_out, n_slices,
                                                                       T.fix_bits);
         BB_LAUNCH_CHECK();
     }
     return BLOND_OK;
+}
+
+// One backward turn (blond_adjoint_backward_turn), with programmatic stream
+// serialization when pdl.
+static int adj_backward_launch(const double* dt, const double* dt_next, int64_t n,
+                                double* lam_dt, double* lam_dE, const double* lam_p_next,
+                                int kick, int n_rf, const double* voltage,
+                                const double* omega_rf, const double* phi_rf, double charge,
+                                double drift_coeff, const double* induced_voltage,
+                                int n_slices, double bin_center0, double inv_bin_width,
+                                double* lam_v, double* grad_rf, void* stream,
+                                bool pdl = false) {
+    BB_CHECK_SIZE(n_rf >= 0 && n_rf <= kAdjMaxRf, "adjoint_backward_turn: n_rf=%d not in "
+                  "[0, %d]", n_rf, kAdjMaxRf);
+    BB_CHECK_ARG(n >= 0 && n_slices >= 2, "adjoint_backward_turn: bad size");
+    BB_CHECK_ARG(n == 0 || (lam_dt && lam_dE), "adjoint_backward_turn: null adjoint");
+    BB_CHECK_ARG(!lam_p_next || dt_next, "adjoint_backward_turn: lam_p_next needs dt_next");
+    BB_CHECK_ARG(!kick || ((n == 0 || dt) && grad_rf && (!induced_voltage || lam_v) &&
+                           (n_rf == 0 || (voltage && omega_rf && phi_rf))),
+                 "adjoint_backward_turn: null pointer");
+    if (n == 0) return BLOND_OK;
+    AdjTurn T = {};
+    T.n = n;
+    T.n_rf = n_rf;
+    T.V = voltage;
+    T.om = omega_rf;
+    T.ph = phi_rf;
+    T.charge = charge;
+    T.drift_c = drift_coeff;
+    T.vind = kick ? induced_voltage : nullptr;
+    T.S = n_slices;
+    T.bc0 = bin_center0;
+    T.inv_w = inv_bin_width;
+    T.smem_hist = n_slices <= adj_smem_limit() ? 1 : 0;
+    T.vind_smem = T.vind && T.smem_hist && 3 * sizeof(double) * n_slices <= kAdjVindSmem;
+    int rc;
+    const auto k = adj_backward_for(kick ? n_rf : 0);
+    if ((rc = adj_allow_smem(k))) return rc;
+    const size_t smem = T.smem_hist ? (T.vind_smem ? 3 : 2) * sizeof(double) * n_slices : 0;
+    const int grid = particle_grid(n, kAdjThreads, 4);
+    return adj_launch(k, grid, smem, as_stream(stream), pdl, T, kick, dt, dt_next, lam_p_next,
+                      lam_dt, lam_dE, lam_v, grad_rf);
 }
 
 }  // namespace bb
@@ -496,38 +565,9 @@ int blond_adjoint_backward_turn(const double* dt, const double* dt_next, int64_t
                                 double drift_coeff, const double* induced_voltage,
                                 int n_slices, double bin_center0, double inv_bin_width,
                                 double* lam_v, double* grad_rf, void* stream) {
-    BB_CHECK_SIZE(n_rf >= 0 && n_rf <= kAdjMaxRf, "adjoint_backward_turn: n_rf=%d not in "
-                  "[0, %d]", n_rf, kAdjMaxRf);
-    BB_CHECK_ARG(n >= 0 && n_slices >= 2, "adjoint_backward_turn: bad size");
-    BB_CHECK_ARG(n == 0 || (lam_dt && lam_dE), "adjoint_backward_turn: null adjoint");
-    BB_CHECK_ARG(!lam_p_next || dt_next, "adjoint_backward_turn: lam_p_next needs dt_next");
-    BB_CHECK_ARG(!kick || ((n == 0 || dt) && grad_rf && (!induced_voltage || lam_v) &&
-                           (n_rf == 0 || (voltage && omega_rf && phi_rf))),
-                 "adjoint_backward_turn: null pointer");
-    if (n == 0) return BLOND_OK;
-    AdjTurn T = {};
-    T.n = n;
-    T.n_rf = n_rf;
-    T.V = voltage;
-    T.om = omega_rf;
-    T.ph = phi_rf;
-    T.charge = charge;
-    T.drift_c = drift_coeff;
-    T.vind = kick ? induced_voltage : nullptr;
-    T.S = n_slices;
-    T.bc0 = bin_center0;
-    T.inv_w = inv_bin_width;
-    T.smem_hist = n_slices <= adj_smem_limit() ? 1 : 0;
-    T.vind_smem = T.vind && T.smem_hist && 3 * sizeof(double) * n_slices <= kAdjVindSmem;
-    int rc;
-    const auto k = adj_backward_for(kick ? n_rf : 0);
-    if ((rc = adj_allow_smem(k))) return rc;
-    const size_t smem = T.smem_hist ? (T.vind_smem ? 3 : 2) * sizeof(double) * n_slices : 0;
-    const int grid = particle_grid(n, kAdjThreads, 4);
-    k<<<grid, kAdjThreads, smem, as_stream(stream)>>>(T, kick, dt, dt_next, lam_p_next, lam_dt,
-                                                      lam_dE, lam_v, grad_rf);
-    BB_LAUNCH_CHECK();
-    return BLOND_OK;
+    return adj_backward_launch(dt, dt_next, n, lam_dt, lam_dE, lam_p_next, kick, n_rf, voltage,
+                               omega_rf, phi_rf, charge, drift_coeff, induced_voltage, n_slices,
+                               bin_center0, inv_bin_width, lam_v, grad_rf, stream);
 }
 
 int blond_adjoint_spectral(int mode, const double* x, int n_slices, const double* impedance,
@@ -591,6 +631,7 @@ struct AdjSpectral {
         SpecParams P = {};
         P.p = plan;
         P.twg = tw;
+        P.pdl = 1;  // inside the turn loops of the runs
         P.mode = SPEC_FORWARD | SPEC_MULTIPLY | SPEC_INVERSE;
         P.in_f64 = x;
         P.n_in = S;
@@ -675,7 +716,8 @@ int blond_adjoint_forward_run(int precision, double* dt, void* dE, int64_t n, in
         if ((rc = adj_forward_launch(
                  precision, dt, dE, dt, dE, n, n_rf, voltage + t * n_rf, omega_rf + t * n_rf,
                  phi_rf + t * n_rf, acc_kick[t], charge, drift_coeff[t], vind, n_slices,
-                 bin_center0, inv_bin_width, profile + (t + 1) * n_slices, done.p, stream)))
+                 bin_center0, inv_bin_width, profile + (t + 1) * n_slices, done.p, stream,
+                 true)))
             return rc;
     }
     return BLOND_OK;
@@ -722,21 +764,22 @@ int blond_adjoint_backward_run(int precision, int64_t n, int n_rf, int64_t n_tur
         BB_CUDA(cudaMemcpyAsync(dE_work, static_cast<const char*>(ckpt_dE) + (size_t)seg * n * esz,
                                 esz * n, cudaMemcpyDeviceToDevice, s));
         for (int64_t t = a; t < b; ++t) {
-            if ((rc = blond_adjoint_forward_turn(
+            if ((rc = adj_forward_launch(
                      precision, states + (t - a) * n, dE_work, states + (t - a + 1) * n,
                      dE_work, n, n_rf, voltage + t * n_rf, omega_rf + t * n_rf,
                      phi_rf + t * n_rf, acc_kick[t], charge, drift_coeff[t],
                      has_z ? induced_voltage + t * n_slices : nullptr, n_slices, bin_center0,
-                     inv_bin_width, nullptr, stream)))
+                     inv_bin_width, nullptr, nullptr, stream, true)))
                 return rc;
         }
         for (int64_t t = b - 1; t >= a; --t) {
-            if ((rc = blond_adjoint_backward_turn(
+            if ((rc = adj_backward_launch(
                      states + (t - a) * n, states + (t - a + 1) * n, n, lam_dt, lam_dE, lam_p, 1,
                      n_rf, voltage + t * n_rf, omega_rf + t * n_rf, phi_rf + t * n_rf, charge,
                      drift_coeff[t], has_z ? induced_voltage + t * n_slices : nullptr,
                      n_slices, bin_center0, inv_bin_width,
-                     has_z ? lam_v + t * n_slices : nullptr, grad_rf + t * 2 * n_rf, stream)))
+                     has_z ? lam_v + t * n_slices : nullptr, grad_rf + t * 2 * n_rf, stream,
+                     true)))
                 return rc;
             if (has_z) {
                 if ((rc = sp.run(1, lam_v + t * n_slices, n_slices, impedance_conj, scale,
