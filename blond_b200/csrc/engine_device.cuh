@@ -290,11 +290,23 @@ __device__ __forceinline__ void track_pair(double& t0, double& t1,
             s1 = (E)x1;
         } else {
             float x0 = 0.0f, x1 = 0.0f;
-            // unrolled by two: C2 F32P64 (one harmonic) pass 47.3 -> 46.8 us
+            if (RF2 && a.n_rf == 2) {
+                // as rf_sum_pair: four independent sines, the loop's expressions
+                const float s00 = rf_sinf(fma(c.op[0].x, t0, c.op[0].y));
+                const float s10 = rf_sinf(fma(c.op[0].x, t1, c.op[0].y));
+                const float s01 = rf_sinf(fma(c.op[1].x, t0, c.op[1].y));
+                const float s11 = rf_sinf(fma(c.op[1].x, t1, c.op[1].y));
+                x0 += c.Vf[0] * s00;
+                x1 += c.Vf[0] * s10;
+                x0 += c.Vf[1] * s01;
+                x1 += c.Vf[1] * s11;
+            } else {
+                // unrolled by two: C2 F32P64 (one harmonic) pass 47.3 -> 46.8 us
 #pragma unroll 2
-            for (int j = 0; j < a.n_rf; ++j) {
-                x0 += c.Vf[j] * rf_sinf(fma(c.op[j].x, t0, c.op[j].y));
-                x1 += c.Vf[j] * rf_sinf(fma(c.op[j].x, t1, c.op[j].y));
+                for (int j = 0; j < a.n_rf; ++j) {
+                    x0 += c.Vf[j] * rf_sinf(fma(c.op[j].x, t0, c.op[j].y));
+                    x1 += c.Vf[j] * rf_sinf(fma(c.op[j].x, t1, c.op[j].y));
+                }
             }
             s0 = (E)x0;
             s1 = (E)x1;
